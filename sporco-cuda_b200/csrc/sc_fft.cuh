@@ -1,0 +1,358 @@
+// In-shared-memory mixed-radix Stockham FFT executed by a group of threads.
+//
+// This replaces the role cuFFT plays in the reference (cufftPlanMany /
+// cufftExecR2C / cufftExecC2R at sporco_cuda/src/cbpdn.cu:171-180, 283-350):
+// every 1-D transform of the ADMM iteration (length W along image rows,
+// length H along columns) is done by one thread group inside a fused kernel,
+// on data staged in shared memory, so that the transforms never make their
+// own round trip through HBM.
+//
+// Conventions
+//  * Forward transform, unnormalised: X[k] = sum_j x[j] exp(-2 pi i jk/n)
+//    (numpy / cuFFT convention).  Inverse transforms are done by the callers
+//    as conj(FFT(conj(x))), which costs nothing extra because the callers
+//    stage the data into and out of shared memory anyway.
+//  * Twiddles: one table tw[j] = exp(-2 pi i j/n), j < n, evaluated in
+//    double precision and rounded to float.  Every twiddle of every
+//    pass is an entry of that table.
+//  * Stockham auto-sort (natural order in and out): a pass of radix R with
+//    Ns = product of the previous radices maps butterfly j (0 <= j < n/R)
+//        in[j + q n/R] (q < R)  ->  out[(j/Ns) Ns R + j%Ns + q Ns]
+//    after multiplying input q by w_{Ns R}^{q (j%Ns)} and taking an R-point
+//    DFT.  Passes are done in place: every thread first loads and combines
+//    all of its butterflies into registers, the group synchronises, then all
+//    results are stored.
+//  * A group of g threads does one transform; several groups of a CTA run
+//    transforms of the same length in lock step and synchronise with
+//    __syncthreads() (all groups must call the routine together).
+//  * MAXE bounds the elements one thread holds: the caller guarantees
+//    n <= MAXE * g.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define SC_FFT_MAX_PASS 24
+
+struct FftPlan {
+  int n;
+  int npass;
+  int radix[SC_FFT_MAX_PASS];
+};
+
+// ---------------------------------------------------------------- complex --
+__device__ __forceinline__ float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 c_mul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+__device__ __forceinline__ float2 c_mulc(float2 a, float2 b) {
+  return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__device__ __forceinline__ float2 c_conj(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ float2 c_scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+// (-i) * a
+__device__ __forceinline__ float2 c_mul_mi(float2 a) { return make_float2(a.y, -a.x); }
+// (+i) * a
+__device__ __forceinline__ float2 c_mul_pi(float2 a) { return make_float2(-a.y, a.x); }
+__device__ __forceinline__ float c_abs2(float2 a) { return a.x * a.x + a.y * a.y; }
+
+// ------------------------------------------------------------- butterflies --
+// Forward R-point DFTs, in registers.  Constants are exact values of the
+// roots of unity (cos/sin of 2 pi/3, 2 pi/5, 4 pi/5, pi/4) to float precision.
+__device__ __forceinline__ void dft2(float2* v) {
+  float2 a = v[0];
+  v[0] = c_add(a, v[1]);
+  v[1] = c_sub(a, v[1]);
+}
+
+__device__ __forceinline__ void dft3(float2* v) {
+  const float h = 0.8660254037844386f;  // sin(2 pi / 3)
+  float2 s = c_add(v[1], v[2]);
+  float2 d = c_sub(v[1], v[2]);
+  float2 a = v[0];
+  v[0] = c_add(a, s);
+  float2 m = make_float2(a.x - 0.5f * s.x, a.y - 0.5f * s.y);
+  float2 t = c_mul_mi(c_scale(d, h));  // -i sin(2pi/3) (b - c)
+  v[1] = c_add(m, t);
+  v[2] = c_sub(m, t);
+}
+
+__device__ __forceinline__ void dft4(float2* v) {
+  float2 t0 = c_add(v[0], v[2]);
+  float2 t1 = c_sub(v[0], v[2]);
+  float2 t2 = c_add(v[1], v[3]);
+  float2 t3 = c_mul_mi(c_sub(v[1], v[3]));
+  v[0] = c_add(t0, t2);
+  v[2] = c_sub(t0, t2);
+  v[1] = c_add(t1, t3);
+  v[3] = c_sub(t1, t3);
+}
+
+__device__ __forceinline__ void dft5(float2* v) {
+  const float c1 = 0.30901699437494745f;   // cos(2 pi/5)
+  const float c2 = -0.8090169943749475f;   // cos(4 pi/5)
+  const float s1 = 0.9510565162951535f;    // sin(2 pi/5)
+  const float s2 = 0.5877852522924731f;    // sin(4 pi/5)
+  float2 a0 = v[0];
+  float2 t1 = c_add(v[1], v[4]), d1 = c_sub(v[1], v[4]);
+  float2 t2 = c_add(v[2], v[3]), d2 = c_sub(v[2], v[3]);
+  v[0] = c_add(a0, c_add(t1, t2));
+  float2 m1 = make_float2(a0.x + c1 * t1.x + c2 * t2.x, a0.y + c1 * t1.y + c2 * t2.y);
+  float2 m2 = make_float2(a0.x + c2 * t1.x + c1 * t2.x, a0.y + c2 * t1.y + c1 * t2.y);
+  float2 e1 = c_mul_mi(make_float2(s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y));
+  float2 e2 = c_mul_mi(make_float2(s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y));
+  v[1] = c_add(m1, e1);
+  v[4] = c_sub(m1, e1);
+  v[2] = c_add(m2, e2);
+  v[3] = c_sub(m2, e2);
+}
+
+__device__ __forceinline__ void dft8(float2* v) {
+  const float r = 0.7071067811865476f;  // cos(pi/4)
+  float2 e[4] = {v[0], v[2], v[4], v[6]};
+  float2 o[4] = {v[1], v[3], v[5], v[7]};
+  dft4(e);
+  dft4(o);
+  // w8^1 = r (1 - i), w8^2 = -i, w8^3 = r (-1 - i)
+  float2 o1 = make_float2(r * (o[1].x + o[1].y), r * (o[1].y - o[1].x));
+  float2 o2 = c_mul_mi(o[2]);
+  float2 o3 = make_float2(r * (o[3].y - o[3].x), -r * (o[3].x + o[3].y));
+  v[0] = c_add(e[0], o[0]);
+  v[4] = c_sub(e[0], o[0]);
+  v[1] = c_add(e[1], o1);
+  v[5] = c_sub(e[1], o1);
+  v[2] = c_add(e[2], o2);
+  v[6] = c_sub(e[2], o2);
+  v[3] = c_add(e[3], o3);
+  v[7] = c_sub(e[3], o3);
+}
+
+template <int R>
+__device__ __forceinline__ void dft_r(float2* v) {
+  if constexpr (R == 2) dft2(v);
+  else if constexpr (R == 3) dft3(v);
+  else if constexpr (R == 4) dft4(v);
+  else if constexpr (R == 5) dft5(v);
+  else if constexpr (R == 8) dft8(v);
+}
+
+// ------------------------------------------------------------------ passes --
+template <int R, int MAXE>
+__device__ __forceinline__ void stockham_pass(float2* data, int n, int Ns,
+                                              const float2* __restrict__ tw,
+                                              int t, int g) {
+  constexpr int MAXB = (MAXE + R - 1) / R;
+  const int B = n / R;
+  const int step = n / (Ns * R);
+  float2 v[MAXB][R];
+#pragma unroll
+  for (int i = 0; i < MAXB; ++i) {
+    const int j = t + i * g;
+    if (j < B) {
+#pragma unroll
+      for (int q = 0; q < R; ++q) v[i][q] = data[j + q * B];
+      if (Ns > 1) {
+        const int k = j % Ns;
+#pragma unroll
+        for (int q = 1; q < R; ++q) v[i][q] = c_mul(v[i][q], __ldg(&tw[q * k * step]));
+      }
+      dft_r<R>(v[i]);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < MAXB; ++i) {
+    const int j = t + i * g;
+    if (j < B) {
+      const int k = j % Ns;
+      const int base = (j - k) * R + k;
+#pragma unroll
+      for (int q = 0; q < R; ++q) data[base + q * Ns] = v[i][q];
+    }
+  }
+  __syncthreads();
+}
+
+// Any radix (used for prime factors other than 2, 3, 5): each thread
+// computes whole outputs, O(R) work per output.
+template <int MAXE>
+__device__ __noinline__ void generic_pass(float2* data, int n, int R, int Ns,
+                                             const float2* __restrict__ tw,
+                                             int t, int g) {
+  const int B = n / R;
+  const int step = n / (Ns * R);
+  float2 out[MAXE];
+#pragma unroll
+  for (int i = 0; i < MAXE; ++i) {
+    const int o = t + i * g;
+    if (o < n) {
+      const int q = o / B;
+      const int j = o - q * B;
+      const int k = j % Ns;
+      const int e1 = k * step + q * B;  // < n
+      float2 acc = make_float2(0.f, 0.f);
+      int e = 0;
+      for (int s = 0; s < R; ++s) {
+        const float2 x = data[j + s * B];
+        const float2 w = __ldg(&tw[e]);
+        acc.x += x.x * w.x - x.y * w.y;
+        acc.y += x.x * w.y + x.y * w.x;
+        e += e1;
+        if (e >= n) e -= n;
+      }
+      out[i] = acc;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < MAXE; ++i) {
+    const int o = t + i * g;
+    if (o < n) {
+      const int q = o / B;
+      const int j = o - q * B;
+      const int k = j % Ns;
+      data[(j - k) * R + k + q * Ns] = out[i];
+    }
+  }
+  __syncthreads();
+}
+
+// One pass of a runtime plan.  Kept out of line: with the passes inlined into
+// a loop over a runtime radix sequence the register allocation of the
+// calling kernel grows past 200 registers.
+template <int MAXE>
+__device__ __noinline__ void fft_pass(float2* data, int n, int R, int Ns,
+                                      const float2* __restrict__ tw, int t, int g) {
+  switch (R) {
+    case 2: stockham_pass<2, MAXE>(data, n, Ns, tw, t, g); break;
+    case 3: stockham_pass<3, MAXE>(data, n, Ns, tw, t, g); break;
+    case 4: stockham_pass<4, MAXE>(data, n, Ns, tw, t, g); break;
+    case 5: stockham_pass<5, MAXE>(data, n, Ns, tw, t, g); break;
+    case 8: stockham_pass<8, MAXE>(data, n, Ns, tw, t, g); break;
+    default: generic_pass<MAXE>(data, n, R, Ns, tw, t, g); break;
+  }
+}
+
+// In-place forward DFT of data[0..n) (shared memory) by a group of g threads,
+// for any n (runtime plan; the fallback path).
+template <int MAXE>
+__device__ __forceinline__ void fft_forward(float2* data, const FftPlan& P,
+                                            const float2* __restrict__ tw, int t, int g) {
+  int Ns = 1;
+  const int np = P.npass;
+  for (int p = 0; p < np; ++p) {
+    const int R = P.radix[p];
+    fft_pass<MAXE>(data, P.n, R, Ns, tw, t, g);
+    Ns *= R;
+  }
+}
+
+// ----------------------------------------------------- compile-time plans --
+// Transform lengths known at compile time get a fully unrolled plan: radix
+// sequence, strides, butterflies per thread and twiddle steps are constants,
+// which keeps the pass working set in registers.
+struct CtPlan {
+  int n;
+  int np;
+  int r[SC_FFT_MAX_PASS];
+};
+
+// Radix sequence: 8s, then one 4 or 2, then 3s, 5s, then other primes
+// (the same factorisation the runtime planner uses).
+__host__ __device__ constexpr CtPlan ct_plan(int n) {
+  CtPlan p{n, 0, {}};
+  int m = n, a = 0;
+  while (m % 2 == 0) { m /= 2; ++a; }
+  for (int i = 0; i < a / 3; ++i) p.r[p.np++] = 8;
+  if (a % 3 == 1) p.r[p.np++] = 2;
+  if (a % 3 == 2) p.r[p.np++] = 4;
+  while (m % 3 == 0) { m /= 3; p.r[p.np++] = 3; }
+  while (m % 5 == 0) { m /= 5; p.r[p.np++] = 5; }
+  for (int f = 7; m > 1 && p.np < SC_FFT_MAX_PASS; f += 2) {
+    while (m % f == 0 && p.np < SC_FFT_MAX_PASS) { m /= f; p.r[p.np++] = f; }
+  }
+  return p;
+}
+
+__host__ __device__ constexpr int ct_ns(const CtPlan& p, int k) {
+  int ns = 1;
+  for (int i = 0; i < k; ++i) ns *= p.r[i];
+  return ns;
+}
+
+__host__ __device__ constexpr int ct_pow2ceil(int x) {
+  int p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+// Threads per transform for a compile-time length: about 8 elements each.
+__host__ __device__ constexpr int ct_threads(int n) {
+  int g = ct_pow2ceil((n + 7) / 8);
+  return g < 32 ? 32 : (g > 256 ? 256 : g);
+}
+
+template <int N, int R, int NS, int G>
+__device__ __forceinline__ void ct_pass(float2* data, const float2* __restrict__ tw, int t) {
+  constexpr int B = N / R;
+  constexpr int NB = (B + G - 1) / G;
+  constexpr int STEP = N / (NS * R);
+  float2 v[NB][R];
+#pragma unroll
+  for (int i = 0; i < NB; ++i) {
+    const int j = t + i * G;
+    if ((B % G) == 0 || j < B) {
+#pragma unroll
+      for (int q = 0; q < R; ++q) v[i][q] = data[j + q * B];
+      if constexpr (NS > 1) {
+        const int k = j % NS;
+#pragma unroll
+        for (int q = 1; q < R; ++q) v[i][q] = c_mul(v[i][q], __ldg(&tw[q * k * STEP]));
+      }
+      dft_r<R>(v[i]);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < NB; ++i) {
+    const int j = t + i * G;
+    if ((B % G) == 0 || j < B) {
+      const int k = j % NS;
+      const int base = (j - k) * R + k;
+#pragma unroll
+      for (int q = 0; q < R; ++q) data[base + q * NS] = v[i][q];
+    }
+  }
+  __syncthreads();
+}
+
+template <int N, int G, int P = 0>
+__device__ __forceinline__ void fft_ct(float2* data, const float2* __restrict__ tw, int t) {
+  constexpr CtPlan pl = ct_plan(N);
+  if constexpr (P < pl.np) {
+    ct_pass<N, pl.r[P], ct_ns(pl, P), G>(data, tw, t);
+    fft_ct<N, G, P + 1>(data, tw, t);
+  }
+}
+
+// True when every radix of n has a hand-written butterfly.
+__host__ __device__ constexpr bool ct_fast_radices(int n) {
+  CtPlan p = ct_plan(n);
+  for (int i = 0; i < p.np; ++i)
+    if (p.r[i] != 2 && p.r[i] != 3 && p.r[i] != 4 && p.r[i] != 5 && p.r[i] != 8) return false;
+  return true;
+}
+
+// Forward DFT of length N (N > 0: compile-time plan, N == 0: runtime plan P
+// with g threads per transform).
+template <int N>
+__device__ __forceinline__ void fft_any(float2* data, const FftPlan& P,
+                                        const float2* __restrict__ tw, int t, int g) {
+  if constexpr (N == 0) {
+    fft_forward<16>(data, P, tw, t, g);
+  } else {
+    fft_ct<N, ct_threads(N)>(data, tw, t);
+  }
+}

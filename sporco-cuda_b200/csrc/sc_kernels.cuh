@@ -1,0 +1,560 @@
+// Fused ADMM kernels of the CBPDN solvers.
+//
+// One ADMM iteration (sporco_cuda/src/cbpdn.cu:319-567, cbpdn_grd.cu:358-606)
+// is three kernels and a conditional fourth:
+//
+//   col_kernel<COL_SOLVE>  spectrum columns: forward column FFT of the row
+//                          spectra of Y - U, b = conj(Df) Sf + rho (Y-U)^,
+//                          Sherman-Morrison solve across the M maps
+//                          (cluster-wide reduction of sum_m Df_m b_m / d_m),
+//                          inverse column FFT.  Replaces CalYU's consumer,
+//                          cufftExecR2C (column half), cuda_solvedbi_sm*,
+//                          cuda_solvedbd_sm*, cufftExecC2R (column half).
+//   row_kernel<ROW_ITER>   image rows: inverse row FFT, over-relaxation,
+//                          soft threshold / AMS mask step, dual update,
+//                          residual partial sums (FP64), then the forward row
+//                          FFT of the new Y - U.  Replaces cufftExecC2R (row
+//                          half), cuda_OverRelax_vec4, cuda_Shrink_CalU_*,
+//                          cuda_Cal_X_minus_U_W, cuda_Cal_residuals_norms_vec4,
+//                          the Yprv copy, cuda_CalYU_vec4 and cufftExecR2C
+//                          (row half).
+//   finalize_kernel        FP64 reduction of the partials, residuals, stopping
+//                          test, adaptive rho (host code at cbpdn.cu:405-559).
+//   row_kernel<ROW_FIXUP>  only when rho changed: U <- U / rsf and the row
+//                          spectra corrected by (1 - 1/rsf) rowFFT(U)
+//                          (replaces cublasSgeam at cbpdn.cu:546-549).
+//
+// HBM layout: real maps (B, M, H, W) float32; spectra (B, M, H, Wp) complex64
+// with Wp = W/2+1 rounded up to a multiple of 4 (storage padding only).
+#pragma once
+
+#include <cooperative_groups.h>
+
+#include "sc_internal.cuh"
+
+namespace cg = cooperative_groups;
+
+// Soft threshold as the reference's shrink kernels compute it
+// (cbpdn_kernels.cu:129-311): sign(v) max(|v| - t, 0), t may be negative.
+__device__ __forceinline__ float soft_threshold(float v, float t) {
+  const float a = fabsf(v) - t;
+  return a > 0.f ? copysignf(a, v) : 0.f;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Deterministic CTA-wide sum of NV doubles; result valid in thread 0.
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double* scratch) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) v[i] = warp_sum(v[i]);
+  if (lane == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) scratch[wid * NV + i] = v[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      double s = 0.0;
+      for (int w = 0; w < nw; ++w) s += scratch[w * NV + i];
+      v[i] = s;
+    }
+  }
+  __syncthreads();
+}
+
+// ============================================================== row pass ==
+// NW > 0: row length W known at compile time (specialised FFT plan);
+// NW == 0: any W (runtime FFT plan).
+template <int MODE, int NW>
+__global__ void __launch_bounds__(SC_ROW_THREADS, 2)
+row_kernel(RowParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* smem = reinterpret_cast<float2*>(smem_raw);
+  __shared__ double red_scratch[(SC_ROW_THREADS / 32) * 5];
+
+  const Geom& G = P.g;
+  const int b = blockIdx.y;
+  const int W = G.W, Wf = G.Wf, Wp = G.Wp, H = G.H;
+  const int g = NW > 0 ? ct_threads(NW) : P.gsz;
+  const int S = blockDim.x / g;
+  const int s = threadIdx.x / g;
+  const int t = threadIdx.x - s * g;
+  float2* z = smem + (size_t)s * W;
+
+  float thr = 0.f, rsf_c = 0.f, inv_rsf = 1.f;
+  if constexpr (MODE == ROW_ITER || MODE == ROW_FIXUP) {
+    const ImgState& st = P.st[b];
+    if (st.done) return;
+    if constexpr (MODE == ROW_ITER) {
+      thr = (float)((double)P.lam[b] / st.rho);
+    } else {
+      if (st.rsf == 1.0) return;
+      rsf_c = (float)(1.0 - 1.0 / st.rsf);
+      inv_rsf = (float)(1.0 / st.rsf);
+    }
+  }
+
+  const long rows = (long)G.M * H;           // rows per image
+  const long npairs = (rows + 1) / 2;
+  const size_t img_real = (size_t)rows * W;
+  const size_t img_spec = (size_t)rows * Wp;
+  float2* Fi = P.F + (size_t)b * img_spec;
+
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+
+  for (long pb = (long)blockIdx.x * S; pb < npairs; pb += (long)gridDim.x * S) {
+    const long p = pb + s;
+    const bool valid = p < npairs;
+    const long r0 = 2 * p, r1 = 2 * p + 1;
+    const bool has1 = valid && (r1 < rows);
+
+    // ---------------------------------------------------------- stage in
+    if constexpr (MODE == ROW_ITER || MODE == ROW_INV_REAL) {
+      // Hermitian-extend the two half spectra and pack them as A + iB; the
+      // inverse FFT is taken as conj(FFT(conj(.))).  The imaginary parts of
+      // the DC and (even W) Nyquist bins are ignored, as a C2R transform does.
+      if (valid) {
+        const float2* a = Fi + r0 * Wp;
+        const float2* bb = Fi + r1 * Wp;
+        for (int k = t; k < W; k += g) {
+          float2 A, Bv, Zc;
+          if (k < Wf) {
+            A = a[k];
+            Bv = has1 ? bb[k] : make_float2(0.f, 0.f);
+            if (k == 0 || 2 * k == W) { A.y = 0.f; Bv.y = 0.f; }
+            Zc = make_float2(A.x - Bv.y, -(A.y + Bv.x));
+          } else {
+            const int kk = W - k;
+            A = a[kk];
+            Bv = has1 ? bb[kk] : make_float2(0.f, 0.f);
+            Zc = make_float2(A.x + Bv.y, -(Bv.x - A.y));
+          }
+          z[k] = Zc;
+        }
+      }
+      __syncthreads();
+      fft_any<NW>(z, P.pw, P.twW, t, g);
+    }
+
+    // ---------------------------------------------------------- epilogue
+    if constexpr (MODE == ROW_ITER) {
+      if (valid) {
+        const int m0 = (int)(r0 / H), h0 = (int)(r0 - (long)m0 * H);
+        const int m1 = (int)(r1 / H), h1 = (int)(r1 - (long)m1 * H);
+        float* Y0 = P.Y + (size_t)b * img_real + (size_t)r0 * W;
+        float* U0 = P.U + (size_t)b * img_real + (size_t)r0 * W;
+        float* Y1 = Y0 + W;
+        float* U1 = U0 + W;
+        const int32_t* mk = P.mask ? P.mask + (size_t)b * H * W : nullptr;
+        float w0 = P.l1_scalar, w1 = P.l1_scalar;
+        if (P.l1_kind == 1) { w0 = P.l1w[m0]; w1 = has1 ? P.l1w[m1] : 0.f; }
+        const float* wr0 = P.l1_kind == 2 ? P.l1w + ((size_t)m0 * H + h0) * W : nullptr;
+        const float* wr1 = (P.l1_kind == 2 && has1) ? P.l1w + ((size_t)m1 * H + h1) * W : nullptr;
+        const bool ams0 = mk && m0 == 0, ams1 = mk && m1 == 0;
+        const float a = P.relax, a1 = 1.f - P.relax;
+        const bool relax = P.relax != 1.f;
+        for (int k = t; k < W; k += g) {
+          const float2 zz = z[k];
+          float yu0, yu1 = 0.f;
+          {
+            const float x = zz.x * P.invN;
+            const float yo = Y0[k], uo = U0[k];
+            const float xr = relax ? a * x + a1 * yo : x;
+            const float v = xr + uo;
+            float y;
+            if (ams0) y = (float)(1 - mk[h0 * W + k]) * v;
+            else y = soft_threshold(v, thr * (wr0 ? wr0[k] : w0));
+            const float u = v - y;
+            Y0[k] = y;
+            U0[k] = u;
+            yu0 = y - u;
+            const float dxy = x - y, dyy = yo - y;
+            acc[0] += (double)(x * x);
+            acc[1] += (double)(y * y);
+            acc[2] += (double)(u * u);
+            acc[3] += (double)(dxy * dxy);
+            acc[4] += (double)(dyy * dyy);
+          }
+          if (has1) {
+            const float x = -zz.y * P.invN;
+            const float yo = Y1[k], uo = U1[k];
+            const float xr = relax ? a * x + a1 * yo : x;
+            const float v = xr + uo;
+            float y;
+            if (ams1) y = (float)(1 - mk[h1 * W + k]) * v;
+            else y = soft_threshold(v, thr * (wr1 ? wr1[k] : w1));
+            const float u = v - y;
+            Y1[k] = y;
+            U1[k] = u;
+            yu1 = y - u;
+            const float dxy = x - y, dyy = yo - y;
+            acc[0] += (double)(x * x);
+            acc[1] += (double)(y * y);
+            acc[2] += (double)(u * u);
+            acc[3] += (double)(dxy * dxy);
+            acc[4] += (double)(dyy * dyy);
+          }
+          z[k] = make_float2(yu0, yu1);
+        }
+      }
+    } else if constexpr (MODE == ROW_INV_REAL) {
+      if (valid) {
+        float* d0 = P.dst + (size_t)b * img_real + (size_t)r0 * W;
+        for (int k = t; k < W; k += g) {
+          const float2 zz = z[k];
+          d0[k] = zz.x * P.invN;
+          if (has1) d0[W + k] = -zz.y * P.invN;
+        }
+      }
+    } else if constexpr (MODE == ROW_FWD_REAL) {
+      if (valid) {
+        const float* s0 = P.src + (size_t)b * img_real + (size_t)r0 * W;
+        for (int k = t; k < W; k += g)
+          z[k] = make_float2(s0[k], has1 ? s0[W + k] : 0.f);
+      }
+    } else if constexpr (MODE == ROW_FWD_DICT) {
+      if (valid) {
+        const int m0 = (int)(r0 / H), h0 = (int)(r0 - (long)m0 * H);
+        const int m1 = (int)(r1 / H), h1 = (int)(r1 - (long)m1 * H);
+        for (int k = t; k < W; k += g) {
+          float v0 = 0.f, v1 = 0.f;
+          if (h0 < P.Kr && k < P.Kc) v0 = P.D[((size_t)m0 * P.Kr + h0) * P.Kc + k];
+          if (has1 && h1 < P.Kr && k < P.Kc) v1 = P.D[((size_t)m1 * P.Kr + h1) * P.Kc + k];
+          z[k] = make_float2(v0, v1);
+        }
+      }
+    } else if constexpr (MODE == ROW_FIXUP) {
+      if (valid) {
+        float* U0 = P.U + (size_t)b * img_real + (size_t)r0 * W;
+        for (int k = t; k < W; k += g) {
+          const float u0 = U0[k];
+          const float u1 = has1 ? U0[W + k] : 0.f;
+          z[k] = make_float2(u0, u1);
+          U0[k] = u0 * inv_rsf;
+          if (has1) U0[W + k] = u1 * inv_rsf;
+        }
+      }
+    }
+
+    // ---------------------------------------------------------- forward + out
+    if constexpr (MODE != ROW_INV_REAL) {
+      __syncthreads();
+      fft_any<NW>(z, P.pw, P.twW, t, g);
+      if (valid) {
+        float2* a = Fi + r0 * Wp;
+        float2* bb = Fi + r1 * Wp;
+        for (int k = t; k < Wf; k += g) {
+          const float2 Zk = z[k];
+          const float2 Zm = z[k == 0 ? 0 : W - k];
+          // A = (Z_k + conj Z_{-k}) / 2 ;  B = (Z_k - conj Z_{-k}) / (2i)
+          const float2 A = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
+          const float2 Bv = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
+          if constexpr (MODE == ROW_FIXUP) {
+            float2 fa = a[k];
+            a[k] = make_float2(fa.x + rsf_c * A.x, fa.y + rsf_c * A.y);
+            if (has1) {
+              float2 fb = bb[k];
+              bb[k] = make_float2(fb.x + rsf_c * Bv.x, fb.y + rsf_c * Bv.y);
+            }
+          } else {
+            a[k] = A;
+            if (has1) bb[k] = Bv;
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  if constexpr (MODE == ROW_ITER) {
+    block_sum<5>(acc, red_scratch);
+    if (threadIdx.x == 0) {
+      double* out = P.partials + ((size_t)b * P.nblk + blockIdx.x) * 5;
+#pragma unroll
+      for (int i = 0; i < 5; ++i) out[i] = acc[i];
+    }
+  }
+}
+
+// =========================================================== column pass ==
+// Grid (G, ntiles, B).  For COL_SOLVE the G CTAs of one column tile form a
+// thread-block cluster; each handles a contiguous chunk of the maps.
+// NH > 0: column length H known at compile time; NH == 0: any H.
+template <int MODE, int NH>
+__global__ void __launch_bounds__(SC_COL_MAX_THREADS)
+col_kernel(ColParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Geom& G = P.g;
+  const int H = G.H, Wf = G.Wf, Wp = G.Wp, M = G.M;
+  const int Hs = P.Hs;
+  constexpr int T = SC_COL_TILE;
+  float2* buf = reinterpret_cast<float2*>(smem_raw);            // T x Hs
+  float2* num = buf + (size_t)T * Hs;                            // T*H (solve)
+  float* sden = reinterpret_cast<float*>(num + (size_t)T * H);   // T*H (solve)
+
+  const int b = blockIdx.z;
+  const int tile = blockIdx.y;
+  const int rank = blockIdx.x;
+  const int c0 = tile * T;
+  const int g = NH > 0 ? ct_threads(NH) : P.gsz;
+  const int grp = threadIdx.x / g;
+  const int t = threadIdx.x - grp * g;
+  const int NT = blockDim.x;
+  const int E = T * H;
+
+  float rho = 0.f;
+  if constexpr (MODE == COL_SOLVE) {
+    const ImgState& st = P.st[b];
+    if (st.done) return;  // uniform over the cluster (same image)
+    rho = (float)st.rho;
+  }
+
+  const int nmaps = M;
+  const int chunk = (nmaps + P.G - 1) / P.G;
+  const int m0 = rank * chunk;
+  const int m1 = min(nmaps, m0 + chunk);
+  float2* Fi = P.F + (size_t)b * nmaps * H * Wp;
+
+  auto load_tile = [&](int m, bool conj_in) {
+    const float2* src = Fi + (size_t)m * H * Wp + c0;
+    for (int e = threadIdx.x; e < E; e += NT) {
+      const int kr = e / T, c = e - kr * T;
+      float2 v = make_float2(0.f, 0.f);
+      if (c0 + c < Wf) v = src[(size_t)kr * Wp + c];
+      if (conj_in) v.y = -v.y;
+      buf[c * Hs + kr] = v;
+    }
+    __syncthreads();
+  };
+  auto store_tile = [&](int m, bool conj_out) {
+    float2* dst = Fi + (size_t)m * H * Wp + c0;
+    for (int e = threadIdx.x; e < E; e += NT) {
+      const int kr = e / T, c = e - kr * T;
+      if (c0 + c < Wf) {
+        float2 v = buf[c * Hs + kr];
+        if (conj_out) v.y = -v.y;
+        dst[(size_t)kr * Wp + c] = v;
+      }
+    }
+  };
+
+  if constexpr (MODE == COL_FWD || MODE == COL_INV) {
+    const bool inv = MODE == COL_INV;
+    for (int m = m0; m < m1; ++m) {
+      load_tile(m, inv);
+      fft_any<NH>(buf + grp * Hs, P.ph, P.twH, t, g);
+      store_tile(m, inv);
+      __syncthreads();
+    }
+    return;
+  } else {
+    const float2* Sh = P.Sh + (size_t)b * H * Wp + c0;
+    const float mu = P.mu;
+    const bool grd = P.grd != 0;
+    // ------------------------------------------------------------ pass 1
+    for (int e = threadIdx.x; e < E; e += NT) {
+      num[e] = make_float2(0.f, 0.f);
+      sden[e] = 0.f;
+    }
+    for (int m = m0; m < m1; ++m) {
+      load_tile(m, false);
+      fft_any<NH>(buf + grp * Hs, P.ph, P.twH, t, g);
+      const float2* Dm = P.Dh + (size_t)m * H * Wp + c0;
+      const float wg = grd ? mu * P.wgrd[m] : 0.f;
+      for (int e = threadIdx.x; e < E; e += NT) {
+        const int kr = e / T, c = e - kr * T;
+        const int kc = c0 + c;
+        if (kc < Wf) {
+          const float2 Dv = Dm[(size_t)kr * Wp + c];
+          const float2 Sv = Sh[(size_t)kr * Wp + c];
+          const float2 yu = buf[c * Hs + kr];
+          // b = conj(D) S + rho (Y - U)^
+          const float2 bv = make_float2(Dv.x * Sv.x + Dv.y * Sv.y + rho * yu.x,
+                                        Dv.x * Sv.y - Dv.y * Sv.x + rho * yu.y);
+          float d = rho;
+          if (grd) {
+            const float gh = 4.f - 2.f * __ldg(&P.twW[kc]).x - 2.f * __ldg(&P.twH[kr]).x;
+            d = wg * gh + rho;
+          }
+          const float id = 1.f / d;
+          const int a = c * H + kr;
+          float2 nv = num[a];
+          nv.x += (Dv.x * bv.x - Dv.y * bv.y) * id;
+          nv.y += (Dv.x * bv.y + Dv.y * bv.x) * id;
+          num[a] = nv;
+          sden[a] += (Dv.x * Dv.x + Dv.y * Dv.y) * id;
+        }
+      }
+      __syncthreads();
+    }
+    // ------------------------------------------------- reduce over the maps
+    if (P.G > 1) {
+      cg::cluster_group cluster = cg::this_cluster();
+      cluster.sync();
+      const int sl = (E + P.G - 1) / P.G;
+      const int e0 = rank * sl, e1 = min(E, e0 + sl);
+      for (int e = e0 + threadIdx.x; e < e1; e += NT) {
+        float2 ns = make_float2(0.f, 0.f);
+        float ds = 0.f;
+        for (int r = 0; r < P.G; ++r) {
+          const float2* rn = cluster.map_shared_rank(num, r);
+          const float* rd = cluster.map_shared_rank(sden, r);
+          const float2 v = rn[e];
+          ns.x += v.x;
+          ns.y += v.y;
+          ds += rd[e];
+        }
+        const float q = 1.f / (1.f + ds);
+        num[e] = make_float2(ns.x * q, ns.y * q);
+      }
+      cluster.sync();
+      for (int e = threadIdx.x; e < E; e += NT) {
+        const int owner = e / sl;
+        if (owner != rank) num[e] = cluster.map_shared_rank(num, owner)[e];
+      }
+      cluster.sync();
+    } else {
+      for (int e = threadIdx.x; e < E; e += NT) {
+        const float q = 1.f / (1.f + sden[e]);
+        num[e] = make_float2(num[e].x * q, num[e].y * q);
+      }
+      __syncthreads();
+    }
+    // ------------------------------------------------------------ pass 2
+    for (int m = m0; m < m1; ++m) {
+      load_tile(m, false);
+      fft_any<NH>(buf + grp * Hs, P.ph, P.twH, t, g);
+      const float2* Dm = P.Dh + (size_t)m * H * Wp + c0;
+      const float wg = grd ? mu * P.wgrd[m] : 0.f;
+      for (int e = threadIdx.x; e < E; e += NT) {
+        const int kr = e / T, c = e - kr * T;
+        const int kc = c0 + c;
+        float2 xo = make_float2(0.f, 0.f);
+        if (kc < Wf) {
+          const float2 Dv = Dm[(size_t)kr * Wp + c];
+          const float2 Sv = Sh[(size_t)kr * Wp + c];
+          const float2 yu = buf[c * Hs + kr];
+          const float2 bv = make_float2(Dv.x * Sv.x + Dv.y * Sv.y + rho * yu.x,
+                                        Dv.x * Sv.y - Dv.y * Sv.x + rho * yu.y);
+          float d = rho;
+          if (grd) {
+            const float gh = 4.f - 2.f * __ldg(&P.twW[kc]).x - 2.f * __ldg(&P.twH[kr]).x;
+            d = wg * gh + rho;
+          }
+          const float id = 1.f / d;
+          const float2 cb = num[c * H + kr];
+          // x = (b - conj(D) cb) / d
+          xo.x = (bv.x - (Dv.x * cb.x + Dv.y * cb.y)) * id;
+          xo.y = (bv.y - (Dv.x * cb.y - Dv.y * cb.x)) * id;
+        }
+        buf[c * Hs + kr] = make_float2(xo.x, -xo.y);  // conj for the inverse
+      }
+      __syncthreads();
+      fft_any<NH>(buf + grp * Hs, P.ph, P.twH, t, g);
+      store_tile(m, true);
+      __syncthreads();
+    }
+  }
+}
+
+// ============================================================== finalize ==
+// One CTA per image: FP64 reduction of the row-pass partials, residuals,
+// stopping test and adaptive rho (cbpdn.cu:405-436, 519-559; Boyd et al.
+// 2010 3.3-3.4; Wohlberg 2015).
+__global__ void finalize_kernel(const double* __restrict__ partials, int nblk,
+                                ImgState* st, FinParams F) {
+  __shared__ double scratch[(256 / 32) * 5];
+  const int b = blockIdx.x;
+  ImgState& S = st[b];
+  if (S.done) return;
+  double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  const double* p = partials + (size_t)b * nblk * 5;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
+#pragma unroll
+    for (int j = 0; j < 5; ++j) v[j] += p[(size_t)i * 5 + j];
+  }
+  block_sum<5>(v, scratch);
+  if (threadIdx.x != 0) return;
+  const double rho = S.rho;
+  const double nX = sqrt(v[0]), nY = sqrt(v[1]), nU = sqrt(v[2]);
+  double r = sqrt(v[3]);
+  double s = rho * sqrt(v[4]);
+  const double sq = sqrt(F.nelem);
+  double epri = sq * F.abs_tol + fmax(nX, nY) * F.rel_tol;
+  double edua = sq * F.abs_tol + rho * nU * F.rel_tol;
+  if (!F.std_residuals) {
+    double rn = fmax(nX, nY);
+    if (rn == 0.0) rn = 1.0;
+    const double sn = rho * (nU == 0.0 ? 1.0 : nU);
+    r /= rn;
+    s /= sn;
+    epri /= rn;
+    edua /= sn;
+  }
+  const int k = S.k + 1;
+  if (F.itstat) {
+    double* it = F.itstat + ((size_t)b * F.max_iter + (k - 1)) * 5;
+    it[0] = r; it[1] = s; it[2] = rho; it[3] = epri; it[4] = edua;
+  }
+  double rsf = 1.0;
+  if (F.auto_rho && k > 1 && (k % F.period) == 0) {
+    const double xi = F.xi[b];
+    double rhomlt;
+    if (F.auto_scaling) {
+      rhomlt = (s * xi > 0.0) ? sqrt(r / (s * xi)) : INFINITY;
+      if (rhomlt < 1.0) rhomlt = rhomlt > 0.0 ? 1.0 / rhomlt : INFINITY;
+      if (rhomlt > F.rho_scaling) rhomlt = F.rho_scaling;
+    } else {
+      rhomlt = F.rho_scaling;
+    }
+    if (r > xi * F.rsdl_ratio * s) rsf = rhomlt;
+    if (s > (F.rsdl_ratio / xi) * r) rsf = 1.0 / rhomlt;
+  }
+  S.nX = nX; S.nY = nY; S.nU = nU;
+  S.r = r; S.s = s; S.epri = epri; S.edua = edua;
+  S.rho = rsf * rho;
+  S.rsf = rsf;
+  S.k = k;
+  bool done = (r <= epri && s <= edua) || k >= F.max_iter;
+  if (!isfinite(r) || !isfinite(s)) {
+    S.status = 5;  // SC_ERR_NONFINITE
+    done = true;
+  }
+  if (done) {
+    S.done = 1;
+    if (F.ndone) atomicAdd(F.ndone, 1);
+  }
+}
+
+__global__ void init_state_kernel(ImgState* st, const float* rho0, int B, int* ndone) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b == 0 && ndone) *ndone = 0;
+  if (b >= B) return;
+  ImgState s;
+  s.rho = (double)rho0[b];
+  s.rsf = 1.0;
+  s.r = s.s = s.epri = s.edua = 0.0;
+  s.nX = s.nY = s.nU = 0.0;
+  s.k = 0;
+  s.done = 0;
+  s.status = 0;
+  s.pad = 0;
+  st[b] = s;
+}
+
+// tw[j] = exp(-2 pi i j / n), evaluated in double precision.
+__global__ void twiddle_kernel(float2* tw, int n) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  double s, c;
+  sincospi(-2.0 * (double)j / (double)n, &s, &c);
+  tw[j] = make_float2((float)c, (float)s);
+}

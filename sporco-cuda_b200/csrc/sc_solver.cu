@@ -1,0 +1,533 @@
+// Host driver of the CBPDN solvers: planning, workspace layout, launch
+// sequence, and the C ABI (native sc_* layer + reference-compatible layer).
+//
+// The reference's drivers (sporco_cuda/src/cbpdn.cu:86-616 and
+// cbpdn_grd.cu:97-658) allocate 9 full-size arrays, build cuFFT plans and
+// drive every ADMM iteration from the host with two device synchronisations
+// and managed-memory reads per iteration.  Here the iteration runs entirely
+// on the device: rho, the residuals and the stopping decision live in device
+// memory (ImgState), and the host only polls a "finished" counter every
+// `check_every` iterations.  State per image is Y, U (real) and one spectrum
+// array; the dictionary spectrum is shared by the batch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/sporco_b200.h"
+#include "sc_kernels.cuh"
+
+#define SC_VERSION "0.1.0"
+
+// ------------------------------------------------------------- error state --
+static thread_local int g_last_status = SC_OK;
+static thread_local char g_last_error[512] = "";
+
+static int set_status(int st, const char* fmt, ...) {
+  g_last_status = st;
+  if (fmt) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+    va_end(ap);
+  } else {
+    g_last_error[0] = 0;
+  }
+  return st;
+}
+
+#define CU_TRY(call)                                                          \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess)                                                    \
+      return set_status(e_ == cudaErrorMemoryAllocation ? SC_ERR_OOM : SC_ERR_CUDA, \
+                        "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                  \
+  } while (0)
+
+int sc_set_status_external(int st, const char* msg) { return set_status(st, msg && *msg ? "%s" : nullptr, msg); }
+
+extern "C" int sc_last_status(void) { return g_last_status; }
+extern "C" const char* sc_last_error(void) { return g_last_error; }
+extern "C" const char* sc_version(void) { return SC_VERSION; }
+
+// ------------------------------------------------------------------ planning --
+static int make_fft_plan(int n, FftPlan* p) {
+  memset(p, 0, sizeof(*p));
+  p->n = n;
+  int m = n, a = 0;
+  while (m % 2 == 0) { m /= 2; ++a; }
+  int q = a / 3, r = a % 3;
+  for (int i = 0; i < q; ++i) p->radix[p->npass++] = 8;
+  if (r == 1) p->radix[p->npass++] = 2;
+  if (r == 2) p->radix[p->npass++] = 4;
+  while (m % 3 == 0) { m /= 3; p->radix[p->npass++] = 3; }
+  while (m % 5 == 0) { m /= 5; p->radix[p->npass++] = 5; }
+  for (int f = 7; m > 1; f += 2) {
+    while (m % f == 0) {
+      m /= f;
+      if (p->npass >= SC_FFT_MAX_PASS) return -1;
+      p->radix[p->npass++] = f;
+    }
+    if (f * f > m && m > 1) {
+      if (p->npass >= SC_FFT_MAX_PASS) return -1;
+      p->radix[p->npass++] = m;
+      m = 1;
+    }
+  }
+  return 0;
+}
+
+static int pow2ceil(int x) {
+  int p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+// Threads per transform of length n on the runtime-plan path: a power of
+// two >= 32 with n <= MAXE*g.
+static int group_size(int n) {
+  int g = pow2ceil((n + SC_MAXE - 1) / SC_MAXE);
+  return std::max(32, g);
+}
+
+// Transform lengths with compile-time FFT plans (all benchmark sizes).
+#define SC_SPEC_ROW(X) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096) \
+  X(48) X(96) X(192) X(384) X(768) X(1536)
+#define SC_SPEC_COL(X) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) \
+  X(48) X(96) X(192) X(384) X(768) X(1536)
+#define SC_CASE_LABEL(n) case n:
+
+static bool spec_row(int n) {
+  switch (n) { SC_SPEC_ROW(SC_CASE_LABEL) return true; default: return false; }
+}
+static bool spec_col(int n) {
+  switch (n) { SC_SPEC_COL(SC_CASE_LABEL) return true; default: return false; }
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct Plan {
+  Geom g;
+  FftPlan pw, ph;
+  // hot row kernels (iteration, fix-up): compile-time plan when available
+  int row_g, row_nblk;
+  size_t row_smem;
+  // setup row kernels: runtime plan
+  int rowg_g;
+  size_t rowg_smem;
+  // hot column kernel (solve) and setup column kernels
+  int col_g, col_G, col_ntiles, col_NT, Hs;
+  size_t col_smem;
+  int colg_g, colg_NT;
+  size_t colg_smem;
+  int max_iter;
+  size_t off_U, off_F, off_Dh, off_Sh, off_twW, off_twH, off_part, off_st, off_it,
+      off_xi, off_ndone, total;
+};
+
+static int g_num_sms = 0;
+
+static int num_sms() {
+  if (g_num_sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 148;
+  }
+  return g_num_sms;
+}
+
+static int plan_geometry(int B, int M, int H, int W, Plan* pl) {
+  if (B < 1 || M < 1 || H < 1 || W < 1)
+    return set_status(SC_ERR_INVALID, "sizes must be positive (B=%d M=%d H=%d W=%d)", B, M, H, W);
+  if (W > SC_MAX_N || H > 2048)
+    return set_status(SC_ERR_UNSUPPORTED, "image %dx%d exceeds this build's limits (H<=2048, W<=%d)",
+                      H, W, SC_MAX_N);
+  Geom& g = pl->g;
+  g.B = B; g.M = M; g.H = H; g.W = W;
+  g.Wf = W / 2 + 1;
+  g.Wp = (g.Wf + 3) & ~3;
+  if (make_fft_plan(W, &pl->pw) || make_fft_plan(H, &pl->ph))
+    return set_status(SC_ERR_UNSUPPORTED, "cannot factor %d or %d", W, H);
+  pl->row_g = spec_row(W) ? ct_threads(W) : group_size(W);
+  const int S = SC_ROW_THREADS / pl->row_g;
+  const long rows = (long)M * H;
+  const long npairs = (rows + 1) / 2;
+  long want = (npairs + S - 1) / S;
+  long cap = std::max(1L, (long)num_sms() * 8 / B);
+  pl->row_nblk = (int)std::min(want, cap);
+  pl->row_smem = (size_t)S * W * sizeof(float2);
+  pl->rowg_g = group_size(W);
+  pl->rowg_smem = (size_t)(SC_ROW_THREADS / pl->rowg_g) * W * sizeof(float2);
+
+  pl->Hs = H + 1;
+  pl->col_ntiles = (g.Wf + SC_COL_TILE - 1) / SC_COL_TILE;
+  pl->col_g = spec_col(H) ? ct_threads(H) : group_size(H);
+  pl->col_NT = SC_COL_TILE * pl->col_g;
+  pl->col_G = std::min(8, M);
+  pl->col_smem = (size_t)SC_COL_TILE * pl->Hs * sizeof(float2) +
+                 (size_t)SC_COL_TILE * H * (sizeof(float2) + sizeof(float));
+  pl->colg_g = group_size(H);
+  pl->colg_NT = SC_COL_TILE * pl->colg_g;
+  pl->colg_smem = (size_t)SC_COL_TILE * pl->Hs * sizeof(float2);
+  return SC_OK;
+}
+
+static int plan_problem(const sc_problem* p, const sc_options* o, Plan* pl) {
+  int st = plan_geometry(p->B, p->M, p->H, p->W, pl);
+  if (st) return st;
+  if (p->Kr < 1 || p->Kc < 1 || p->Kr > p->H || p->Kc > p->W)
+    return set_status(SC_ERR_INVALID, "filter size %dx%d invalid for image %dx%d", p->Kr, p->Kc,
+                      p->H, p->W);
+  if (o->max_iter < 0) return set_status(SC_ERR_INVALID, "max_iter < 0");
+  pl->max_iter = o->max_iter;
+  const Geom& g = pl->g;
+  const size_t real_img = (size_t)g.M * g.H * g.W;
+  const size_t spec_img = (size_t)g.M * g.H * g.Wp;
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t r = off; off = align256(off + bytes); return r; };
+  pl->off_U = take(sizeof(float) * real_img * g.B);
+  pl->off_F = take(sizeof(float2) * spec_img * g.B);
+  pl->off_Dh = take(sizeof(float2) * spec_img);
+  pl->off_Sh = take(sizeof(float2) * (size_t)g.H * g.Wp * g.B);
+  pl->off_twW = take(sizeof(float2) * g.W);
+  pl->off_twH = take(sizeof(float2) * g.H);
+  pl->off_part = take(sizeof(double) * 5 * (size_t)pl->row_nblk * g.B);
+  pl->off_st = take(sizeof(ImgState) * g.B);
+  pl->off_it = take(o->record_itstat ? sizeof(double) * 5 * (size_t)std::max(1, o->max_iter) * g.B : 0);
+  pl->off_xi = take(sizeof(double) * g.B);
+  pl->off_ndone = take(sizeof(int));
+  pl->total = off;
+  return SC_OK;
+}
+
+extern "C" size_t sc_workspace_size(const sc_problem* p, const sc_options* o) {
+  Plan pl;
+  if (plan_problem(p, o, &pl)) return 0;
+  return pl.total;
+}
+
+// --------------------------------------------------------------- launchers --
+typedef void (*RowFn)(RowParams);
+typedef void (*ColFn)(ColParams);
+
+template <int MODE>
+static RowFn row_fn(int W) {
+#define SC_ROW_CASE(n) case n: return row_kernel<MODE, n>;
+  if constexpr (MODE == ROW_ITER || MODE == ROW_FIXUP) {
+    switch (W) { SC_SPEC_ROW(SC_ROW_CASE) default: break; }
+  }
+#undef SC_ROW_CASE
+  return row_kernel<MODE, 0>;
+}
+
+template <int MODE>
+static ColFn col_fn(int H) {
+#define SC_COL_CASE(n) case n: return col_kernel<MODE, n>;
+  if constexpr (MODE == COL_SOLVE) {
+    switch (H) { SC_SPEC_COL(SC_COL_CASE) default: break; }
+  }
+#undef SC_COL_CASE
+  return col_kernel<MODE, 0>;
+}
+
+// Opt every kernel instantiation into large dynamic shared memory once.
+static int prepare_fn(const void* fn, bool cluster) {
+  static std::vector<const void*> done;
+  for (const void* d : done)
+    if (d == fn) return SC_OK;
+  CU_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+  if (cluster) CU_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  done.push_back(fn);
+  return SC_OK;
+}
+
+// Hot row modes (iteration, fix-up) use the compile-time plan when the row
+// length has one; the setup modes always use the runtime plan.
+template <int MODE>
+static int launch_row(const Plan& pl, RowParams rp, int B, cudaStream_t s, int nblk = 0) {
+  const bool hot = MODE == ROW_ITER || MODE == ROW_FIXUP;
+  RowFn fn = row_fn<MODE>(rp.g.W);
+  int st = prepare_fn((const void*)fn, false);
+  if (st) return st;
+  rp.gsz = hot ? pl.row_g : pl.rowg_g;
+  rp.nblk = nblk > 0 ? nblk : pl.row_nblk;
+  dim3 grid(rp.nblk, B);
+  fn<<<grid, SC_ROW_THREADS, hot ? pl.row_smem : pl.rowg_smem, s>>>(rp);
+  CU_TRY(cudaGetLastError());
+  return SC_OK;
+}
+
+template <int MODE>
+static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s) {
+  cp.Hs = pl.Hs;
+  if (MODE == COL_SOLVE) {
+    ColFn fn = col_fn<COL_SOLVE>(cp.g.H);
+    int st = prepare_fn((const void*)fn, true);
+    if (st) return st;
+    cp.gsz = pl.col_g;
+    cp.G = pl.col_G;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(pl.col_G, pl.col_ntiles, B);
+    cfg.blockDim = dim3(pl.col_NT);
+    cfg.dynamicSmemBytes = pl.col_smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = pl.col_G;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CU_TRY(cudaLaunchKernelEx(&cfg, fn, cp));
+  } else {
+    // forward / inverse only: maps split 8 ways, no cluster
+    ColFn fn = col_fn<MODE>(cp.g.H);
+    int st = prepare_fn((const void*)fn, false);
+    if (st) return st;
+    cp.gsz = pl.colg_g;
+    cp.G = std::min(8, cp.g.M);
+    dim3 grid(cp.G, pl.col_ntiles, B);
+    fn<<<grid, pl.colg_NT, pl.colg_smem, s>>>(cp);
+    CU_TRY(cudaGetLastError());
+  }
+  return SC_OK;
+}
+
+static void carve(const Plan& pl, unsigned char* ws, float** U, float2** F, float2** Dh,
+                  float2** Sh, float2** twW, float2** twH, double** part, ImgState** st,
+                  double** it, double** xi, int** ndone) {
+  *U = (float*)(ws + pl.off_U);
+  *F = (float2*)(ws + pl.off_F);
+  *Dh = (float2*)(ws + pl.off_Dh);
+  *Sh = (float2*)(ws + pl.off_Sh);
+  *twW = (float2*)(ws + pl.off_twW);
+  *twH = (float2*)(ws + pl.off_twH);
+  *part = (double*)(ws + pl.off_part);
+  *st = (ImgState*)(ws + pl.off_st);
+  *it = (double*)(ws + pl.off_it);
+  *xi = (double*)(ws + pl.off_xi);
+  *ndone = (int*)(ws + pl.off_ndone);
+}
+
+__global__ void xi_kernel(double* xi, const float* lam, int B, float target, int std_res) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  double v;
+  if (target > 0.f) v = target;
+  else if (std_res) v = 1.0;
+  else {
+    const double l = lam[b];
+    v = l > 0.0 ? 1.0 + pow(18.3, log10(l) + 1.0) : 1.0;
+  }
+  xi[b] = v;
+}
+
+extern "C" void sc_options_from_algopt(const AlgOpt* a, sc_options* o) {
+  memset(o, 0, sizeof(*o));
+  o->max_iter = a->MaxMainIter;
+  o->relax = a->RelaxParam;
+  o->abs_tol = a->AbsStopTol;
+  o->rel_tol = a->RelStopTol;
+  o->auto_rho = a->AutoRho;
+  o->auto_rho_period = a->AutoRhoPeriod > 0 ? a->AutoRhoPeriod : 1;
+  o->rho_scaling = a->RhoScaling;
+  o->rsdl_ratio = a->RhoRsdlRatio;
+  o->rsdl_target = a->RhoRsdlTarget;
+  o->auto_scaling = a->AutoRhoScaling;
+  o->std_residuals = a->StdResiduals;
+  o->record_itstat = a->Verbose ? 1 : 0;
+  o->check_every = 32;
+}
+
+extern "C" int sc_cbpdn_solve(const sc_problem* p, const sc_options* o, void* workspace,
+                              size_t workspace_bytes, sc_result* res, void* stream) {
+  set_status(SC_OK, nullptr);
+  if (!p || !o) return set_status(SC_ERR_INVALID, "null problem or options");
+  Plan pl;
+  int st = plan_problem(p, o, &pl);
+  if (st) return st;
+  if (!workspace || workspace_bytes < pl.total)
+    return set_status(SC_ERR_WORKSPACE, "workspace of %zu bytes needed", pl.total);
+  if (((uintptr_t)workspace) & 255) return set_status(SC_ERR_WORKSPACE, "workspace not 256-byte aligned");
+  if (!p->D || !p->S || !p->lmbda || !p->rho0 || !p->Y)
+    return set_status(SC_ERR_INVALID, "null device pointer");
+  if (p->grd && !p->wgrd) return set_status(SC_ERR_INVALID, "grd problem without GradWeight");
+  if (p->l1_kind != SC_L1_SCALAR && !p->l1w) return set_status(SC_ERR_INVALID, "missing L1Weight");
+  cudaStream_t s = (cudaStream_t)stream;
+  const Geom& g = pl.g;
+
+  float* U; float2 *F, *Dh, *Sh, *twW, *twH; double *part, *it, *xi; ImgState* sts; int* ndone;
+  carve(pl, (unsigned char*)workspace, &U, &F, &Dh, &Sh, &twW, &twH, &part, &sts, &it, &xi, &ndone);
+
+  twiddle_kernel<<<(g.W + 255) / 256, 256, 0, s>>>(twW, g.W);
+  twiddle_kernel<<<(g.H + 255) / 256, 256, 0, s>>>(twH, g.H);
+  CU_TRY(cudaGetLastError());
+
+  // Dictionary spectrum: rfft2 of the zero-padded filters (cuda_Pad_Dict +
+  // R2C, cbpdn.cu:277-289), computed without materialising the padding.
+  {
+    RowParams rp = {};
+    rp.g = g; rp.g.B = 1;
+    rp.pw = pl.pw; rp.twW = twW; rp.F = Dh; rp.D = p->D; rp.Kr = p->Kr; rp.Kc = p->Kc;
+    if ((st = launch_row<ROW_FWD_DICT>(pl, rp, 1, s))) return st;
+    ColParams cp = {};
+    cp.g = g; cp.g.B = 1; cp.ph = pl.ph; cp.twH = twH; cp.twW = twW; cp.F = Dh;
+    if ((st = launch_col<COL_FWD>(pl, cp, 1, s))) return st;
+  }
+  // Signal spectra (B images, one map each).
+  {
+    RowParams rp = {};
+    rp.g = g; rp.g.M = 1;
+    rp.pw = pl.pw; rp.twW = twW; rp.F = Sh; rp.src = p->S;
+    const long npairs = ((long)g.H + 1) / 2;
+    const int S = SC_ROW_THREADS / pl.rowg_g;
+    const int nb = (int)std::max(1L, std::min((npairs + S - 1) / S, (long)num_sms()));
+    if ((st = launch_row<ROW_FWD_REAL>(pl, rp, g.B, s, nb))) return st;
+    ColParams cp = {};
+    cp.g = g; cp.g.M = 1; cp.ph = pl.ph; cp.twH = twH; cp.twW = twW; cp.F = Sh;
+    if ((st = launch_col<COL_FWD>(pl, cp, g.B, s))) return st;
+  }
+  const size_t real_all = (size_t)g.B * g.M * g.H * g.W;
+  CU_TRY(cudaMemsetAsync(p->Y, 0, sizeof(float) * real_all, s));
+  CU_TRY(cudaMemsetAsync(U, 0, sizeof(float) * real_all, s));
+  CU_TRY(cudaMemsetAsync(F, 0, sizeof(float2) * (size_t)g.B * g.M * g.H * g.Wp, s));
+  init_state_kernel<<<(g.B + 127) / 128, 128, 0, s>>>(sts, p->rho0, g.B, ndone);
+  xi_kernel<<<(g.B + 127) / 128, 128, 0, s>>>(xi, p->lmbda, g.B, o->rsdl_target, o->std_residuals);
+  CU_TRY(cudaGetLastError());
+
+  RowParams rp = {};
+  rp.g = g; rp.pw = pl.pw; rp.twW = twW; rp.F = F; rp.Y = p->Y; rp.U = U;
+  rp.lam = p->lmbda; rp.l1_kind = p->l1_kind; rp.l1_scalar = p->l1_scalar; rp.l1w = p->l1w;
+  rp.mask = p->mask; rp.relax = o->relax; rp.invN = (float)(1.0 / ((double)g.H * g.W));
+  rp.partials = part; rp.st = sts;
+  ColParams cp = {};
+  cp.g = g; cp.ph = pl.ph; cp.twH = twH; cp.twW = twW; cp.F = F; cp.Dh = Dh; cp.Sh = Sh;
+  cp.grd = p->grd; cp.mu = p->mu; cp.wgrd = p->wgrd; cp.st = sts;
+  FinParams fp = {};
+  fp.max_iter = o->max_iter;
+  fp.auto_rho = o->auto_rho; fp.period = std::max(1, o->auto_rho_period);
+  fp.auto_scaling = o->auto_scaling; fp.std_residuals = o->std_residuals;
+  fp.rho_scaling = o->rho_scaling; fp.rsdl_ratio = o->rsdl_ratio;
+  fp.abs_tol = o->abs_tol; fp.rel_tol = o->rel_tol;
+  fp.nelem = (double)g.M * g.H * g.W;
+  fp.xi = xi; fp.itstat = o->record_itstat ? it : nullptr; fp.ndone = ndone;
+
+  int done_iters = 0;
+  while (done_iters < o->max_iter) {
+    int chunk = o->max_iter - done_iters;
+    if (o->check_every > 0) chunk = std::min(chunk, o->check_every);
+    for (int i = 0; i < chunk; ++i) {
+      if ((st = launch_col<COL_SOLVE>(pl, cp, g.B, s))) return st;
+      if ((st = launch_row<ROW_ITER>(pl, rp, g.B, s))) return st;
+      finalize_kernel<<<g.B, 256, 0, s>>>(part, pl.row_nblk, sts, fp);
+      CU_TRY(cudaGetLastError());
+      if (o->auto_rho) {
+        if ((st = launch_row<ROW_FIXUP>(pl, rp, g.B, s))) return st;
+      }
+    }
+    done_iters += chunk;
+    if (done_iters < o->max_iter) {
+      int nd = 0;
+      CU_TRY(cudaMemcpyAsync(&nd, ndone, sizeof(int), cudaMemcpyDeviceToHost, s));
+      CU_TRY(cudaStreamSynchronize(s));
+      if (nd >= g.B) break;
+    }
+  }
+  if (res) {
+    ImgState h0;
+    CU_TRY(cudaMemcpyAsync(&h0, sts, sizeof(ImgState), cudaMemcpyDeviceToHost, s));
+    CU_TRY(cudaStreamSynchronize(s));
+    res->iterations = h0.k;
+    res->rho = h0.rho;
+    res->r = h0.r;
+    res->s = h0.s;
+    if (g.B > 1) {
+      std::vector<ImgState> hs(g.B);
+      CU_TRY(cudaMemcpy(hs.data(), sts, sizeof(ImgState) * g.B, cudaMemcpyDeviceToHost));
+      for (auto& x : hs) res->iterations = std::max(res->iterations, x.k);
+      for (auto& x : hs)
+        if (x.status) return set_status(x.status, "non-finite residual");
+    }
+    if (h0.status) return set_status(h0.status, "non-finite residual");
+  }
+  return SC_OK;
+}
+
+extern "C" int sc_read_state(const sc_problem* p, const sc_options* o, const void* workspace,
+                             int* iterations, double* rho, double* itstat, void* stream) {
+  Plan pl;
+  int st = plan_problem(p, o, &pl);
+  if (st) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  const unsigned char* ws = (const unsigned char*)workspace;
+  std::vector<ImgState> hs(pl.g.B);
+  CU_TRY(cudaMemcpyAsync(hs.data(), ws + pl.off_st, sizeof(ImgState) * pl.g.B,
+                         cudaMemcpyDeviceToHost, s));
+  if (itstat && o->record_itstat)
+    CU_TRY(cudaMemcpyAsync(itstat, ws + pl.off_it,
+                           sizeof(double) * 5 * (size_t)std::max(1, o->max_iter) * pl.g.B,
+                           cudaMemcpyDeviceToHost, s));
+  CU_TRY(cudaStreamSynchronize(s));
+  for (int b = 0; b < pl.g.B; ++b) {
+    if (iterations) iterations[b] = hs[b].k;
+    if (rho) rho[b] = hs[b].rho;
+  }
+  return SC_OK;
+}
+
+// --------------------------------------------------------------- rfft2 tools --
+extern "C" int sc_rfft2(const float* x, void* xf, int count, int H, int W, void* stream) {
+  set_status(SC_OK, nullptr);
+  Plan pl;
+  int st = plan_geometry(count, 1, H, W, &pl);
+  if (st) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  pl.g.Wp = pl.g.Wf;  // dense numpy layout
+  float2* tw = nullptr;
+  CU_TRY(cudaMallocAsync((void**)&tw, sizeof(float2) * (W + H), s));
+  twiddle_kernel<<<(W + 255) / 256, 256, 0, s>>>(tw, W);
+  twiddle_kernel<<<(H + 255) / 256, 256, 0, s>>>(tw + W, H);
+  RowParams rp = {};
+  rp.g = pl.g; rp.pw = pl.pw; rp.twW = tw; rp.F = (float2*)xf; rp.src = x;
+  if ((st = launch_row<ROW_FWD_REAL>(pl, rp, count, s))) return st;
+  ColParams cp = {};
+  cp.g = pl.g; cp.ph = pl.ph; cp.twH = tw + W; cp.twW = tw; cp.F = (float2*)xf;
+  if ((st = launch_col<COL_FWD>(pl, cp, count, s))) return st;
+  CU_TRY(cudaFreeAsync(tw, s));
+  return SC_OK;
+}
+
+extern "C" int sc_irfft2(const void* xf, float* x, int count, int H, int W, void* stream) {
+  set_status(SC_OK, nullptr);
+  Plan pl;
+  int st = plan_geometry(count, 1, H, W, &pl);
+  if (st) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  pl.g.Wp = pl.g.Wf;
+  float2* tw = nullptr;
+  float2* tmp = nullptr;
+  const size_t nspec = (size_t)count * H * pl.g.Wf;
+  CU_TRY(cudaMallocAsync((void**)&tw, sizeof(float2) * (W + H), s));
+  CU_TRY(cudaMallocAsync((void**)&tmp, sizeof(float2) * nspec, s));
+  CU_TRY(cudaMemcpyAsync(tmp, xf, sizeof(float2) * nspec, cudaMemcpyDeviceToDevice, s));
+  twiddle_kernel<<<(W + 255) / 256, 256, 0, s>>>(tw, W);
+  twiddle_kernel<<<(H + 255) / 256, 256, 0, s>>>(tw + W, H);
+  ColParams cp = {};
+  cp.g = pl.g; cp.ph = pl.ph; cp.twH = tw + W; cp.twW = tw; cp.F = tmp;
+  if ((st = launch_col<COL_INV>(pl, cp, count, s))) return st;
+  RowParams rp = {};
+  rp.g = pl.g; rp.pw = pl.pw; rp.twW = tw; rp.F = tmp; rp.dst = x;
+  rp.invN = (float)(1.0 / ((double)H * W));
+  if ((st = launch_row<ROW_INV_REAL>(pl, rp, count, s))) return st;
+  CU_TRY(cudaFreeAsync(tmp, s));
+  CU_TRY(cudaFreeAsync(tw, s));
+  return SC_OK;
+}

@@ -1,0 +1,118 @@
+"""Parity of the CUDA solvers with the compiled reference's outputs (golden
+fixtures) and with the FP64 oracle."""
+
+import os
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+import cases
+import sporco_cuda.cbpdn as cb
+from oracle import cbpdn_oracle as O
+
+GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_outputs.npz"))
+
+# Relative error bound of the FP32 GPU path against the FP64 oracle.
+REL_TOL = 1e-4
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("i", range(1, cases.NCASES + 1))
+def test_numpy_path_matches_reference_and_oracle(i):
+    c = cases.make_case(i)
+    X = cases.run(cb, c)
+    Xo = cases.run(O, c)
+    assert X.dtype == np.float32 and X.shape == Xo.shape
+    # same bound as the reference's own tests (test_cbpdn.py:32,90)
+    if i != 19:  # case 19: the reference's U rescale differs (see test_oracle_golden)
+        assert O.mse(X, GOLD["case%02d" % i]) < c["tol"]
+    tol = 5e-4 if i in (3, 15) else REL_TOL  # case 3: an unregularised map
+    assert _rel(X, Xo) < tol
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("i", [1, 4, 6, 11, 14, 16, 19])
+def test_torch_path_matches_numpy_path(i):
+    c = cases.make_case(i)
+    X = cases.run(cb, c)
+    ct = dict(c)
+    ct["D"] = torch.as_tensor(c["D"], device="cuda")
+    ct["S"] = torch.as_tensor(c["S"], device="cuda")
+    Xt = cases.run(cb, ct).cpu().numpy()
+    assert _rel(Xt, X.astype(np.float64)) < 1e-6
+
+
+@pytest.mark.gpu
+def test_deterministic_bitwise():
+    c = cases.make_case(16)
+    a = cases.run(cb, c)
+    b = cases.run(cb, c)
+    assert np.array_equal(a, b)
+
+
+def _synth(H, W, M, K, density, seed):
+    rng = np.random.default_rng(seed)
+    D = rng.standard_normal((K, K, M))
+    D /= np.sqrt(np.sum(D * D, axis=(0, 1), keepdims=True))
+    X0 = (rng.random((H, W, M)) < density) * rng.standard_normal((H, W, M))
+    Df = np.fft.rfft2(D, s=(H, W), axes=(0, 1))
+    s = np.fft.irfft2(np.sum(Df * np.fft.rfft2(X0, axes=(0, 1)), axis=2), s=(H, W))
+    s = s + 0.01 * rng.standard_normal((H, W))
+    return D.astype(np.float32), (s - s.mean()).astype(np.float32)
+
+
+@pytest.mark.gpu
+def test_benchmark_shape_256_fixed_rho():
+    """256x256, 64 filters 8x8, lambda 0.05, fixed rho: the 200-iteration
+    benchmark problem cut to 40 iterations for the FP64 oracle's sake."""
+    D, S = _synth(256, 256, 64, 8, 0.01, 12345)
+    lam = 0.05
+    opt = {"MaxMainIter": 40, "RelStopTol": 0.0, "RelaxParam": 1.8,
+           "rho": float(np.float32(50 * np.float32(lam) + 1)), "AutoRho": {"Enabled": False}}
+    X = cb.cbpdn(D, S, lam, opt)
+    Xo = O.cbpdn(D, S, lam, opt)
+    assert _rel(X, Xo) < REL_TOL
+    Dm = np.moveaxis(D, 2, 0).astype(np.float64)
+    J = O.objective(Dm, S, np.moveaxis(X.astype(np.float64), 2, 0), np.float32(lam))
+    Jo = O.objective(Dm, S, np.moveaxis(Xo, 2, 0), np.float32(lam))
+    assert abs(J - Jo) / Jo < 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", ["cbpdngrd", "cbpdnmsk"])
+def test_autorho_trajectory_512(variant):
+    """512x512 shapes with adaptive rho: the GPU rho trajectory and result
+    follow the FP64 oracle (the oracle run is cut to 30 iterations)."""
+    D, S = _synth(128, 128, 16, 12, 0.005, 7)
+    lam, mu = 0.05, 0.1
+    opt = {"MaxMainIter": 30, "RelStopTol": 0.0, "AutoRho": {"Enabled": True}}
+    if variant == "cbpdngrd":
+        X = cb.cbpdngrd(D, S, lam, mu, opt)
+        Xo = O.cbpdngrd(D, S, lam, mu, opt)
+    else:
+        W = (np.random.default_rng(3).random(S.shape) < 0.7).astype(np.float32)
+        X = cb.cbpdnmsk(D, S * W, W, lam, opt)
+        Xo = O.cbpdnmsk(D, S * W, W, lam, opt)
+    assert _rel(X, Xo) < REL_TOL
+
+
+@pytest.mark.gpu
+def test_early_stopping_iteration_count():
+    c = cases.make_case(1)
+    opt = dict(c["opt"])
+    opt["MaxMainIter"] = 500
+    opt["RelStopTol"] = 1e-3
+    D = torch.as_tensor(c["D"], device="cuda")
+    S = torch.as_tensor(c["S"], device="cuda")
+    ds = cb.prepare_device(D.permute(2, 0, 1).contiguous(), S[None], c["lmbda"], opt,
+                           check_every=8)
+    ds.run()
+    it = ds.state()["iterations"][0]
+    _, info = O.cbpdn(c["D"], c["S"], c["lmbda"], opt, return_info=True)
+    assert it == info["iterations"]

@@ -243,7 +243,13 @@ static int prepare_fn(const void* fn, bool cluster) {
   static std::vector<const void*> done;
   for (const void* d : done)
     if (d == fn) return SC_OK;
-  CU_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+  int dev = 0, optin = 0;
+  CU_TRY(cudaGetDevice(&dev));
+  CU_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa;
+  CU_TRY(cudaFuncGetAttributes(&fa, fn));
+  CU_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              optin - (int)fa.sharedSizeBytes));
   if (cluster) CU_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   done.push_back(fn);
   return SC_OK;
@@ -350,6 +356,7 @@ extern "C" void sc_options_from_algopt(const AlgOpt* a, sc_options* o) {
 extern "C" int sc_cbpdn_solve(const sc_problem* p, const sc_options* o, void* workspace,
                               size_t workspace_bytes, sc_result* res, void* stream) {
   set_status(SC_OK, nullptr);
+  (void)cudaGetLastError();  // do not report an earlier call's error as ours
   if (!p || !o) return set_status(SC_ERR_INVALID, "null problem or options");
   Plan pl;
   int st = plan_problem(p, o, &pl);
@@ -486,6 +493,7 @@ extern "C" int sc_read_state(const sc_problem* p, const sc_options* o, const voi
 // --------------------------------------------------------------- rfft2 tools --
 extern "C" int sc_rfft2(const float* x, void* xf, int count, int H, int W, void* stream) {
   set_status(SC_OK, nullptr);
+  (void)cudaGetLastError();
   Plan pl;
   int st = plan_geometry(count, 1, H, W, &pl);
   if (st) return st;
@@ -507,6 +515,7 @@ extern "C" int sc_rfft2(const float* x, void* xf, int count, int H, int W, void*
 
 extern "C" int sc_irfft2(const void* xf, float* x, int count, int H, int W, void* stream) {
   set_status(SC_OK, nullptr);
+  (void)cudaGetLastError();
   Plan pl;
   int st = plan_geometry(count, 1, H, W, &pl);
   if (st) return st;

@@ -1,0 +1,434 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 CBPDN ADMM solvers (ADMM iterations per second).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config C] [--impl ours|reference]
+
+Workload (default --config 1): one 512x512 float32 image, 100 unit-norm 12x12
+Gaussian filters, S synthesised from Bernoulli(0.005) x N(0,1) sparse maps plus
+N(0, 0.01^2) noise and mean-subtracted (seed 12346); a step is one cbpdngrd solve
+(lambda 0.05, mu 0.1) plus one cbpdnmsk solve (Bernoulli(0.7) mask, 101 maps
+with the AMS impulse), AutoRho on, 500 ADMM iterations each (no early stop).
+Configs 0 (256x256, M=64, 200 iterations, fixed rho) and 4 (2048x2048,
+M=256, 100 iterations, AutoRho) are selectable.  Data are synthetic.
+
+Printed JSON line (rank 0): ``value`` = ADMM iterations per second with inputs
+resident in device memory, summed over ranks (each rank runs an independent
+replica: the path has no data-path collective); ``e2e`` = the same metric
+through the reference-facing API (numpy host buffers in and out, host<->device
+copies inside the timed region); ``roofline`` = algorithmic HBM bytes of one
+ADMM iteration (4R + 6C + 2C_D, R = 4 M H W, C = C_D = 8 M H (W/2+1)) over the
+measured device time of one iteration (CUDA events around every kernel of the
+timed solves), against the measured HBM copy bandwidth; ``cpu_baseline`` = the
+FP64 CPU restatement of the algorithm timed on this host on a bounded sample.
+
+``--impl reference`` times the reference algorithm's CPU implementation (the
+FP64 restatement; the reference ships no CPU solver of its own) on this host's
+cores, on the same workload, one bounded sample per step.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "sporco-cuda_b200"))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = ("ADMM iters/s & HBM GB/s (plain vs batched vs fwd+adjoint), "
+          "rel err ≤1e-4 vs FP64")
+
+CONFIGS = {
+    0: dict(workload="cbpdn 256x256 M=64 8x8, 200 iterations, fixed rho",
+            H=256, W=256, M=64, K=8, density=0.01, lmbda=0.05, mu=0.0,
+            variants=["cbpdn"], iters=200, autorho=False, mask_p=None),
+    1: dict(workload="cbpdngrd + cbpdnmsk 512x512 M=100 12x12, 500 iterations, AutoRho",
+            H=512, W=512, M=100, K=12, density=0.005, lmbda=0.05, mu=0.1,
+            variants=["cbpdngrd", "cbpdnmsk"], iters=500, autorho=True, mask_p=0.7),
+    4: dict(workload="cbpdn 2048x2048 M=256 16x16, 100 iterations, AutoRho",
+            H=2048, W=2048, M=256, K=16, density=0.01, lmbda=0.02, mu=0.0,
+            variants=["cbpdn"], iters=100, autorho=True, mask_p=None),
+}
+
+
+# ---------------------------------------------------------------- helpers --
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def opt_for(cfg, variant):
+    lam = np.float32(cfg["lmbda"])
+    opt = {"Verbose": False, "MaxMainIter": cfg["iters"], "RelStopTol": 0.0, "AbsStopTol": 0.0,
+           "RelaxParam": 1.8, "L1Weight": 1.0, "GradWeight": 1.0,
+           "AutoRho": {"Enabled": cfg["autorho"], "Period": 1, "Scaling": 1000.0,
+                       "RsdlRatio": 1.2, "RsdlTarget": None, "AutoScaling": True,
+                       "StdResiduals": False}}
+    opt["rho"] = None if cfg["autorho"] else float(np.float32(50 * lam + 1))
+    return opt
+
+
+def algorithmic_bytes(H, W, M):
+    """Per-iteration HBM bytes of the byte model (two-pass 2-D FFT)."""
+    R = 4.0 * M * H * W
+    Cs = 8.0 * M * H * (W // 2 + 1)
+    return 4 * R + 6 * Cs + 2 * Cs
+
+
+def synth(cfg, seed, device):
+    """Unit-norm Gaussian filters, sparse maps, S = sum_m d_m * x_m + noise,
+    mean-subtracted.  Spectral products use this package's own FFT."""
+    import torch
+    from sporco_cuda import _lib
+    H, W, M, K = cfg["H"], cfg["W"], cfg["M"], cfg["K"]
+    g = torch.Generator(device=device).manual_seed(seed)
+    D = torch.randn((M, K, K), generator=g, device=device)
+    D /= torch.sqrt(torch.sum(D * D, dim=(1, 2), keepdim=True))
+    Dp = torch.zeros((M, H, W), device=device)
+    Dp[:, :K, :K] = D
+    X0 = (torch.rand((M, H, W), generator=g, device=device) < cfg["density"]).float() * \
+        torch.randn((M, H, W), generator=g, device=device)
+    Wf = W // 2 + 1
+    s = torch.cuda.current_stream().cuda_stream
+    Df = torch.empty((M, H, Wf), dtype=torch.complex64, device=device)
+    Xf = torch.empty((M, H, Wf), dtype=torch.complex64, device=device)
+    _lib.check(_lib.sc_rfft2(C.c_void_p(Dp.data_ptr()), C.c_void_p(Df.data_ptr()), M, H, W,
+                             C.c_void_p(s)))
+    _lib.check(_lib.sc_rfft2(C.c_void_p(X0.data_ptr()), C.c_void_p(Xf.data_ptr()), M, H, W,
+                             C.c_void_p(s)))
+    Sf = torch.sum(Df * Xf, dim=0).contiguous()
+    S = torch.empty((1, H, W), device=device)
+    _lib.check(_lib.sc_irfft2(C.c_void_p(Sf.data_ptr()), C.c_void_p(S.data_ptr()), 1, H, W,
+                              C.c_void_p(s)))
+    S = S[0] + 0.01 * torch.randn((H, W), generator=g, device=device)
+    S = S - S.mean()
+    mask = None
+    if cfg["mask_p"] is not None:
+        mask = (torch.rand((H, W), generator=g, device=device) < cfg["mask_p"]).float()
+    del Dp, X0, Df, Xf, Sf
+    return D.contiguous(), S.contiguous(), mask
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_sample(cfg, D, S, mask, budget_s=15.0):
+    """FP64 CPU restatement on this host: iterations/s on a bounded sample of
+    the workload (the first n ADMM iterations of each variant)."""
+    from oracle import cbpdn_oracle as O
+    Dn = np.ascontiguousarray(np.moveaxis(D, 0, 2))
+    lam = cfg["lmbda"]
+
+    def run(variant, n):
+        opt = opt_for(cfg, variant)
+        opt["MaxMainIter"] = n
+        if variant == "cbpdn":
+            O.cbpdn(Dn, S, lam, opt)
+        elif variant == "cbpdngrd":
+            O.cbpdngrd(Dn, S, lam, cfg["mu"], opt)
+        elif variant == "cbpdnmsk":
+            O.cbpdnmsk(Dn, S * mask, mask, lam, opt)
+    t0 = time.perf_counter()
+    for v in cfg["variants"]:
+        run(v, 1)
+    per = (time.perf_counter() - t0) / len(cfg["variants"])
+    n = max(1, int(budget_s / max(per, 1e-6) / len(cfg["variants"])))
+    n = min(n, cfg["iters"])
+    t0 = time.perf_counter()
+    for v in cfg["variants"]:
+        run(v, n)
+    dt = time.perf_counter() - t0
+    total = n * len(cfg["variants"])
+    return {"value": total / dt, "unit": "iter/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": "%s: first %d ADMM iterations of each of %s (FP64 numpy/scipy, "
+                      "scipy.fft workers=%d)" % (cfg["workload"], n, "+".join(cfg["variants"]),
+                                                 os.cpu_count())}
+
+
+# ------------------------------------------------------------------ arms --
+
+def run_ours(args, cfg, rank, world, local_rank):
+    import torch
+    import sporco_cuda.cbpdn as cb
+    from sporco_cuda import _lib
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    D, S, mask = synth(cfg, 12345 + args.config, dev)
+    lam = cfg["lmbda"]
+    # device-resident solves
+    solves = []
+    for v in cfg["variants"]:
+        opt = opt_for(cfg, v)
+        if v == "cbpdnmsk":
+            M1 = cfg["M"] + 1
+            Di = torch.zeros((M1, cfg["K"], cfg["K"]), device=dev)
+            Di[0, 0, 0] = 1.0
+            Di[1:] = D
+            l1 = np.ones(M1, np.float32)
+            l1[0] = 0.0
+            ds = cb.prepare_device(Di, (S * mask)[None], lam, opt, l1=l1,
+                                   mask=mask.to(torch.int32)[None], profile=True)
+        else:
+            ds = cb.prepare_device(D, S[None], lam, opt, mu=cfg["mu"],
+                                   grd=(v == "cbpdngrd"), profile=True)
+        solves.append((v, ds))
+
+    def step():
+        prof = {}
+        for v, ds in solves:
+            ds.run()
+            for k, (ms, n) in ds.profile().items():
+                a = prof.setdefault(k, [0.0, 0])
+                a[0] += ms
+                a[1] += n
+        return prof
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    n_launch0 = _lib.sc_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    prof_tot = {}
+    with ClockSampler(local_rank) as clk:
+        ev0.record()
+        for _ in range(args.steps):
+            p = step()
+            for k, (ms, n) in p.items():
+                a = prof_tot.setdefault(k, [0.0, 0])
+                a[0] += ms
+                a[1] += n
+        ev1.record()
+        barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = _lib.sc_launch_count() - n_launch0
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    iters_per_step = cfg["iters"] * len(cfg["variants"])
+    value = world * iters_per_step * args.steps / (ms / 1e3)
+
+    # end-to-end through the reference-facing API (numpy host buffers)
+    Dn = np.ascontiguousarray(D.permute(1, 2, 0).cpu().numpy())
+    Sn = S.cpu().numpy()
+    Wn = mask.cpu().numpy() if mask is not None else None
+
+    def e2e_step():
+        for v in cfg["variants"]:
+            opt = opt_for(cfg, v)
+            if v == "cbpdn":
+                cb.cbpdn(Dn, Sn, lam, opt)
+            elif v == "cbpdngrd":
+                cb.cbpdngrd(Dn, Sn, lam, cfg["mu"], opt)
+            else:
+                cb.cbpdnmsk(Dn, Sn * Wn, Wn, lam, opt)
+    e2e_step()
+    barrier()
+    e_steps = max(1, min(args.steps, 3))
+    t0 = time.perf_counter()
+    for _ in range(e_steps):
+        e2e_step()
+    barrier()
+    e_ms = (time.perf_counter() - t0) * 1e3
+    if world > 1:
+        t = torch.tensor([e_ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e_ms = float(t.item())
+    e_value = world * iters_per_step * e_steps / (e_ms / 1e3)
+    h2d = d2h = 0
+    for v in cfg["variants"]:
+        M = cfg["M"] + (1 if v == "cbpdnmsk" else 0)
+        h2d += 4 * M * cfg["K"] ** 2 + 4 * cfg["H"] * cfg["W"] + 8  # D, S, scalars
+        if v == "cbpdnmsk":
+            h2d += 4 * cfg["H"] * cfg["W"] + 4 * M  # mask, l1 weights
+        if v == "cbpdngrd":
+            h2d += 4 * M
+        d2h += 4 * M * cfg["H"] * cfg["W"]
+
+    # roofline of one ADMM iteration (the timed solves' kernels)
+    peak, peak_kind = measured_peaks()
+    it_ms = sum(a[0] for a in prof_tot.values())
+    n_it = prof_tot.get("col_kernel", [0, 1])[1]
+    bytes_it = 0.0
+    for v in cfg["variants"]:
+        M = cfg["M"] + (1 if v == "cbpdnmsk" else 0)
+        bytes_it += algorithmic_bytes(cfg["H"], cfg["W"], M) * cfg["iters"] * args.steps
+    achieved = bytes_it / (it_ms / 1e3) / 1e9 if it_ms > 0 else None
+    kern = {k: {"ms_per_launch": a[0] / max(1, a[1]), "launches": a[1],
+                "share": a[0] / it_ms if it_ms else None} for k, a in prof_tot.items()}
+    out = None
+    if rank == 0:
+        cpu = cpu_sample(cfg, D.cpu().numpy(), Sn, Wn) if world == 1 and not args.no_cpu else None
+        out = {
+            "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "H": cfg["H"], "W": cfg["W"],
+                       "M": cfg["M"], "K": cfg["K"], "iterations_per_solve": cfg["iters"],
+                       "solves_per_step": len(cfg["variants"]),
+                       "parallelism": "replicas%d" % world if world > 1 else "single",
+                       "l2": "working set larger than L2 (no flush)" if
+                       algorithmic_bytes(cfg["H"], cfg["W"], cfg["M"]) > 126e6 else
+                       "working set fits in L2"},
+            "e2e": {"value": e_value, "unit": "iter/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "kernel": "ADMM iteration (col_kernel + row_kernel + "
+                         "finalize_kernel + fixup_kernel)",
+                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                         "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                         "traffic": None,
+                         "algorithmic_bytes_per_iteration":
+                             algorithmic_bytes(cfg["H"], cfg["W"], cfg["M"]),
+                         "iteration_ms": it_ms / max(1, n_it), "kernels": kern},
+            "cpu_baseline": cpu,
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+    return out
+
+
+def run_reference(args, cfg, rank):
+    """The reference algorithm on the host cores (FP64 restatement)."""
+    if rank != 0:
+        return None
+    import torch  # noqa: F401  (device only for synthesis when available)
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    if dev == "cuda":
+        D, S, mask = synth(cfg, 12345 + args.config, torch.device("cuda", 0))
+        D, S = D.cpu().numpy(), S.cpu().numpy()
+        mask = mask.cpu().numpy() if mask is not None else None
+    else:
+        rng = np.random.default_rng(12345 + args.config)
+        D = rng.standard_normal((cfg["M"], cfg["K"], cfg["K"])).astype(np.float32)
+        S = rng.standard_normal((cfg["H"], cfg["W"])).astype(np.float32)
+        mask = (rng.random((cfg["H"], cfg["W"])) < (cfg["mask_p"] or 1)).astype(np.float32)
+    per_step = []
+    budget = float(os.environ.get("SC_REF_STEP_SECONDS", "8"))
+    for i in range(args.warmup + args.steps):
+        r = cpu_sample(cfg, D, S, mask, budget_s=budget)
+        if i >= args.warmup:
+            per_step.append(r)
+    value = statistics.mean(r["value"] for r in per_step)
+    return {
+        "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": cfg["workload"], "H": cfg["H"], "W": cfg["W"], "M": cfg["M"],
+                   "K": cfg["K"]},
+        "cpu_baseline": {"value": value, "unit": "iter/s", "cores": os.cpu_count(),
+                         "kind": "port", "sample": per_step[-1]["sample"]},
+        "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", type=int, default=1, choices=sorted(CONFIGS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        out = run_reference(args, cfg, rank)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    out = run_ours(args, cfg, rank, world, local_rank)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -123,6 +123,7 @@ typedef struct sc_options {
   int std_residuals;    /* AutoRho.StdResiduals */
   int record_itstat;    /* keep per-iteration r, s, rho on the device */
   int check_every;      /* host polls the stop flag every this many iterations (0: never) */
+  int profile;          /* time every iteration kernel with CUDA events (sc_last_profile) */
 } sc_options;
 
 /* L1 weight layouts. */
@@ -172,6 +173,17 @@ int sc_read_state(const sc_problem *p, const sc_options *o, const void *workspac
 int sc_rfft2(const float *x, void *xf, int count, int H, int W, void *stream);
 /* Inverse of sc_rfft2 (numpy irfft2, normalised by 1/(H W)). */
 int sc_irfft2(const void *xf, float *x, int count, int H, int W, void *stream);
+
+/* Per-kernel device time of the last solve run with options.profile set:
+ * index 0 column pass, 1 row pass, 2 finalize, 3 rho fix-up. */
+typedef struct sc_profile {
+  double ms[4];
+  int count[4];
+} sc_profile;
+int sc_last_profile(sc_profile *out);
+
+/* Number of kernels this library has launched since it was loaded. */
+unsigned long long sc_launch_count(void);
 
 /* Last status / message recorded on the calling thread. */
 int sc_last_status(void);

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -52,6 +53,16 @@ static int set_status(int st, const char* fmt, ...) {
   } while (0)
 
 int sc_set_status_external(int st, const char* msg) { return set_status(st, msg && *msg ? "%s" : nullptr, msg); }
+
+static std::atomic<unsigned long long> g_launches{0};
+static thread_local sc_profile g_profile = {};
+
+extern "C" unsigned long long sc_launch_count(void) { return g_launches.load(); }
+extern "C" int sc_last_profile(sc_profile* out) {
+  if (!out) return SC_ERR_INVALID;
+  *out = g_profile;
+  return SC_OK;
+}
 
 extern "C" int sc_last_status(void) { return g_last_status; }
 extern "C" const char* sc_last_error(void) { return g_last_error; }
@@ -268,6 +279,7 @@ static int launch_row(const Plan& pl, RowParams rp, int B, cudaStream_t s, int n
   dim3 grid(rp.nblk, B);
   fn<<<grid, SC_ROW_THREADS, hot ? pl.row_smem : pl.rowg_smem, s>>>(rp);
   CU_TRY(cudaGetLastError());
+  ++g_launches;
   return SC_OK;
 }
 
@@ -293,6 +305,7 @@ static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     CU_TRY(cudaLaunchKernelEx(&cfg, fn, cp));
+    ++g_launches;
   } else {
     // forward / inverse only: maps split 8 ways, no cluster
     ColFn fn = col_fn<MODE>(cp.g.H);
@@ -303,6 +316,7 @@ static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s) {
     dim3 grid(cp.G, pl.col_ntiles, B);
     fn<<<grid, pl.colg_NT, pl.colg_smem, s>>>(cp);
     CU_TRY(cudaGetLastError());
+    ++g_launches;
   }
   return SC_OK;
 }
@@ -377,6 +391,7 @@ extern "C" int sc_cbpdn_solve(const sc_problem* p, const sc_options* o, void* wo
   twiddle_kernel<<<(g.W + 255) / 256, 256, 0, s>>>(twW, g.W);
   twiddle_kernel<<<(g.H + 255) / 256, 256, 0, s>>>(twH, g.H);
   CU_TRY(cudaGetLastError());
+  g_launches += 2;
 
   // Dictionary spectrum: rfft2 of the zero-padded filters (cuda_Pad_Dict +
   // R2C, cbpdn.cu:277-289), computed without materialising the padding.
@@ -409,6 +424,7 @@ extern "C" int sc_cbpdn_solve(const sc_problem* p, const sc_options* o, void* wo
   init_state_kernel<<<(g.B + 127) / 128, 128, 0, s>>>(sts, p->rho0, g.B, ndone);
   xi_kernel<<<(g.B + 127) / 128, 128, 0, s>>>(xi, p->lmbda, g.B, o->rsdl_target, o->std_residuals);
   CU_TRY(cudaGetLastError());
+  g_launches += 2;
 
   RowParams rp = {};
   rp.g = g; rp.pw = pl.pw; rp.twW = twW; rp.F = F; rp.Y = p->Y; rp.U = U;
@@ -427,17 +443,53 @@ extern "C" int sc_cbpdn_solve(const sc_problem* p, const sc_options* o, void* wo
   fp.nelem = (double)g.M * g.H * g.W;
   fp.xi = xi; fp.itstat = o->record_itstat ? it : nullptr; fp.ndone = ndone;
 
+  // Per-kernel event timing (profile mode only); events come from a
+  // grow-only pool so that profiling adds no per-launch host allocation.
+  struct EvRec { cudaEvent_t a, b; int kind; };
+  static std::vector<cudaEvent_t> ev_pool;
+  std::vector<EvRec> evs;
+  size_t ev_next = 0;
+  auto get_ev = [&](cudaEvent_t* e) -> int {
+    if (ev_next == ev_pool.size()) {
+      cudaEvent_t x;
+      CU_TRY(cudaEventCreate(&x));
+      ev_pool.push_back(x);
+    }
+    *e = ev_pool[ev_next++];
+    return SC_OK;
+  };
+  auto timed = [&](int kind, auto&& launch) -> int {
+    if (!o->profile) return launch();
+    EvRec e;
+    e.kind = kind;
+    int r = get_ev(&e.a);
+    if (!r) r = get_ev(&e.b);
+    if (r) return r;
+    CU_TRY(cudaEventRecord(e.a, s));
+    r = launch();
+    CU_TRY(cudaEventRecord(e.b, s));
+    evs.push_back(e);
+    return r;
+  };
+  // Without a stopping tolerance only a non-finite residual can end the
+  // solve early; the host then never waits on the device mid-solve.
+  const bool can_stop = o->rel_tol > 0.f || o->abs_tol > 0.f;
   int done_iters = 0;
   while (done_iters < o->max_iter) {
     int chunk = o->max_iter - done_iters;
-    if (o->check_every > 0) chunk = std::min(chunk, o->check_every);
+    if (o->check_every > 0 && can_stop) chunk = std::min(chunk, o->check_every);
     for (int i = 0; i < chunk; ++i) {
-      if ((st = launch_col<COL_SOLVE>(pl, cp, g.B, s))) return st;
-      if ((st = launch_row<ROW_ITER>(pl, rp, g.B, s))) return st;
-      finalize_kernel<<<g.B, 256, 0, s>>>(part, pl.row_nblk, sts, fp);
-      CU_TRY(cudaGetLastError());
+      if ((st = timed(0, [&] { return launch_col<COL_SOLVE>(pl, cp, g.B, s); }))) return st;
+      if ((st = timed(1, [&] { return launch_row<ROW_ITER>(pl, rp, g.B, s); }))) return st;
+      if ((st = timed(2, [&]() -> int {
+             finalize_kernel<<<g.B, 256, 0, s>>>(part, pl.row_nblk, sts, fp);
+             CU_TRY(cudaGetLastError());
+             ++g_launches;
+             return SC_OK;
+           })))
+        return st;
       if (o->auto_rho) {
-        if ((st = launch_row<ROW_FIXUP>(pl, rp, g.B, s))) return st;
+        if ((st = timed(3, [&] { return launch_row<ROW_FIXUP>(pl, rp, g.B, s); }))) return st;
       }
     }
     done_iters += chunk;
@@ -446,6 +498,16 @@ extern "C" int sc_cbpdn_solve(const sc_problem* p, const sc_options* o, void* wo
       CU_TRY(cudaMemcpyAsync(&nd, ndone, sizeof(int), cudaMemcpyDeviceToHost, s));
       CU_TRY(cudaStreamSynchronize(s));
       if (nd >= g.B) break;
+    }
+  }
+  if (o->profile) {
+    CU_TRY(cudaStreamSynchronize(s));
+    memset(&g_profile, 0, sizeof(g_profile));
+    for (auto& e : evs) {
+      float ms = 0.f;
+      CU_TRY(cudaEventElapsedTime(&ms, e.a, e.b));
+      g_profile.ms[e.kind] += ms;
+      g_profile.count[e.kind] += 1;
     }
   }
   if (res) {

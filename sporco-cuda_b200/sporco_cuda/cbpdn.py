@@ -210,7 +210,7 @@ def _host_solve(Dm, S, Wmask, lmbda, mu, opt, l1, gw, dev, grd):
 
 # ------------------------------------------------------ device (torch) path --
 
-def _sc_options(r, record_itstat=False, check_every=32):
+def _sc_options(r, record_itstat=False, check_every=32, profile=False):
     o = _lib.ScOptions()
     o.max_iter = r["MaxMainIter"]
     o.relax = r["RelaxParam"]
@@ -225,6 +225,7 @@ def _sc_options(r, record_itstat=False, check_every=32):
     o.std_residuals = r["StdResiduals"]
     o.record_itstat = int(bool(record_itstat or r["Verbose"]))
     o.check_every = int(check_every)
+    o.profile = int(bool(profile))
     return o
 
 
@@ -267,9 +268,17 @@ class DeviceSolve:
         _lib.check(st)
         return {"iterations": list(iters), "rho": list(rho), "itstat": it}
 
+    def profile(self):
+        """Per-kernel device time (ms, launches) of the last run with
+        profile=True: column pass, row pass, finalize, rho fix-up."""
+        p = _lib.ScProfile()
+        _lib.check(_lib.sc_last_profile(C.byref(p)))
+        names = ("col_kernel", "row_kernel", "finalize_kernel", "fixup_kernel")
+        return {n: (p.ms[i], p.count[i]) for i, n in enumerate(names)}
+
 
 def prepare_device(Dm, S, lmbda, opt, mu=0.0, grd=False, l1=1.0, gw=1.0, mask=None,
-                   rho0=None, Y=None, record_itstat=False, check_every=32):
+                   rho0=None, Y=None, record_itstat=False, check_every=32, profile=False):
     """Prepare a device solve for a batch of equal-sized images.
 
     Dm: (M, Kr, Kc) float32 CUDA tensor; S: (B, H, W) float32 CUDA tensor;
@@ -334,7 +343,7 @@ def prepare_device(Dm, S, lmbda, opt, mu=0.0, grd=False, l1=1.0, gw=1.0, mask=No
         Y = torch.empty((B, M, H, W), device=dev, dtype=torch.float32)
     keep["Y"] = Y
     prob.Y = Y.data_ptr()
-    o = _sc_options(r, record_itstat=record_itstat, check_every=check_every)
+    o = _sc_options(r, record_itstat=record_itstat, check_every=check_every, profile=profile)
     nbytes = _lib.sc_workspace_size(C.byref(prob), C.byref(o))
     if nbytes == 0:
         _lib.check_last()

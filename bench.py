@@ -296,14 +296,17 @@ def run_ours(args, cfg, rank, world, local_rank):
                 cb.cbpdngrd(Dn, Sn, lam, cfg["mu"], opt)
             else:
                 cb.cbpdnmsk(Dn, Sn * Wn, Wn, lam, opt)
-    e2e_step()
-    barrier()
     e_steps = max(1, min(args.steps, 3))
-    t0 = time.perf_counter()
-    for _ in range(e_steps):
+    if not args.no_e2e:
         e2e_step()
-    barrier()
-    e_ms = (time.perf_counter() - t0) * 1e3
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e_steps):
+            e2e_step()
+        barrier()
+        e_ms = (time.perf_counter() - t0) * 1e3
+    else:
+        e_ms = float("nan")
     if world > 1:
         t = torch.tensor([e_ms], device=dev, dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -406,8 +409,14 @@ def main():
     ap.add_argument("--config", type=int, default=1, choices=sorted(CONFIGS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end arm")
+    ap.add_argument("--iters", type=int, default=0,
+                    help="override the iterations per solve (profiling runs only)")
     args = ap.parse_args()
-    cfg = CONFIGS[args.config]
+    cfg = dict(CONFIGS[args.config])
+    if args.iters > 0:
+        cfg["iters"] = args.iters
+        cfg["workload"] += " [cut to %d iterations]" % args.iters
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -58,6 +58,10 @@ CONFIGS = {
     4: dict(workload="cbpdn 2048x2048 M=256 16x16, 100 iterations, AutoRho",
             H=2048, W=2048, M=256, K=16, density=0.01, lmbda=0.02, mu=0.0,
             variants=["cbpdn"], iters=100, autorho=True, mask_p=None),
+    # small 2048x2048 case for kernel profiles (2 GB on the device)
+    9: dict(workload="cbpdn 2048x2048 M=24 16x16, 20 iterations, AutoRho (profiling case)",
+            H=2048, W=2048, M=24, K=16, density=0.01, lmbda=0.02, mu=0.0,
+            variants=["cbpdn"], iters=20, autorho=True, mask_p=None),
 }
 
 

@@ -25,6 +25,9 @@
 //  * A group of g threads does one transform; several groups of a CTA run
 //    transforms of the same length in lock step and synchronise with
 //    __syncthreads() (all groups must call the routine together).
+//  * The n elements of a transform may be strided (element i at data[i*st]),
+//    so that several transforms can be interleaved in shared memory exactly
+//    as their columns are interleaved in global memory.
 //  * MAXE bounds the elements one thread holds: the caller guarantees
 //    n <= MAXE * g.
 #pragma once
@@ -140,7 +143,7 @@ __device__ __forceinline__ void dft_r(float2* v) {
 
 // ------------------------------------------------------------------ passes --
 template <int R, int MAXE>
-__device__ __forceinline__ void stockham_pass(float2* data, int n, int Ns,
+__device__ __forceinline__ void stockham_pass(float2* data, int n, int Ns, int st,
                                               const float2* __restrict__ tw,
                                               int t, int g) {
   constexpr int MAXB = (MAXE + R - 1) / R;
@@ -152,7 +155,7 @@ __device__ __forceinline__ void stockham_pass(float2* data, int n, int Ns,
     const int j = t + i * g;
     if (j < B) {
 #pragma unroll
-      for (int q = 0; q < R; ++q) v[i][q] = data[j + q * B];
+      for (int q = 0; q < R; ++q) v[i][q] = data[(j + q * B) * st];
       if (Ns > 1) {
         const int k = j % Ns;
 #pragma unroll
@@ -169,7 +172,7 @@ __device__ __forceinline__ void stockham_pass(float2* data, int n, int Ns,
       const int k = j % Ns;
       const int base = (j - k) * R + k;
 #pragma unroll
-      for (int q = 0; q < R; ++q) data[base + q * Ns] = v[i][q];
+      for (int q = 0; q < R; ++q) data[(base + q * Ns) * st] = v[i][q];
     }
   }
   __syncthreads();
@@ -178,9 +181,8 @@ __device__ __forceinline__ void stockham_pass(float2* data, int n, int Ns,
 // Any radix (used for prime factors other than 2, 3, 5): each thread
 // computes whole outputs, O(R) work per output.
 template <int MAXE>
-__device__ __noinline__ void generic_pass(float2* data, int n, int R, int Ns,
-                                             const float2* __restrict__ tw,
-                                             int t, int g) {
+__device__ __noinline__ void generic_pass(float2* data, int n, int R, int Ns, int st,
+                                          const float2* __restrict__ tw, int t, int g) {
   const int B = n / R;
   const int step = n / (Ns * R);
   float2 out[MAXE];
@@ -195,7 +197,7 @@ __device__ __noinline__ void generic_pass(float2* data, int n, int R, int Ns,
       float2 acc = make_float2(0.f, 0.f);
       int e = 0;
       for (int s = 0; s < R; ++s) {
-        const float2 x = data[j + s * B];
+        const float2 x = data[(j + s * B) * st];
         const float2 w = __ldg(&tw[e]);
         acc.x += x.x * w.x - x.y * w.y;
         acc.y += x.x * w.y + x.y * w.x;
@@ -213,7 +215,7 @@ __device__ __noinline__ void generic_pass(float2* data, int n, int R, int Ns,
       const int q = o / B;
       const int j = o - q * B;
       const int k = j % Ns;
-      data[(j - k) * R + k + q * Ns] = out[i];
+      data[((j - k) * R + k + q * Ns) * st] = out[i];
     }
   }
   __syncthreads();
@@ -223,28 +225,28 @@ __device__ __noinline__ void generic_pass(float2* data, int n, int R, int Ns,
 // a loop over a runtime radix sequence the register allocation of the
 // calling kernel grows past 200 registers.
 template <int MAXE>
-__device__ __noinline__ void fft_pass(float2* data, int n, int R, int Ns,
+__device__ __noinline__ void fft_pass(float2* data, int n, int R, int Ns, int st,
                                       const float2* __restrict__ tw, int t, int g) {
   switch (R) {
-    case 2: stockham_pass<2, MAXE>(data, n, Ns, tw, t, g); break;
-    case 3: stockham_pass<3, MAXE>(data, n, Ns, tw, t, g); break;
-    case 4: stockham_pass<4, MAXE>(data, n, Ns, tw, t, g); break;
-    case 5: stockham_pass<5, MAXE>(data, n, Ns, tw, t, g); break;
-    case 8: stockham_pass<8, MAXE>(data, n, Ns, tw, t, g); break;
-    default: generic_pass<MAXE>(data, n, R, Ns, tw, t, g); break;
+    case 2: stockham_pass<2, MAXE>(data, n, Ns, st, tw, t, g); break;
+    case 3: stockham_pass<3, MAXE>(data, n, Ns, st, tw, t, g); break;
+    case 4: stockham_pass<4, MAXE>(data, n, Ns, st, tw, t, g); break;
+    case 5: stockham_pass<5, MAXE>(data, n, Ns, st, tw, t, g); break;
+    case 8: stockham_pass<8, MAXE>(data, n, Ns, st, tw, t, g); break;
+    default: generic_pass<MAXE>(data, n, R, Ns, st, tw, t, g); break;
   }
 }
 
-// In-place forward DFT of data[0..n) (shared memory) by a group of g threads,
-// for any n (runtime plan; the fallback path).
+// In-place forward DFT of data[0], data[st], ..., data[(n-1) st] (shared
+// memory) by a group of g threads, for any n (runtime plan; the fallback).
 template <int MAXE>
-__device__ __forceinline__ void fft_forward(float2* data, const FftPlan& P,
+__device__ __forceinline__ void fft_forward(float2* data, const FftPlan& P, int st,
                                             const float2* __restrict__ tw, int t, int g) {
   int Ns = 1;
   const int np = P.npass;
   for (int p = 0; p < np; ++p) {
     const int R = P.radix[p];
-    fft_pass<MAXE>(data, P.n, R, Ns, tw, t, g);
+    fft_pass<MAXE>(data, P.n, R, Ns, st, tw, t, g);
     Ns *= R;
   }
 }
@@ -294,7 +296,7 @@ __host__ __device__ constexpr int ct_threads(int n) {
   return g < 32 ? 32 : (g > 256 ? 256 : g);
 }
 
-template <int N, int R, int NS, int G>
+template <int N, int R, int NS, int G, int ST>
 __device__ __forceinline__ void ct_pass(float2* data, const float2* __restrict__ tw, int t) {
   constexpr int B = N / R;
   constexpr int NB = (B + G - 1) / G;
@@ -305,7 +307,7 @@ __device__ __forceinline__ void ct_pass(float2* data, const float2* __restrict__
     const int j = t + i * G;
     if ((B % G) == 0 || j < B) {
 #pragma unroll
-      for (int q = 0; q < R; ++q) v[i][q] = data[j + q * B];
+      for (int q = 0; q < R; ++q) v[i][q] = data[(j + q * B) * ST];
       if constexpr (NS > 1) {
         const int k = j % NS;
 #pragma unroll
@@ -322,18 +324,18 @@ __device__ __forceinline__ void ct_pass(float2* data, const float2* __restrict__
       const int k = j % NS;
       const int base = (j - k) * R + k;
 #pragma unroll
-      for (int q = 0; q < R; ++q) data[base + q * NS] = v[i][q];
+      for (int q = 0; q < R; ++q) data[(base + q * NS) * ST] = v[i][q];
     }
   }
   __syncthreads();
 }
 
-template <int N, int G, int P = 0>
+template <int N, int G, int ST, int P = 0>
 __device__ __forceinline__ void fft_ct(float2* data, const float2* __restrict__ tw, int t) {
   constexpr CtPlan pl = ct_plan(N);
   if constexpr (P < pl.np) {
-    ct_pass<N, pl.r[P], ct_ns(pl, P), G>(data, tw, t);
-    fft_ct<N, G, P + 1>(data, tw, t);
+    ct_pass<N, pl.r[P], ct_ns(pl, P), G, ST>(data, tw, t);
+    fft_ct<N, G, ST, P + 1>(data, tw, t);
   }
 }
 
@@ -345,14 +347,15 @@ __host__ __device__ constexpr bool ct_fast_radices(int n) {
   return true;
 }
 
-// Forward DFT of length N (N > 0: compile-time plan, N == 0: runtime plan P
-// with g threads per transform).
-template <int N>
+// Forward DFT of length N of the elements data[0], data[ST], ...
+// (N > 0: compile-time plan; N == 0: runtime plan P with g threads and
+// stride ST).
+template <int N, int ST>
 __device__ __forceinline__ void fft_any(float2* data, const FftPlan& P,
                                         const float2* __restrict__ tw, int t, int g) {
   if constexpr (N == 0) {
-    fft_forward<16>(data, P, tw, t, g);
+    fft_forward<16>(data, P, ST, tw, t, g);
   } else {
-    fft_ct<N, ct_threads(N)>(data, tw, t);
+    fft_ct<N, ct_threads(N), ST>(data, tw, t);
   }
 }

@@ -21,6 +21,7 @@
 struct ImgState {
   double rho;    // rho used by the next iteration
   double rsf;    // scale factor chosen by the last adaptive-rho step (1: none)
+  double uscale; // the next row pass reads U scaled by this (1 / rsf)
   double r, s;   // last residuals (normalised unless StdResiduals)
   double epri, edua;
   double nX, nY, nU;
@@ -95,3 +96,23 @@ struct ColParams {
 
 enum RowMode { ROW_ITER = 0, ROW_FWD_REAL = 1, ROW_FWD_DICT = 2, ROW_INV_REAL = 3, ROW_FIXUP = 4 };
 enum ColMode { COL_SOLVE = 0, COL_FWD = 1, COL_INV = 2 };
+
+__host__ __device__ inline size_t sc_align16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+// Shared memory of one row-pass slot (one row pair in flight).  The
+// iteration mode double-buffers the pair's two spectrum rows and stages the
+// pair's Y and U rows: [z: W complex][F: 2 x 2Wp complex][Y: 2W][U: 2W].
+__host__ __device__ inline size_t row_slot_bytes(int mode, int W, int Wp) {
+  size_t z = sc_align16((size_t)W * 8);
+  if (mode != ROW_ITER) return z;
+  return z + 2 * (size_t)(2 * Wp) * 8 + 2 * sc_align16((size_t)(2 * W) * 4);
+}
+
+// Shared memory of one column-pass CTA: the solve double-buffers the tile
+// (SC_COL_TILE interleaved columns of H complex) and accumulates
+// sum_m Df b / d (complex) and sum_m |Df|^2 / d (real) per tile element.
+__host__ __device__ inline size_t col_smem_bytes(int mode, int H) {
+  const size_t tile = (size_t)SC_COL_TILE * H * 8;
+  if (mode != COL_SOLVE) return tile;
+  return 2 * tile + (size_t)SC_COL_TILE * H * 12;
+}

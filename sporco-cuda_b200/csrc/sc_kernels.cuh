@@ -20,12 +20,19 @@
 //                          (row half).
 //   finalize_kernel        FP64 reduction of the partials, residuals, stopping
 //                          test, adaptive rho (host code at cbpdn.cu:405-559).
-//   row_kernel<ROW_FIXUP>  only when rho changed: U <- U / rsf and the row
-//                          spectra corrected by (1 - 1/rsf) rowFFT(U)
-//                          (replaces cublasSgeam at cbpdn.cu:546-549).
+//   row_kernel<ROW_FIXUP>  only when rho changed: the row spectra corrected
+//                          by (1 - 1/rsf) rowFFT(U); the next row pass reads
+//                          U scaled by 1/rsf (replaces cublasSgeam at
+//                          cbpdn.cu:546-549).
 //
 // HBM layout: real maps (B, M, H, W) float32; spectra (B, M, H, Wp) complex64
 // with Wp = W/2+1 rounded up to a multiple of 4 (storage padding only).
+//
+// Both hot kernels keep copies in flight while they compute: the column pass
+// double-buffers its (H x 4) tiles with cp.async and transforms them in place
+// in the interleaved layout they have in HBM; the row pass double-buffers the
+// spectrum rows of the next row pair and stages the pair's Y and U rows
+// before its inverse FFT.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -33,6 +40,23 @@
 #include "sc_internal.cuh"
 
 namespace cg = cooperative_groups;
+
+// ------------------------------------------------------------ async copies --
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 // Soft threshold as the reference's shrink kernels compute it
 // (cbpdn_kernels.cu:129-311): sign(v) max(|v| - t, 0), t may be negative.
@@ -70,6 +94,25 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* scratch) {
   __syncthreads();
 }
 
+// Hermitian-extend two half spectra (rows a, b of an rfft2 row pass) and pack
+// them as conj(A + iB) for an inverse transform taken as conj(FFT(conj .)).
+// The imaginary parts of the DC and (even W) Nyquist bins are ignored, as a
+// C2R transform does.
+__device__ __forceinline__ float2 pack_inverse(const float2* a, const float2* bb, bool has1,
+                                               int k, int W, int Wf) {
+  float2 A, Bv;
+  if (k < Wf) {
+    A = a[k];
+    Bv = has1 ? bb[k] : make_float2(0.f, 0.f);
+    if (k == 0 || 2 * k == W) { A.y = 0.f; Bv.y = 0.f; }
+    return make_float2(A.x - Bv.y, -(A.y + Bv.x));
+  }
+  const int kk = W - k;
+  A = a[kk];
+  Bv = has1 ? bb[kk] : make_float2(0.f, 0.f);
+  return make_float2(A.x + Bv.y, -(Bv.x - A.y));
+}
+
 // ============================================================== row pass ==
 // NW > 0: row length W known at compile time (specialised FFT plan);
 // NW == 0: any W (runtime FFT plan).
@@ -77,7 +120,6 @@ template <int MODE, int NW>
 __global__ void __launch_bounds__(SC_ROW_THREADS, 2)
 row_kernel(RowParams P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* smem = reinterpret_cast<float2*>(smem_raw);
   __shared__ double red_scratch[(SC_ROW_THREADS / 32) * 5];
 
   const Geom& G = P.g;
@@ -87,86 +129,109 @@ row_kernel(RowParams P) {
   const int S = blockDim.x / g;
   const int s = threadIdx.x / g;
   const int t = threadIdx.x - s * g;
-  float2* z = smem + (size_t)s * W;
+  unsigned char* slot = smem_raw + (size_t)s * row_slot_bytes(MODE, W, Wp);
+  float2* z = reinterpret_cast<float2*>(slot);
 
-  float thr = 0.f, rsf_c = 0.f, inv_rsf = 1.f;
+  float thr = 0.f, rsf_c = 0.f, uscale = 1.f;
   if constexpr (MODE == ROW_ITER || MODE == ROW_FIXUP) {
     const ImgState& st = P.st[b];
     if (st.done) return;
     if constexpr (MODE == ROW_ITER) {
       thr = (float)((double)P.lam[b] / st.rho);
+      uscale = (float)st.uscale;
     } else {
       if (st.rsf == 1.0) return;
       rsf_c = (float)(1.0 - 1.0 / st.rsf);
-      inv_rsf = (float)(1.0 / st.rsf);
     }
   }
 
-  const long rows = (long)G.M * H;           // rows per image
+  const long rows = (long)G.M * H;  // rows per image
   const long npairs = (rows + 1) / 2;
   const size_t img_real = (size_t)rows * W;
   const size_t img_spec = (size_t)rows * Wp;
   float2* Fi = P.F + (size_t)b * img_spec;
+  const long pstride = (long)gridDim.x * S;
 
-  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  if constexpr (MODE == ROW_ITER) {
+    // --------------------------------------------------------- iteration
+    float2* fst = reinterpret_cast<float2*>(slot + sc_align16((size_t)W * 8));
+    float* ysm = reinterpret_cast<float*>(fst + 2 * 2 * (size_t)Wp);
+    float* usm = ysm + sc_align16((size_t)(2 * W) * 4) / 4;
+    const float* Yi = P.Y + (size_t)b * img_real;
+    const float* Ui = P.U + (size_t)b * img_real;
+    const bool vec = (W & 3) == 0;
 
-  for (long pb = (long)blockIdx.x * S; pb < npairs; pb += (long)gridDim.x * S) {
-    const long p = pb + s;
-    const bool valid = p < npairs;
-    const long r0 = 2 * p, r1 = 2 * p + 1;
-    const bool has1 = valid && (r1 < rows);
-
-    // ---------------------------------------------------------- stage in
-    if constexpr (MODE == ROW_ITER || MODE == ROW_INV_REAL) {
-      // Hermitian-extend the two half spectra and pack them as A + iB; the
-      // inverse FFT is taken as conj(FFT(conj(.))).  The imaginary parts of
-      // the DC and (even W) Nyquist bins are ignored, as a C2R transform does.
-      if (valid) {
-        const float2* a = Fi + r0 * Wp;
-        const float2* bb = Fi + r1 * Wp;
-        for (int k = t; k < W; k += g) {
-          float2 A, Bv, Zc;
-          if (k < Wf) {
-            A = a[k];
-            Bv = has1 ? bb[k] : make_float2(0.f, 0.f);
-            if (k == 0 || 2 * k == W) { A.y = 0.f; Bv.y = 0.f; }
-            Zc = make_float2(A.x - Bv.y, -(A.y + Bv.x));
-          } else {
-            const int kk = W - k;
-            A = a[kk];
-            Bv = has1 ? bb[kk] : make_float2(0.f, 0.f);
-            Zc = make_float2(A.x + Bv.y, -(Bv.x - A.y));
+    auto issue_F = [&](long p, int stage) {
+      if (p < npairs) {
+        const int nrow = (2 * p + 1 < rows) ? 2 : 1;
+        const float2* src = Fi + 2 * p * Wp;
+        float2* dst = fst + stage * 2 * Wp;
+        const int nch = nrow * Wp / 2;
+        for (int q = t; q < nch; q += g) cp_async16(dst + 2 * q, src + 2 * q);
+      }
+    };
+    auto issue_YU = [&](long p) {
+      if (p < npairs) {
+        const int n = ((2 * p + 1 < rows) ? 2 : 1) * W;
+        const float* ys = Yi + 2 * p * W;
+        const float* us = Ui + 2 * p * W;
+        if (vec) {
+          for (int q = t; q < n / 4; q += g) {
+            cp_async16(ysm + 4 * q, ys + 4 * q);
+            cp_async16(usm + 4 * q, us + 4 * q);
           }
-          z[k] = Zc;
+        } else {
+          for (int q = t; q < n; q += g) {
+            cp_async4(ysm + q, ys + q);
+            cp_async4(usm + q, us + q);
+          }
         }
       }
-      __syncthreads();
-      fft_any<NW>(z, P.pw, P.twW, t, g);
-    }
+    };
 
-    // ---------------------------------------------------------- epilogue
-    if constexpr (MODE == ROW_ITER) {
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const int32_t* mk = P.mask ? P.mask + (size_t)b * H * W : nullptr;
+    const float a = P.relax, a1 = 1.f - P.relax;
+    const bool relax = P.relax != 1.f;
+
+    issue_F((long)blockIdx.x * S + s, 0);
+    cp_async_commit();
+    int it = 0;
+    for (long pb = (long)blockIdx.x * S; pb < npairs; pb += pstride, ++it) {
+      const long p = pb + s;
+      const bool valid = p < npairs;
+      const long r0 = 2 * p, r1 = 2 * p + 1;
+      const bool has1 = valid && (r1 < rows);
+      issue_YU(p);
+      cp_async_commit();
+      issue_F(p + pstride, (it + 1) & 1);
+      cp_async_commit();
+      cp_async_wait<2>();
+      __syncthreads();
+      if (valid) {
+        const float2* fa = fst + (it & 1) * 2 * Wp;
+        for (int k = t; k < W; k += g) z[k] = pack_inverse(fa, fa + Wp, has1, k, W, Wf);
+      }
+      __syncthreads();
+      fft_any<NW, 1>(z, P.pw, P.twW, t, g);
+      cp_async_wait<1>();
+      __syncthreads();
       if (valid) {
         const int m0 = (int)(r0 / H), h0 = (int)(r0 - (long)m0 * H);
         const int m1 = (int)(r1 / H), h1 = (int)(r1 - (long)m1 * H);
         float* Y0 = P.Y + (size_t)b * img_real + (size_t)r0 * W;
         float* U0 = P.U + (size_t)b * img_real + (size_t)r0 * W;
-        float* Y1 = Y0 + W;
-        float* U1 = U0 + W;
-        const int32_t* mk = P.mask ? P.mask + (size_t)b * H * W : nullptr;
         float w0 = P.l1_scalar, w1 = P.l1_scalar;
         if (P.l1_kind == 1) { w0 = P.l1w[m0]; w1 = has1 ? P.l1w[m1] : 0.f; }
         const float* wr0 = P.l1_kind == 2 ? P.l1w + ((size_t)m0 * H + h0) * W : nullptr;
         const float* wr1 = (P.l1_kind == 2 && has1) ? P.l1w + ((size_t)m1 * H + h1) * W : nullptr;
         const bool ams0 = mk && m0 == 0, ams1 = mk && m1 == 0;
-        const float a = P.relax, a1 = 1.f - P.relax;
-        const bool relax = P.relax != 1.f;
         for (int k = t; k < W; k += g) {
           const float2 zz = z[k];
           float yu0, yu1 = 0.f;
           {
             const float x = zz.x * P.invN;
-            const float yo = Y0[k], uo = U0[k];
+            const float yo = ysm[k], uo = usm[k] * uscale;
             const float xr = relax ? a * x + a1 * yo : x;
             const float v = xr + uo;
             float y;
@@ -185,15 +250,15 @@ row_kernel(RowParams P) {
           }
           if (has1) {
             const float x = -zz.y * P.invN;
-            const float yo = Y1[k], uo = U1[k];
+            const float yo = ysm[W + k], uo = usm[W + k] * uscale;
             const float xr = relax ? a * x + a1 * yo : x;
             const float v = xr + uo;
             float y;
             if (ams1) y = (float)(1 - mk[h1 * W + k]) * v;
             else y = soft_threshold(v, thr * (wr1 ? wr1[k] : w1));
             const float u = v - y;
-            Y1[k] = y;
-            U1[k] = u;
+            Y0[W + k] = y;
+            U0[W + k] = u;
             yu1 = y - u;
             const float dxy = x - y, dyy = yo - y;
             acc[0] += (double)(x * x);
@@ -205,63 +270,86 @@ row_kernel(RowParams P) {
           z[k] = make_float2(yu0, yu1);
         }
       }
-    } else if constexpr (MODE == ROW_INV_REAL) {
-      if (valid) {
-        float* d0 = P.dst + (size_t)b * img_real + (size_t)r0 * W;
-        for (int k = t; k < W; k += g) {
-          const float2 zz = z[k];
-          d0[k] = zz.x * P.invN;
-          if (has1) d0[W + k] = -zz.y * P.invN;
-        }
-      }
-    } else if constexpr (MODE == ROW_FWD_REAL) {
-      if (valid) {
-        const float* s0 = P.src + (size_t)b * img_real + (size_t)r0 * W;
-        for (int k = t; k < W; k += g)
-          z[k] = make_float2(s0[k], has1 ? s0[W + k] : 0.f);
-      }
-    } else if constexpr (MODE == ROW_FWD_DICT) {
-      if (valid) {
-        const int m0 = (int)(r0 / H), h0 = (int)(r0 - (long)m0 * H);
-        const int m1 = (int)(r1 / H), h1 = (int)(r1 - (long)m1 * H);
-        for (int k = t; k < W; k += g) {
-          float v0 = 0.f, v1 = 0.f;
-          if (h0 < P.Kr && k < P.Kc) v0 = P.D[((size_t)m0 * P.Kr + h0) * P.Kc + k];
-          if (has1 && h1 < P.Kr && k < P.Kc) v1 = P.D[((size_t)m1 * P.Kr + h1) * P.Kc + k];
-          z[k] = make_float2(v0, v1);
-        }
-      }
-    } else if constexpr (MODE == ROW_FIXUP) {
-      if (valid) {
-        float* U0 = P.U + (size_t)b * img_real + (size_t)r0 * W;
-        for (int k = t; k < W; k += g) {
-          const float u0 = U0[k];
-          const float u1 = has1 ? U0[W + k] : 0.f;
-          z[k] = make_float2(u0, u1);
-          U0[k] = u0 * inv_rsf;
-          if (has1) U0[W + k] = u1 * inv_rsf;
-        }
-      }
-    }
-
-    // ---------------------------------------------------------- forward + out
-    if constexpr (MODE != ROW_INV_REAL) {
       __syncthreads();
-      fft_any<NW>(z, P.pw, P.twW, t, g);
+      fft_any<NW, 1>(z, P.pw, P.twW, t, g);
+      if (valid) {
+        float2* fa = Fi + r0 * Wp;
+        for (int k = t; k < Wf; k += g) {
+          const float2 Zk = z[k];
+          const float2 Zm = z[k == 0 ? 0 : W - k];
+          // A = (Z_k + conj Z_{-k}) / 2 ;  B = (Z_k - conj Z_{-k}) / (2i)
+          fa[k] = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
+          if (has1) fa[Wp + k] = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
+        }
+      }
+      __syncthreads();
+    }
+    cp_async_wait<0>();
+    block_sum<5>(acc, red_scratch);
+    if (threadIdx.x == 0) {
+      double* out = P.partials + ((size_t)b * P.nblk + blockIdx.x) * 5;
+#pragma unroll
+      for (int i = 0; i < 5; ++i) out[i] = acc[i];
+    }
+    return;
+  } else {
+    // ------------------------------------- setup, tool and fix-up modes
+    for (long pb = (long)blockIdx.x * S; pb < npairs; pb += pstride) {
+      const long p = pb + s;
+      const bool valid = p < npairs;
+      const long r0 = 2 * p, r1 = 2 * p + 1;
+      const bool has1 = valid && (r1 < rows);
+      if constexpr (MODE == ROW_INV_REAL) {
+        if (valid) {
+          const float2* a = Fi + r0 * Wp;
+          for (int k = t; k < W; k += g) z[k] = pack_inverse(a, a + Wp, has1, k, W, Wf);
+        }
+        __syncthreads();
+        fft_any<NW, 1>(z, P.pw, P.twW, t, g);
+        if (valid) {
+          float* d0 = P.dst + (size_t)b * img_real + (size_t)r0 * W;
+          for (int k = t; k < W; k += g) {
+            const float2 zz = z[k];
+            d0[k] = zz.x * P.invN;
+            if (has1) d0[W + k] = -zz.y * P.invN;
+          }
+        }
+        __syncthreads();
+        continue;
+      }
+      if (valid) {
+        if constexpr (MODE == ROW_FWD_REAL) {
+          const float* s0 = P.src + (size_t)b * img_real + (size_t)r0 * W;
+          for (int k = t; k < W; k += g) z[k] = make_float2(s0[k], has1 ? s0[W + k] : 0.f);
+        } else if constexpr (MODE == ROW_FWD_DICT) {
+          const int m0 = (int)(r0 / H), h0 = (int)(r0 - (long)m0 * H);
+          const int m1 = (int)(r1 / H), h1 = (int)(r1 - (long)m1 * H);
+          for (int k = t; k < W; k += g) {
+            float v0 = 0.f, v1 = 0.f;
+            if (h0 < P.Kr && k < P.Kc) v0 = P.D[((size_t)m0 * P.Kr + h0) * P.Kc + k];
+            if (has1 && h1 < P.Kr && k < P.Kc) v1 = P.D[((size_t)m1 * P.Kr + h1) * P.Kc + k];
+            z[k] = make_float2(v0, v1);
+          }
+        } else if constexpr (MODE == ROW_FIXUP) {
+          const float* U0 = P.U + (size_t)b * img_real + (size_t)r0 * W;
+          for (int k = t; k < W; k += g) z[k] = make_float2(U0[k], has1 ? U0[W + k] : 0.f);
+        }
+      }
+      __syncthreads();
+      fft_any<NW, 1>(z, P.pw, P.twW, t, g);
       if (valid) {
         float2* a = Fi + r0 * Wp;
         float2* bb = Fi + r1 * Wp;
         for (int k = t; k < Wf; k += g) {
           const float2 Zk = z[k];
           const float2 Zm = z[k == 0 ? 0 : W - k];
-          // A = (Z_k + conj Z_{-k}) / 2 ;  B = (Z_k - conj Z_{-k}) / (2i)
           const float2 A = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
           const float2 Bv = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
           if constexpr (MODE == ROW_FIXUP) {
-            float2 fa = a[k];
+            const float2 fa = a[k];
             a[k] = make_float2(fa.x + rsf_c * A.x, fa.y + rsf_c * A.y);
             if (has1) {
-              float2 fb = bb[k];
+              const float2 fb = bb[k];
               bb[k] = make_float2(fb.x + rsf_c * Bv.x, fb.y + rsf_c * Bv.y);
             }
           } else {
@@ -270,45 +358,37 @@ row_kernel(RowParams P) {
           }
         }
       }
-    }
-    __syncthreads();
-  }
-
-  if constexpr (MODE == ROW_ITER) {
-    block_sum<5>(acc, red_scratch);
-    if (threadIdx.x == 0) {
-      double* out = P.partials + ((size_t)b * P.nblk + blockIdx.x) * 5;
-#pragma unroll
-      for (int i = 0; i < 5; ++i) out[i] = acc[i];
+      __syncthreads();
     }
   }
 }
 
 // =========================================================== column pass ==
 // Grid (G, ntiles, B).  For COL_SOLVE the G CTAs of one column tile form a
-// thread-block cluster; each handles a contiguous chunk of the maps.
-// NH > 0: column length H known at compile time; NH == 0: any H.
+// thread-block cluster; each handles a contiguous chunk of the maps.  Tiles
+// keep their HBM layout in shared memory: element (kr, c) of the tile at
+// [kr * T + c]; thread tid works on column c = tid % T.
 template <int MODE, int NH>
-__global__ void __launch_bounds__(SC_COL_MAX_THREADS)
+__global__ void __launch_bounds__(NH > 1024 ? SC_COL_MAX_THREADS : SC_COL_MAX_THREADS / 2)
 col_kernel(ColParams P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int T = SC_COL_TILE;
   const Geom& G = P.g;
   const int H = G.H, Wf = G.Wf, Wp = G.Wp, M = G.M;
-  const int Hs = P.Hs;
-  constexpr int T = SC_COL_TILE;
-  float2* buf = reinterpret_cast<float2*>(smem_raw);            // T x Hs
-  float2* num = buf + (size_t)T * Hs;                            // T*H (solve)
-  float* sden = reinterpret_cast<float*>(num + (size_t)T * H);   // T*H (solve)
+  const int E = T * H;
+  float2* stg = reinterpret_cast<float2*>(smem_raw);     // [2][E] (solve) / [E]
+  float2* num = stg + 2 * (size_t)E;                      // [E] (solve)
+  float* sden = reinterpret_cast<float*>(num + E);        // [E] (solve)
 
   const int b = blockIdx.z;
   const int tile = blockIdx.y;
   const int rank = blockIdx.x;
   const int c0 = tile * T;
   const int g = NH > 0 ? ct_threads(NH) : P.gsz;
-  const int grp = threadIdx.x / g;
-  const int t = threadIdx.x - grp * g;
   const int NT = blockDim.x;
-  const int E = T * H;
+  const int tid = threadIdx.x;
+  const int cc = tid % T;   // column of this thread (T divides NT)
+  const int t = tid / T;    // index within the column's thread group
 
   float rho = 0.f;
   if constexpr (MODE == COL_SOLVE) {
@@ -317,91 +397,100 @@ col_kernel(ColParams P) {
     rho = (float)st.rho;
   }
 
-  const int nmaps = M;
-  const int chunk = (nmaps + P.G - 1) / P.G;
+  const int chunk = (M + P.G - 1) / P.G;
   const int m0 = rank * chunk;
-  const int m1 = min(nmaps, m0 + chunk);
-  float2* Fi = P.F + (size_t)b * nmaps * H * Wp;
-
-  auto load_tile = [&](int m, bool conj_in) {
-    const float2* src = Fi + (size_t)m * H * Wp + c0;
-    for (int e = threadIdx.x; e < E; e += NT) {
-      const int kr = e / T, c = e - kr * T;
-      float2 v = make_float2(0.f, 0.f);
-      if (c0 + c < Wf) v = src[(size_t)kr * Wp + c];
-      if (conj_in) v.y = -v.y;
-      buf[c * Hs + kr] = v;
-    }
-    __syncthreads();
-  };
-  auto store_tile = [&](int m, bool conj_out) {
-    float2* dst = Fi + (size_t)m * H * Wp + c0;
-    for (int e = threadIdx.x; e < E; e += NT) {
-      const int kr = e / T, c = e - kr * T;
-      if (c0 + c < Wf) {
-        float2 v = buf[c * Hs + kr];
-        if (conj_out) v.y = -v.y;
-        dst[(size_t)kr * Wp + c] = v;
-      }
-    }
-  };
+  const int m1 = min(M, m0 + chunk);
+  float2* Fi = P.F + (size_t)b * M * H * Wp;
 
   if constexpr (MODE == COL_FWD || MODE == COL_INV) {
+    // setup / tool: plain loads (the spectrum pitch may be unaligned here)
     const bool inv = MODE == COL_INV;
     for (int m = m0; m < m1; ++m) {
-      load_tile(m, inv);
-      fft_any<NH>(buf + grp * Hs, P.ph, P.twH, t, g);
-      store_tile(m, inv);
-      __syncthreads();
-    }
-    return;
-  } else {
-    const float2* Sh = P.Sh + (size_t)b * H * Wp + c0;
-    const float mu = P.mu;
-    const bool grd = P.grd != 0;
-    // ------------------------------------------------------------ pass 1
-    for (int e = threadIdx.x; e < E; e += NT) {
-      num[e] = make_float2(0.f, 0.f);
-      sden[e] = 0.f;
-    }
-    for (int m = m0; m < m1; ++m) {
-      load_tile(m, false);
-      fft_any<NH>(buf + grp * Hs, P.ph, P.twH, t, g);
-      const float2* Dm = P.Dh + (size_t)m * H * Wp + c0;
-      const float wg = grd ? mu * P.wgrd[m] : 0.f;
-      for (int e = threadIdx.x; e < E; e += NT) {
+      float2* src = Fi + (size_t)m * H * Wp + c0;
+      for (int e = tid; e < E; e += NT) {
         const int kr = e / T, c = e - kr * T;
-        const int kc = c0 + c;
-        if (kc < Wf) {
-          const float2 Dv = Dm[(size_t)kr * Wp + c];
-          const float2 Sv = Sh[(size_t)kr * Wp + c];
-          const float2 yu = buf[c * Hs + kr];
-          // b = conj(D) S + rho (Y - U)^
-          const float2 bv = make_float2(Dv.x * Sv.x + Dv.y * Sv.y + rho * yu.x,
-                                        Dv.x * Sv.y - Dv.y * Sv.x + rho * yu.y);
-          float d = rho;
-          if (grd) {
-            const float gh = 4.f - 2.f * __ldg(&P.twW[kc]).x - 2.f * __ldg(&P.twH[kr]).x;
-            d = wg * gh + rho;
-          }
-          const float id = 1.f / d;
-          const int a = c * H + kr;
-          float2 nv = num[a];
-          nv.x += (Dv.x * bv.x - Dv.y * bv.y) * id;
-          nv.y += (Dv.x * bv.y + Dv.y * bv.x) * id;
-          num[a] = nv;
-          sden[a] += (Dv.x * Dv.x + Dv.y * Dv.y) * id;
+        float2 v = make_float2(0.f, 0.f);
+        if (c0 + c < Wf) v = src[(size_t)kr * Wp + c];
+        if (inv) v.y = -v.y;
+        stg[e] = v;
+      }
+      __syncthreads();
+      fft_any<NH, T>(stg + cc, P.ph, P.twH, t, g);
+      for (int e = tid; e < E; e += NT) {
+        const int kr = e / T, c = e - kr * T;
+        if (c0 + c < Wf) {
+          float2 v = stg[e];
+          if (inv) v.y = -v.y;
+          src[(size_t)kr * Wp + c] = v;
         }
       }
       __syncthreads();
     }
+    return;
+  } else {
+    // tile row (kr, 0..3) is 32 contiguous bytes: two 16-byte async copies
+    auto issue_tile = [&](int m, float2* dst) {
+      const float2* src = Fi + (size_t)m * H * Wp + c0;
+      for (int q = tid; q < 2 * H; q += NT) {
+        const int kr = q >> 1, h = q & 1;
+        cp_async16(dst + kr * T + 2 * h, src + (size_t)kr * Wp + 2 * h);
+      }
+    };
+    const float2* Sh = P.Sh + (size_t)b * H * Wp + c0;
+    const float mu = P.mu;
+    const bool grd = P.grd != 0;
+    const int kc = c0 + cc;
+    const bool colok = kc < Wf;
+    const float gw_col = grd && colok ? 2.f - 2.f * __ldg(&P.twW[kc]).x : 0.f;
+
+    // ------------------------------------------------------------ pass 1
+    for (int e = tid; e < E; e += NT) {
+      num[e] = make_float2(0.f, 0.f);
+      sden[e] = 0.f;
+    }
+    if (m0 < m1) issue_tile(m0, stg);
+    cp_async_commit();
+    int it = 0;
+    for (int m = m0; m < m1; ++m, ++it) {
+      float2* cur = stg + (size_t)(it & 1) * E;
+      if (m + 1 < m1) issue_tile(m + 1, stg + (size_t)((it + 1) & 1) * E);
+      cp_async_commit();
+      cp_async_wait<1>();
+      __syncthreads();
+      fft_any<NH, T>(cur + cc, P.ph, P.twH, t, g);
+      const float2* Dm = P.Dh + (size_t)m * H * Wp + c0;
+      const float wg = grd ? mu * P.wgrd[m] : 0.f;
+      if (colok) {
+        for (int e = tid; e < E; e += NT) {
+          const int kr = e / T;
+          const float2 Dv = __ldg(&Dm[(size_t)kr * Wp + cc]);
+          const float2 Sv = __ldg(&Sh[(size_t)kr * Wp + cc]);
+          const float2 yu = cur[e];
+          // b = conj(D) S + rho (Y - U)^
+          const float2 bv = make_float2(Dv.x * Sv.x + Dv.y * Sv.y + rho * yu.x,
+                                        Dv.x * Sv.y - Dv.y * Sv.x + rho * yu.y);
+          float d = rho;
+          if (grd) d = wg * (gw_col + 2.f - 2.f * __ldg(&P.twH[kr]).x) + rho;
+          const float id = 1.f / d;
+          float2 nv = num[e];
+          nv.x += (Dv.x * bv.x - Dv.y * bv.y) * id;
+          nv.y += (Dv.x * bv.y + Dv.y * bv.x) * id;
+          num[e] = nv;
+          sden[e] += (Dv.x * Dv.x + Dv.y * Dv.y) * id;
+        }
+      }
+      __syncthreads();
+    }
+    // prefetch the first tile of pass 2 while the maps are reduced
+    if (m0 < m1) issue_tile(m0, stg);
+    cp_async_commit();
     // ------------------------------------------------- reduce over the maps
     if (P.G > 1) {
       cg::cluster_group cluster = cg::this_cluster();
       cluster.sync();
       const int sl = (E + P.G - 1) / P.G;
       const int e0 = rank * sl, e1 = min(E, e0 + sl);
-      for (int e = e0 + threadIdx.x; e < e1; e += NT) {
+      for (int e = e0 + tid; e < e1; e += NT) {
         float2 ns = make_float2(0.f, 0.f);
         float ds = 0.f;
         for (int r = 0; r < P.G; ++r) {
@@ -416,52 +505,61 @@ col_kernel(ColParams P) {
         num[e] = make_float2(ns.x * q, ns.y * q);
       }
       cluster.sync();
-      for (int e = threadIdx.x; e < E; e += NT) {
+      for (int e = tid; e < E; e += NT) {
         const int owner = e / sl;
         if (owner != rank) num[e] = cluster.map_shared_rank(num, owner)[e];
       }
       cluster.sync();
     } else {
-      for (int e = threadIdx.x; e < E; e += NT) {
+      for (int e = tid; e < E; e += NT) {
         const float q = 1.f / (1.f + sden[e]);
         num[e] = make_float2(num[e].x * q, num[e].y * q);
       }
       __syncthreads();
     }
     // ------------------------------------------------------------ pass 2
-    for (int m = m0; m < m1; ++m) {
-      load_tile(m, false);
-      fft_any<NH>(buf + grp * Hs, P.ph, P.twH, t, g);
+    it = 0;
+    for (int m = m0; m < m1; ++m, ++it) {
+      float2* cur = stg + (size_t)(it & 1) * E;
+      if (m + 1 < m1) issue_tile(m + 1, stg + (size_t)((it + 1) & 1) * E);
+      cp_async_commit();
+      cp_async_wait<1>();
+      __syncthreads();
+      fft_any<NH, T>(cur + cc, P.ph, P.twH, t, g);
       const float2* Dm = P.Dh + (size_t)m * H * Wp + c0;
       const float wg = grd ? mu * P.wgrd[m] : 0.f;
-      for (int e = threadIdx.x; e < E; e += NT) {
-        const int kr = e / T, c = e - kr * T;
-        const int kc = c0 + c;
+      for (int e = tid; e < E; e += NT) {
+        const int kr = e / T;
         float2 xo = make_float2(0.f, 0.f);
-        if (kc < Wf) {
-          const float2 Dv = Dm[(size_t)kr * Wp + c];
-          const float2 Sv = Sh[(size_t)kr * Wp + c];
-          const float2 yu = buf[c * Hs + kr];
+        if (colok) {
+          const float2 Dv = __ldg(&Dm[(size_t)kr * Wp + cc]);
+          const float2 Sv = __ldg(&Sh[(size_t)kr * Wp + cc]);
+          const float2 yu = cur[e];
           const float2 bv = make_float2(Dv.x * Sv.x + Dv.y * Sv.y + rho * yu.x,
                                         Dv.x * Sv.y - Dv.y * Sv.x + rho * yu.y);
           float d = rho;
-          if (grd) {
-            const float gh = 4.f - 2.f * __ldg(&P.twW[kc]).x - 2.f * __ldg(&P.twH[kr]).x;
-            d = wg * gh + rho;
-          }
+          if (grd) d = wg * (gw_col + 2.f - 2.f * __ldg(&P.twH[kr]).x) + rho;
           const float id = 1.f / d;
-          const float2 cb = num[c * H + kr];
+          const float2 cb = num[e];
           // x = (b - conj(D) cb) / d
           xo.x = (bv.x - (Dv.x * cb.x + Dv.y * cb.y)) * id;
           xo.y = (bv.y - (Dv.x * cb.y - Dv.y * cb.x)) * id;
         }
-        buf[c * Hs + kr] = make_float2(xo.x, -xo.y);  // conj for the inverse
+        cur[e] = make_float2(xo.x, -xo.y);  // conj: inverse via forward FFT
       }
       __syncthreads();
-      fft_any<NH>(buf + grp * Hs, P.ph, P.twH, t, g);
-      store_tile(m, true);
+      fft_any<NH, T>(cur + cc, P.ph, P.twH, t, g);
+      float2* dst = Fi + (size_t)m * H * Wp + c0;
+      if (colok) {
+        for (int e = tid; e < E; e += NT) {
+          const int kr = e / T;
+          const float2 v = cur[e];
+          dst[(size_t)kr * Wp + cc] = make_float2(v.x, -v.y);
+        }
+      }
       __syncthreads();
     }
+    cp_async_wait<0>();
   }
 }
 
@@ -522,6 +620,9 @@ __global__ void finalize_kernel(const double* __restrict__ partials, int nblk,
   S.r = r; S.s = s; S.epri = epri; S.edua = edua;
   S.rho = rsf * rho;
   S.rsf = rsf;
+  // U as stored is the U of this iteration; the next row pass reads it scaled
+  // by 1/rsf (U <- U / rsf, cbpdn.cu:543-549)
+  S.uscale = 1.0 / rsf;
   S.k = k;
   bool done = (r <= epri && s <= edua) || k >= F.max_iter;
   if (!isfinite(r) || !isfinite(s)) {
@@ -541,6 +642,7 @@ __global__ void init_state_kernel(ImgState* st, const float* rho0, int B, int* n
   ImgState s;
   s.rho = (double)rho0[b];
   s.rsf = 1.0;
+  s.uscale = 1.0;
   s.r = s.s = s.epri = s.edua = 0.0;
   s.nX = s.nY = s.nU = 0.0;
   s.k = 0;

@@ -129,7 +129,7 @@ struct Plan {
   FftPlan pw, ph;
   // hot row kernels (iteration, fix-up): compile-time plan when available
   int row_g, row_nblk;
-  size_t row_smem;
+  size_t row_smem, row_smem_fix;
   // setup row kernels: runtime plan
   int rowg_g;
   size_t rowg_smem;
@@ -174,20 +174,20 @@ static int plan_geometry(int B, int M, int H, int W, Plan* pl) {
   long want = (npairs + S - 1) / S;
   long cap = std::max(1L, (long)num_sms() * 8 / B);
   pl->row_nblk = (int)std::min(want, cap);
-  pl->row_smem = (size_t)S * W * sizeof(float2);
+  pl->row_smem = (size_t)S * row_slot_bytes(ROW_ITER, W, g.Wp);
+  pl->row_smem_fix = (size_t)S * row_slot_bytes(ROW_FIXUP, W, g.Wp);
   pl->rowg_g = group_size(W);
-  pl->rowg_smem = (size_t)(SC_ROW_THREADS / pl->rowg_g) * W * sizeof(float2);
+  pl->rowg_smem = (size_t)(SC_ROW_THREADS / pl->rowg_g) * row_slot_bytes(ROW_FWD_REAL, W, g.Wp);
 
   pl->Hs = H + 1;
   pl->col_ntiles = (g.Wf + SC_COL_TILE - 1) / SC_COL_TILE;
   pl->col_g = spec_col(H) ? ct_threads(H) : group_size(H);
   pl->col_NT = SC_COL_TILE * pl->col_g;
   pl->col_G = std::min(8, M);
-  pl->col_smem = (size_t)SC_COL_TILE * pl->Hs * sizeof(float2) +
-                 (size_t)SC_COL_TILE * H * (sizeof(float2) + sizeof(float));
+  pl->col_smem = col_smem_bytes(COL_SOLVE, H);
   pl->colg_g = group_size(H);
   pl->colg_NT = SC_COL_TILE * pl->colg_g;
-  pl->colg_smem = (size_t)SC_COL_TILE * pl->Hs * sizeof(float2);
+  pl->colg_smem = col_smem_bytes(COL_FWD, H);
   return SC_OK;
 }
 
@@ -277,7 +277,9 @@ static int launch_row(const Plan& pl, RowParams rp, int B, cudaStream_t s, int n
   rp.gsz = hot ? pl.row_g : pl.rowg_g;
   rp.nblk = nblk > 0 ? nblk : pl.row_nblk;
   dim3 grid(rp.nblk, B);
-  fn<<<grid, SC_ROW_THREADS, hot ? pl.row_smem : pl.rowg_smem, s>>>(rp);
+  const size_t smem = MODE == ROW_ITER ? pl.row_smem
+                     : MODE == ROW_FIXUP ? pl.row_smem_fix : pl.rowg_smem;
+  fn<<<grid, SC_ROW_THREADS, smem, s>>>(rp);
   CU_TRY(cudaGetLastError());
   ++g_launches;
   return SC_OK;
@@ -382,6 +384,8 @@ extern "C" int sc_cbpdn_solve(const sc_problem* p, const sc_options* o, void* wo
     return set_status(SC_ERR_INVALID, "null device pointer");
   if (p->grd && !p->wgrd) return set_status(SC_ERR_INVALID, "grd problem without GradWeight");
   if (p->l1_kind != SC_L1_SCALAR && !p->l1w) return set_status(SC_ERR_INVALID, "missing L1Weight");
+  if ((p->W % 4) == 0 && (((uintptr_t)p->Y) & 15))
+    return set_status(SC_ERR_INVALID, "Y must be 16-byte aligned");
   cudaStream_t s = (cudaStream_t)stream;
   const Geom& g = pl.g;
 

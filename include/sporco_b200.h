@@ -145,6 +145,7 @@ typedef struct sc_problem {
   const float *l1w;      /* (M,) or (M, H, W) */
   const int32_t *mask;   /* (B, H, W) AMS mask, map 0 is the impulse; NULL: none */
   float *Y;              /* (B, M, H, W) output; also the Y iterate */
+  int wgrd_uniform;      /* grd only: 1 when all M GradWeight entries are equal */
 } sc_problem;
 
 typedef struct sc_result {

@@ -209,6 +209,9 @@ void run_compat(float* D, float* S, float lambda, float mu, void* vopt, float* Y
     }
     gwhost.resize(M);
     for (int m = 0; m < M; ++m) gwhost[m] = opt->GrdWeight ? opt->GrdWeight[nw == 1 ? 0 : m] : 1.f;
+    p.wgrd_uniform = 1;
+    for (int m = 1; m < M; ++m)
+      if (gwhost[m] != gwhost[0]) p.wgrd_uniform = 0;
   }
   const bool masked = opt->nWeight > 1 && opt->Weight;
   if (masked && opt->nWeight != H * W) {

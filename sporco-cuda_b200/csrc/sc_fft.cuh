@@ -132,6 +132,40 @@ __device__ __forceinline__ void dft8(float2* v) {
   v[7] = c_sub(e[3], o3);
 }
 
+// 16-point DFT as 4 x 4: DFT4 over the stride-4 subsequences, twiddles
+// w16^(n2 k1), DFT4 across them (X[k1 + 4 k2]).
+__device__ __forceinline__ void dft16(float2* v) {
+  const float c1 = 0.9238795325112867f;  // cos(pi/8)
+  const float s1 = 0.3826834323650898f;  // sin(pi/8)
+  const float r = 0.7071067811865476f;   // cos(pi/4)
+  float2 y[4][4];
+#pragma unroll
+  for (int n2 = 0; n2 < 4; ++n2) {
+    float2 a[4] = {v[n2], v[n2 + 4], v[n2 + 8], v[n2 + 12]};
+    dft4(a);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) y[n2][k1] = a[k1];
+  }
+  // w16^1 = (c1, -s1), w16^2 = (r, -r), w16^3 = (s1, -c1), w16^4 = -i,
+  // w16^6 = (-r, -r), w16^9 = (-c1, s1)
+  y[1][1] = c_mul(y[1][1], make_float2(c1, -s1));
+  y[1][2] = c_mul(y[1][2], make_float2(r, -r));
+  y[1][3] = c_mul(y[1][3], make_float2(s1, -c1));
+  y[2][1] = c_mul(y[2][1], make_float2(r, -r));
+  y[2][2] = c_mul_mi(y[2][2]);
+  y[2][3] = c_mul(y[2][3], make_float2(-r, -r));
+  y[3][1] = c_mul(y[3][1], make_float2(s1, -c1));
+  y[3][2] = c_mul(y[3][2], make_float2(-r, -r));
+  y[3][3] = c_mul(y[3][3], make_float2(-c1, s1));
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) {
+    float2 b[4] = {y[0][k1], y[1][k1], y[2][k1], y[3][k1]};
+    dft4(b);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = b[k2];
+  }
+}
+
 template <int R>
 __device__ __forceinline__ void dft_r(float2* v) {
   if constexpr (R == 2) dft2(v);
@@ -139,6 +173,46 @@ __device__ __forceinline__ void dft_r(float2* v) {
   else if constexpr (R == 4) dft4(v);
   else if constexpr (R == 5) dft5(v);
   else if constexpr (R == 8) dft8(v);
+  else if constexpr (R == 16) dft16(v);
+}
+
+// Multiply v[q] (q = 1..R-1) by w^q, w = tw[i1]: w, w^4 and w^8 come from the
+// table, the other powers are products of at most two factors.
+template <int R>
+__device__ __forceinline__ void twiddle_r(float2* v, const float2* __restrict__ tw, int i1) {
+  const float2 w1 = __ldg(&tw[i1]);
+  if constexpr (R == 2) {
+    v[1] = c_mul(v[1], w1);
+  } else if constexpr (R == 3) {
+    v[1] = c_mul(v[1], w1);
+    v[2] = c_mul(v[2], c_mul(w1, w1));
+  } else {
+    const float2 w2 = c_mul(w1, w1);
+    const float2 w3 = c_mul(w2, w1);
+    v[1] = c_mul(v[1], w1);
+    v[2] = c_mul(v[2], w2);
+    v[3] = c_mul(v[3], w3);
+    if constexpr (R == 5) {
+      v[4] = c_mul(v[4], c_mul(w2, w2));
+    } else if constexpr (R >= 8) {
+      const float2 w4 = __ldg(&tw[4 * i1]);
+      v[4] = c_mul(v[4], w4);
+#pragma unroll
+      for (int q = 1; q < 4; ++q) v[4 + q] = c_mul(v[4 + q], c_mul(w4, q == 1 ? w1 : q == 2 ? w2 : w3));
+      if constexpr (R == 16) {
+        const float2 w8 = __ldg(&tw[8 * i1]);
+        const float2 w12 = c_mul(w8, w4);
+        v[8] = c_mul(v[8], w8);
+        v[12] = c_mul(v[12], w12);
+#pragma unroll
+        for (int q = 1; q < 4; ++q) {
+          const float2 wq = q == 1 ? w1 : q == 2 ? w2 : w3;
+          v[8 + q] = c_mul(v[8 + q], c_mul(w8, wq));
+          v[12 + q] = c_mul(v[12 + q], c_mul(w12, wq));
+        }
+      }
+    }
+  }
 }
 
 // ------------------------------------------------------------------ passes --
@@ -261,15 +335,16 @@ struct CtPlan {
   int r[SC_FFT_MAX_PASS];
 };
 
-// Radix sequence: 8s, then one 4 or 2, then 3s, 5s, then other primes
-// (the same factorisation the runtime planner uses).
-__host__ __device__ constexpr CtPlan ct_plan(int n) {
+// Radix sequence for compile-time lengths: radix-RM passes (RM = 8 or 16),
+// then one smaller power of two, then 3s, 5s, then other primes.
+__host__ __device__ constexpr CtPlan ct_plan(int n, int RM) {
   CtPlan p{n, 0, {}};
   int m = n, a = 0;
   while (m % 2 == 0) { m /= 2; ++a; }
-  for (int i = 0; i < a / 3; ++i) p.r[p.np++] = 8;
-  if (a % 3 == 1) p.r[p.np++] = 2;
-  if (a % 3 == 2) p.r[p.np++] = 4;
+  const int lr = RM == 16 ? 4 : 3;
+  for (int i = 0; i < a / lr; ++i) p.r[p.np++] = RM;
+  const int rem = a % lr;
+  if (rem > 0) p.r[p.np++] = 1 << rem;
   while (m % 3 == 0) { m /= 3; p.r[p.np++] = 3; }
   while (m % 5 == 0) { m /= 5; p.r[p.np++] = 5; }
   for (int f = 7; m > 1 && p.np < SC_FFT_MAX_PASS; f += 2) {
@@ -290,13 +365,26 @@ __host__ __device__ constexpr int ct_pow2ceil(int x) {
   return p;
 }
 
-// Threads per transform for a compile-time length: about 8 elements each.
-__host__ __device__ constexpr int ct_threads(int n) {
-  int g = ct_pow2ceil((n + 7) / 8);
-  return g < 32 ? 32 : (g > 256 ? 256 : g);
+// Threads per transform for a compile-time length: RM elements each (one
+// radix-RM butterfly per pass), at least 8 threads.
+__host__ __device__ constexpr int ct_threads(int n, int RM) {
+  int g = (n + RM - 1) / RM;
+  return g < 8 ? 8 : g;
 }
 
-template <int N, int R, int NS, int G, int ST>
+// Shared-memory slot of element i of a compile-time transform: one pad slot
+// after every ct_pad elements (the first radix), which spreads the strided
+// stores of the first pass over all banks.
+__host__ __device__ constexpr int ct_pad(int n, int RM) { return ct_plan(n, RM).r[0]; }
+template <int N, int RM>
+__device__ __forceinline__ int ct_phys(int i) {
+  constexpr int P = ct_pad(N, RM);
+  return i + i / P;
+}
+// Padded length (elements) of a compile-time transform.
+__host__ __device__ constexpr int ct_padded(int n, int RM) { return n + n / ct_pad(n, RM); }
+
+template <int N, int RM, int R, int NS, int G, int ST>
 __device__ __forceinline__ void ct_pass(float2* data, const float2* __restrict__ tw, int t) {
   constexpr int B = N / R;
   constexpr int NB = (B + G - 1) / G;
@@ -307,12 +395,8 @@ __device__ __forceinline__ void ct_pass(float2* data, const float2* __restrict__
     const int j = t + i * G;
     if ((B % G) == 0 || j < B) {
 #pragma unroll
-      for (int q = 0; q < R; ++q) v[i][q] = data[(j + q * B) * ST];
-      if constexpr (NS > 1) {
-        const int k = j % NS;
-#pragma unroll
-        for (int q = 1; q < R; ++q) v[i][q] = c_mul(v[i][q], __ldg(&tw[q * k * STEP]));
-      }
+      for (int q = 0; q < R; ++q) v[i][q] = data[ct_phys<N, RM>(j + q * B) * ST];
+      if constexpr (NS > 1) twiddle_r<R>(v[i], tw, (j % NS) * STEP);
       dft_r<R>(v[i]);
     }
   }
@@ -324,38 +408,38 @@ __device__ __forceinline__ void ct_pass(float2* data, const float2* __restrict__
       const int k = j % NS;
       const int base = (j - k) * R + k;
 #pragma unroll
-      for (int q = 0; q < R; ++q) data[(base + q * NS) * ST] = v[i][q];
+      for (int q = 0; q < R; ++q) data[ct_phys<N, RM>(base + q * NS) * ST] = v[i][q];
     }
   }
   __syncthreads();
 }
 
-template <int N, int G, int ST, int P = 0>
+template <int N, int RM, int G, int ST, int P = 0>
 __device__ __forceinline__ void fft_ct(float2* data, const float2* __restrict__ tw, int t) {
-  constexpr CtPlan pl = ct_plan(N);
+  constexpr CtPlan pl = ct_plan(N, RM);
   if constexpr (P < pl.np) {
-    ct_pass<N, pl.r[P], ct_ns(pl, P), G, ST>(data, tw, t);
-    fft_ct<N, G, ST, P + 1>(data, tw, t);
+    ct_pass<N, RM, pl.r[P], ct_ns(pl, P), G, ST>(data, tw, t);
+    fft_ct<N, RM, G, ST, P + 1>(data, tw, t);
   }
 }
 
-// True when every radix of n has a hand-written butterfly.
-__host__ __device__ constexpr bool ct_fast_radices(int n) {
-  CtPlan p = ct_plan(n);
-  for (int i = 0; i < p.np; ++i)
-    if (p.r[i] != 2 && p.r[i] != 3 && p.r[i] != 4 && p.r[i] != 5 && p.r[i] != 8) return false;
-  return true;
-}
-
-// Forward DFT of length N of the elements data[0], data[ST], ...
-// (N > 0: compile-time plan; N == 0: runtime plan P with g threads and
-// stride ST).
-template <int N, int ST>
+// Forward DFT of length N of the elements of one transform (N > 0:
+// compile-time plan with radix-RM passes, element i at
+// data[ct_phys<N, RM>(i) * ST]; N == 0: runtime plan P with g threads,
+// element i at data[i * ST]).
+template <int N, int ST, int RM>
 __device__ __forceinline__ void fft_any(float2* data, const FftPlan& P,
                                         const float2* __restrict__ tw, int t, int g) {
   if constexpr (N == 0) {
     fft_forward<16>(data, P, ST, tw, t, g);
   } else {
-    fft_ct<N, ct_threads(N), ST>(data, tw, t);
+    fft_ct<N, RM, ct_threads(N, RM), ST>(data, tw, t);
   }
+}
+
+// Element index -> shared-memory slot for either path.
+template <int N, int RM>
+__device__ __forceinline__ int fft_slot(int i) {
+  if constexpr (N == 0) return i;
+  else return ct_phys<N, RM>(i);
 }

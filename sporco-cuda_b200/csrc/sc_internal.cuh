@@ -13,7 +13,12 @@
 // Image columns (spectrum columns) per column-pass CTA.
 #define SC_COL_TILE 4
 // Largest column-pass CTA (SC_COL_TILE transforms of length <= 2048).
-#define SC_COL_MAX_THREADS 1024
+#define SC_COL_MAX_THREADS 512
+// Largest radix of the compile-time FFT plans of the row and column passes.
+#define SC_ROW_RADIX 8
+// Column pass: radix-16 plans (16 elements per thread) for long columns,
+// radix-8 plans (8 per thread, twice the threads) for short ones.
+__host__ __device__ constexpr int col_radix(int H) { return H >= 512 ? 16 : 8; }
 // Largest transform length this build supports along a row or a column.
 #define SC_MAX_N 4096
 
@@ -91,28 +96,33 @@ struct ColParams {
   int grd;
   float mu;
   const float* wgrd;       // (M,)
+  const float* Psum;       // (H, Wp) sum_m |Df_m|^2 (solve with one d for all maps)
   ImgState* st;
 };
 
 enum RowMode { ROW_ITER = 0, ROW_FWD_REAL = 1, ROW_FWD_DICT = 2, ROW_INV_REAL = 3, ROW_FIXUP = 4 };
-enum ColMode { COL_SOLVE = 0, COL_FWD = 1, COL_INV = 2 };
+// COL_SOLVE: all maps share d (cbpdn, or cbpdngrd with one GradWeight), so
+// sum_m |Df_m|^2 / d comes from the precomputed Psum; COL_SOLVE_W: per-map
+// d_m = mu w_m |G|^2 + rho, the sum is accumulated over the maps.
+enum ColMode { COL_SOLVE = 0, COL_FWD = 1, COL_INV = 2, COL_SOLVE_W = 3 };
 
 __host__ __device__ inline size_t sc_align16(size_t x) { return (x + 15) & ~(size_t)15; }
 
-// Shared memory of one row-pass slot (one row pair in flight).  The
+// Shared memory of one row-pass slot (one row pair in flight); zlen is the
+// (padded) number of shared-memory slots of one row transform.  The
 // iteration mode double-buffers the pair's two spectrum rows and stages the
-// pair's Y and U rows: [z: W complex][F: 2 x 2Wp complex][Y: 2W][U: 2W].
-__host__ __device__ inline size_t row_slot_bytes(int mode, int W, int Wp) {
-  size_t z = sc_align16((size_t)W * 8);
+// pair's Y and U rows: [z: zlen complex][F: 2 x 2Wp complex][Y: 2W][U: 2W].
+__host__ __device__ inline size_t row_slot_bytes(int mode, int zlen, int W, int Wp) {
+  size_t z = sc_align16((size_t)zlen * 8);
   if (mode != ROW_ITER) return z;
   return z + 2 * (size_t)(2 * Wp) * 8 + 2 * sc_align16((size_t)(2 * W) * 4);
 }
 
-// Shared memory of one column-pass CTA: the solve double-buffers the tile
-// (SC_COL_TILE interleaved columns of H complex) and accumulates
-// sum_m Df b / d (complex) and sum_m |Df|^2 / d (real) per tile element.
-__host__ __device__ inline size_t col_smem_bytes(int mode, int H) {
-  const size_t tile = (size_t)SC_COL_TILE * H * 8;
-  if (mode != COL_SOLVE) return tile;
-  return 2 * tile + (size_t)SC_COL_TILE * H * 12;
+// Shared memory of one column-pass CTA; hlen is the (padded) number of
+// shared-memory slots of one column transform.  A tile is SC_COL_TILE
+// interleaved columns.  The solve double-buffers the spectrum tile and stages
+// the dictionary tile: [F0][F1][D]; the cluster reduction reuses [F1][D].
+__host__ __device__ inline size_t col_smem_bytes(int mode, int hlen) {
+  const size_t tile = (size_t)SC_COL_TILE * hlen * 8;
+  return (mode == COL_SOLVE || mode == COL_SOLVE_W) ? 3 * tile : tile;
 }

@@ -125,12 +125,15 @@ row_kernel(RowParams P) {
   const Geom& G = P.g;
   const int b = blockIdx.y;
   const int W = G.W, Wf = G.Wf, Wp = G.Wp, H = G.H;
-  const int g = NW > 0 ? ct_threads(NW) : P.gsz;
+  constexpr int RM = SC_ROW_RADIX;
+  const int g = NW > 0 ? ct_threads(NW, RM) : P.gsz;
   const int S = blockDim.x / g;
   const int s = threadIdx.x / g;
   const int t = threadIdx.x - s * g;
-  unsigned char* slot = smem_raw + (size_t)s * row_slot_bytes(MODE, W, Wp);
+  const int zlen = NW > 0 ? ct_padded(NW, RM) : W;
+  unsigned char* slot = smem_raw + (size_t)s * row_slot_bytes(MODE, zlen, W, Wp);
   float2* z = reinterpret_cast<float2*>(slot);
+  auto zs = [](int k) { return fft_slot<NW, RM>(k); };
 
   float thr = 0.f, rsf_c = 0.f, uscale = 1.f;
   if constexpr (MODE == ROW_ITER || MODE == ROW_FIXUP) {
@@ -154,7 +157,7 @@ row_kernel(RowParams P) {
 
   if constexpr (MODE == ROW_ITER) {
     // --------------------------------------------------------- iteration
-    float2* fst = reinterpret_cast<float2*>(slot + sc_align16((size_t)W * 8));
+    float2* fst = reinterpret_cast<float2*>(slot + sc_align16((size_t)zlen * 8));
     float* ysm = reinterpret_cast<float*>(fst + 2 * 2 * (size_t)Wp);
     float* usm = ysm + sc_align16((size_t)(2 * W) * 4) / 4;
     const float* Yi = P.Y + (size_t)b * img_real;
@@ -210,10 +213,10 @@ row_kernel(RowParams P) {
       __syncthreads();
       if (valid) {
         const float2* fa = fst + (it & 1) * 2 * Wp;
-        for (int k = t; k < W; k += g) z[k] = pack_inverse(fa, fa + Wp, has1, k, W, Wf);
+        for (int k = t; k < W; k += g) z[zs(k)] = pack_inverse(fa, fa + Wp, has1, k, W, Wf);
       }
       __syncthreads();
-      fft_any<NW, 1>(z, P.pw, P.twW, t, g);
+      fft_any<NW, 1, RM>(z, P.pw, P.twW, t, g);
       cp_async_wait<1>();
       __syncthreads();
       if (valid) {
@@ -227,7 +230,7 @@ row_kernel(RowParams P) {
         const float* wr1 = (P.l1_kind == 2 && has1) ? P.l1w + ((size_t)m1 * H + h1) * W : nullptr;
         const bool ams0 = mk && m0 == 0, ams1 = mk && m1 == 0;
         for (int k = t; k < W; k += g) {
-          const float2 zz = z[k];
+          const float2 zz = z[zs(k)];
           float yu0, yu1 = 0.f;
           {
             const float x = zz.x * P.invN;
@@ -267,16 +270,16 @@ row_kernel(RowParams P) {
             acc[3] += (double)(dxy * dxy);
             acc[4] += (double)(dyy * dyy);
           }
-          z[k] = make_float2(yu0, yu1);
+          z[zs(k)] = make_float2(yu0, yu1);
         }
       }
       __syncthreads();
-      fft_any<NW, 1>(z, P.pw, P.twW, t, g);
+      fft_any<NW, 1, RM>(z, P.pw, P.twW, t, g);
       if (valid) {
         float2* fa = Fi + r0 * Wp;
         for (int k = t; k < Wf; k += g) {
-          const float2 Zk = z[k];
-          const float2 Zm = z[k == 0 ? 0 : W - k];
+          const float2 Zk = z[zs(k)];
+          const float2 Zm = z[zs(k == 0 ? 0 : W - k)];
           // A = (Z_k + conj Z_{-k}) / 2 ;  B = (Z_k - conj Z_{-k}) / (2i)
           fa[k] = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
           if (has1) fa[Wp + k] = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
@@ -302,14 +305,14 @@ row_kernel(RowParams P) {
       if constexpr (MODE == ROW_INV_REAL) {
         if (valid) {
           const float2* a = Fi + r0 * Wp;
-          for (int k = t; k < W; k += g) z[k] = pack_inverse(a, a + Wp, has1, k, W, Wf);
+          for (int k = t; k < W; k += g) z[zs(k)] = pack_inverse(a, a + Wp, has1, k, W, Wf);
         }
         __syncthreads();
-        fft_any<NW, 1>(z, P.pw, P.twW, t, g);
+        fft_any<NW, 1, RM>(z, P.pw, P.twW, t, g);
         if (valid) {
           float* d0 = P.dst + (size_t)b * img_real + (size_t)r0 * W;
           for (int k = t; k < W; k += g) {
-            const float2 zz = z[k];
+            const float2 zz = z[zs(k)];
             d0[k] = zz.x * P.invN;
             if (has1) d0[W + k] = -zz.y * P.invN;
           }
@@ -320,7 +323,7 @@ row_kernel(RowParams P) {
       if (valid) {
         if constexpr (MODE == ROW_FWD_REAL) {
           const float* s0 = P.src + (size_t)b * img_real + (size_t)r0 * W;
-          for (int k = t; k < W; k += g) z[k] = make_float2(s0[k], has1 ? s0[W + k] : 0.f);
+          for (int k = t; k < W; k += g) z[zs(k)] = make_float2(s0[k], has1 ? s0[W + k] : 0.f);
         } else if constexpr (MODE == ROW_FWD_DICT) {
           const int m0 = (int)(r0 / H), h0 = (int)(r0 - (long)m0 * H);
           const int m1 = (int)(r1 / H), h1 = (int)(r1 - (long)m1 * H);
@@ -328,21 +331,21 @@ row_kernel(RowParams P) {
             float v0 = 0.f, v1 = 0.f;
             if (h0 < P.Kr && k < P.Kc) v0 = P.D[((size_t)m0 * P.Kr + h0) * P.Kc + k];
             if (has1 && h1 < P.Kr && k < P.Kc) v1 = P.D[((size_t)m1 * P.Kr + h1) * P.Kc + k];
-            z[k] = make_float2(v0, v1);
+            z[zs(k)] = make_float2(v0, v1);
           }
         } else if constexpr (MODE == ROW_FIXUP) {
           const float* U0 = P.U + (size_t)b * img_real + (size_t)r0 * W;
-          for (int k = t; k < W; k += g) z[k] = make_float2(U0[k], has1 ? U0[W + k] : 0.f);
+          for (int k = t; k < W; k += g) z[zs(k)] = make_float2(U0[k], has1 ? U0[W + k] : 0.f);
         }
       }
       __syncthreads();
-      fft_any<NW, 1>(z, P.pw, P.twW, t, g);
+      fft_any<NW, 1, RM>(z, P.pw, P.twW, t, g);
       if (valid) {
         float2* a = Fi + r0 * Wp;
         float2* bb = Fi + r1 * Wp;
         for (int k = t; k < Wf; k += g) {
-          const float2 Zk = z[k];
-          const float2 Zm = z[k == 0 ? 0 : W - k];
+          const float2 Zk = z[zs(k)];
+          const float2 Zm = z[zs(k == 0 ? 0 : W - k)];
           const float2 A = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
           const float2 Bv = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
           if constexpr (MODE == ROW_FIXUP) {
@@ -367,31 +370,35 @@ row_kernel(RowParams P) {
 // Grid (G, ntiles, B).  For COL_SOLVE the G CTAs of one column tile form a
 // thread-block cluster; each handles a contiguous chunk of the maps.  Tiles
 // keep their HBM layout in shared memory: element (kr, c) of the tile at
-// [kr * T + c]; thread tid works on column c = tid % T.
+// [slot(kr) * T + c]; thread tid works on column c = tid % T and, in the
+// element loops, on rows kr = tid / T + i g.
 template <int MODE, int NH>
-__global__ void __launch_bounds__(NH > 1024 ? SC_COL_MAX_THREADS : SC_COL_MAX_THREADS / 2)
+__global__ void __launch_bounds__(SC_COL_MAX_THREADS)
 col_kernel(ColParams P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int T = SC_COL_TILE;
+  constexpr int RM = col_radix(NH);
+  // elements of the tile per thread (compile-time bound)
+  constexpr int EPT = NH > 0 ? (NH + ct_threads(NH, RM) - 1) / ct_threads(NH, RM) : SC_MAXE;
   const Geom& G = P.g;
   const int H = G.H, Wf = G.Wf, Wp = G.Wp, M = G.M;
-  const int E = T * H;
-  float2* stg = reinterpret_cast<float2*>(smem_raw);     // [2][E] (solve) / [E]
-  float2* num = stg + 2 * (size_t)E;                      // [E] (solve)
-  float* sden = reinterpret_cast<float*>(num + E);        // [E] (solve)
+  const int hlen = NH > 0 ? ct_padded(NH, RM) : H;
+  const int TL = T * hlen;  // shared-memory slots of one tile
+  float2* stg = reinterpret_cast<float2*>(smem_raw);  // [F0][F1][D]
 
   const int b = blockIdx.z;
   const int tile = blockIdx.y;
   const int rank = blockIdx.x;
   const int c0 = tile * T;
-  const int g = NH > 0 ? ct_threads(NH) : P.gsz;
+  const int g = NH > 0 ? ct_threads(NH, RM) : P.gsz;
   const int NT = blockDim.x;
   const int tid = threadIdx.x;
   const int cc = tid % T;   // column of this thread (T divides NT)
   const int t = tid / T;    // index within the column's thread group
+  auto slot = [](int kr) { return fft_slot<NH, RM>(kr); };
 
   float rho = 0.f;
-  if constexpr (MODE == COL_SOLVE) {
+  if constexpr (MODE == COL_SOLVE || MODE == COL_SOLVE_W) {
     const ImgState& st = P.st[b];
     if (st.done) return;  // uniform over the cluster (same image)
     rho = (float)st.rho;
@@ -407,19 +414,19 @@ col_kernel(ColParams P) {
     const bool inv = MODE == COL_INV;
     for (int m = m0; m < m1; ++m) {
       float2* src = Fi + (size_t)m * H * Wp + c0;
-      for (int e = tid; e < E; e += NT) {
+      for (int e = tid; e < T * H; e += NT) {
         const int kr = e / T, c = e - kr * T;
         float2 v = make_float2(0.f, 0.f);
         if (c0 + c < Wf) v = src[(size_t)kr * Wp + c];
         if (inv) v.y = -v.y;
-        stg[e] = v;
+        stg[slot(kr) * T + c] = v;
       }
       __syncthreads();
-      fft_any<NH, T>(stg + cc, P.ph, P.twH, t, g);
-      for (int e = tid; e < E; e += NT) {
+      fft_any<NH, T, RM>(stg + cc, P.ph, P.twH, t, g);
+      for (int e = tid; e < T * H; e += NT) {
         const int kr = e / T, c = e - kr * T;
         if (c0 + c < Wf) {
-          float2 v = stg[e];
+          float2 v = stg[slot(kr) * T + c];
           if (inv) v.y = -v.y;
           src[(size_t)kr * Wp + c] = v;
         }
@@ -428,12 +435,14 @@ col_kernel(ColParams P) {
     }
     return;
   } else {
-    // tile row (kr, 0..3) is 32 contiguous bytes: two 16-byte async copies
-    auto issue_tile = [&](int m, float2* dst) {
-      const float2* src = Fi + (size_t)m * H * Wp + c0;
+    constexpr bool SDEN = MODE == COL_SOLVE_W;  // accumulate sum |Df|^2 / d_m
+    float2* fbuf[2] = {stg, stg + TL};
+    float2* dbuf = stg + 2 * TL;
+    // tile row kr (4 complex = 32 contiguous bytes): two 16-byte async copies
+    auto issue_tile = [&](const float2* base, float2* dst) {
       for (int q = tid; q < 2 * H; q += NT) {
         const int kr = q >> 1, h = q & 1;
-        cp_async16(dst + kr * T + 2 * h, src + (size_t)kr * Wp + 2 * h);
+        cp_async16(dst + slot(kr) * T + 2 * h, base + (size_t)kr * Wp + c0 + 2 * h);
       }
     };
     const float2* Sh = P.Sh + (size_t)b * H * Wp + c0;
@@ -442,49 +451,94 @@ col_kernel(ColParams P) {
     const int kc = c0 + cc;
     const bool colok = kc < Wf;
     const float gw_col = grd && colok ? 2.f - 2.f * __ldg(&P.twW[kc]).x : 0.f;
+    const float irho = 1.f / rho;
+    // 1/d for map m, row kr (d = rho, or mu w_m |G(kr, kc)|^2 + rho)
+    auto inv_d = [&](float wg, int kr) -> float {
+      if (!grd) return irho;
+      return 1.f / (wg * (gw_col + 2.f - 2.f * __ldg(&P.twH[kr]).x) + rho);
+    };
 
-    // ------------------------------------------------------------ pass 1
-    for (int e = tid; e < E; e += NT) {
-      num[e] = make_float2(0.f, 0.f);
-      sden[e] = 0.f;
-    }
-    if (m0 < m1) issue_tile(m0, stg);
+    // ---------------------------------------------------------------- pass 1
+    // forward column FFT of the row spectra of Y - U; accumulate
+    // num = sum_m Df b / d (and sum_m |Df|^2 / d for per-map d); write the
+    // column-transformed (Y - U)^ back in place for pass 2.
+    float2 num[EPT];
+    float sden[SDEN ? EPT : 1];
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) num[i] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int i = 0; i < (SDEN ? EPT : 1); ++i) sden[i] = 0.f;
+    if (m0 < m1) issue_tile(Fi + (size_t)m0 * H * Wp, fbuf[0]);
     cp_async_commit();
     int it = 0;
     for (int m = m0; m < m1; ++m, ++it) {
-      float2* cur = stg + (size_t)(it & 1) * E;
-      if (m + 1 < m1) issue_tile(m + 1, stg + (size_t)((it + 1) & 1) * E);
+      float2* cur = fbuf[it & 1];
+      issue_tile(P.Dh + (size_t)m * H * Wp, dbuf);
       cp_async_commit();
+      if (m + 1 < m1) issue_tile(Fi + (size_t)(m + 1) * H * Wp, fbuf[(it + 1) & 1]);
+      cp_async_commit();
+      cp_async_wait<2>();
+      __syncthreads();
+      fft_any<NH, T, RM>(cur + cc, P.ph, P.twH, t, g);
       cp_async_wait<1>();
       __syncthreads();
-      fft_any<NH, T>(cur + cc, P.ph, P.twH, t, g);
-      const float2* Dm = P.Dh + (size_t)m * H * Wp + c0;
       const float wg = grd ? mu * P.wgrd[m] : 0.f;
+      float2* fout = Fi + (size_t)m * H * Wp + c0;
       if (colok) {
-        for (int e = tid; e < E; e += NT) {
-          const int kr = e / T;
-          const float2 Dv = __ldg(&Dm[(size_t)kr * Wp + cc]);
-          const float2 Sv = __ldg(&Sh[(size_t)kr * Wp + cc]);
-          const float2 yu = cur[e];
-          // b = conj(D) S + rho (Y - U)^
-          const float2 bv = make_float2(Dv.x * Sv.x + Dv.y * Sv.y + rho * yu.x,
-                                        Dv.x * Sv.y - Dv.y * Sv.x + rho * yu.y);
-          float d = rho;
-          if (grd) d = wg * (gw_col + 2.f - 2.f * __ldg(&P.twH[kr]).x) + rho;
-          const float id = 1.f / d;
-          float2 nv = num[e];
-          nv.x += (Dv.x * bv.x - Dv.y * bv.y) * id;
-          nv.y += (Dv.x * bv.y + Dv.y * bv.x) * id;
-          num[e] = nv;
-          sden[e] += (Dv.x * Dv.x + Dv.y * Dv.y) * id;
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+          const int kr = t + i * g;
+          if (kr < H) {
+            const int sl = slot(kr) * T + cc;
+            const float2 Dv = dbuf[sl];
+            const float2 Sv = __ldg(&Sh[(size_t)kr * Wp + cc]);
+            const float2 yu = cur[sl];
+            fout[(size_t)kr * Wp + cc] = yu;
+            // b = conj(D) S + rho (Y - U)^
+            const float2 bv = make_float2(Dv.x * Sv.x + Dv.y * Sv.y + rho * yu.x,
+                                          Dv.x * Sv.y - Dv.y * Sv.x + rho * yu.y);
+            const float id = inv_d(wg, kr);
+            num[i].x += (Dv.x * bv.x - Dv.y * bv.y) * id;
+            num[i].y += (Dv.x * bv.y + Dv.y * bv.x) * id;
+            if constexpr (SDEN) sden[i] += (Dv.x * Dv.x + Dv.y * Dv.y) * id;
+          }
         }
       }
       __syncthreads();
     }
-    // prefetch the first tile of pass 2 while the maps are reduced
-    if (m0 < m1) issue_tile(m0, stg);
+    // prefetch the first tile of pass 2 into F0 while [F1][D] hosts the
+    // reduction over the maps
+    if (m0 < m1) issue_tile(Fi + (size_t)m0 * H * Wp, fbuf[0]);
     cp_async_commit();
     // ------------------------------------------------- reduce over the maps
+    // cb = sum_m Df b / d / (1 + sum_m |Df|^2 / d)
+    const int E = T * H;
+    float2* xn = fbuf[1];                                  // [E] complex
+    float* xd = reinterpret_cast<float*>(xn + E);          // [E] real
+    // sum_m |Df_m|^2 / d_m at tile element (kr, c): accumulated (per-map d)
+    // or, with one d for all maps, Psum / d
+    auto denom = [&](int kr, int c, float ds) -> float {
+      if constexpr (SDEN) {
+        return ds;
+      } else {
+        const int k = c0 + c;
+        if (k >= Wf) return 0.f;
+        float id = irho;
+        if (grd) {
+          const float gwc = 2.f - 2.f * __ldg(&P.twW[k]).x;
+          id = 1.f / (mu * P.wgrd[0] * (gwc + 2.f - 2.f * __ldg(&P.twH[kr]).x) + rho);
+        }
+        return __ldg(&P.Psum[(size_t)kr * Wp + k]) * id;
+      }
+    };
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) {
+      const int kr = t + i * g;
+      if (kr < H) {
+        xn[kr * T + cc] = num[i];
+        if constexpr (SDEN) xd[kr * T + cc] = sden[i];
+      }
+    }
     if (P.G > 1) {
       cg::cluster_group cluster = cg::this_cluster();
       cluster.sync();
@@ -494,73 +548,97 @@ col_kernel(ColParams P) {
         float2 ns = make_float2(0.f, 0.f);
         float ds = 0.f;
         for (int r = 0; r < P.G; ++r) {
-          const float2* rn = cluster.map_shared_rank(num, r);
-          const float* rd = cluster.map_shared_rank(sden, r);
-          const float2 v = rn[e];
+          const float2 v = cluster.map_shared_rank(xn, r)[e];
           ns.x += v.x;
           ns.y += v.y;
-          ds += rd[e];
+          if constexpr (SDEN) ds += cluster.map_shared_rank(xd, r)[e];
         }
-        const float q = 1.f / (1.f + ds);
-        num[e] = make_float2(ns.x * q, ns.y * q);
+        const float q = 1.f / (1.f + denom(e / T, e % T, ds));
+        xn[e] = make_float2(ns.x * q, ns.y * q);
       }
       cluster.sync();
-      for (int e = tid; e < E; e += NT) {
-        const int owner = e / sl;
-        if (owner != rank) num[e] = cluster.map_shared_rank(num, owner)[e];
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        const int kr = t + i * g;
+        if (kr < H) {
+          const int e = kr * T + cc;
+          const int owner = e / sl;
+          num[i] = owner == rank ? xn[e] : cluster.map_shared_rank(xn, owner)[e];
+        }
       }
       cluster.sync();
     } else {
-      for (int e = tid; e < E; e += NT) {
-        const float q = 1.f / (1.f + sden[e]);
-        num[e] = make_float2(num[e].x * q, num[e].y * q);
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        const int kr = t + i * g;
+        const float q = 1.f / (1.f + denom(kr, cc, SDEN ? sden[SDEN ? i : 0] : 0.f));
+        num[i] = make_float2(num[i].x * q, num[i].y * q);
       }
       __syncthreads();
     }
-    // ------------------------------------------------------------ pass 2
+    // num[i] now holds cb for this thread's elements
+    // ---------------------------------------------------------------- pass 2
+    // x = (b - conj(Df) cb) / d from the stored (Y - U)^, inverse column FFT
     it = 0;
     for (int m = m0; m < m1; ++m, ++it) {
-      float2* cur = stg + (size_t)(it & 1) * E;
-      if (m + 1 < m1) issue_tile(m + 1, stg + (size_t)((it + 1) & 1) * E);
+      float2* cur = fbuf[it & 1];
+      issue_tile(P.Dh + (size_t)m * H * Wp, dbuf);
+      cp_async_commit();
+      if (m + 1 < m1) issue_tile(Fi + (size_t)(m + 1) * H * Wp, fbuf[(it + 1) & 1]);
       cp_async_commit();
       cp_async_wait<1>();
       __syncthreads();
-      fft_any<NH, T>(cur + cc, P.ph, P.twH, t, g);
-      const float2* Dm = P.Dh + (size_t)m * H * Wp + c0;
       const float wg = grd ? mu * P.wgrd[m] : 0.f;
-      for (int e = tid; e < E; e += NT) {
-        const int kr = e / T;
-        float2 xo = make_float2(0.f, 0.f);
-        if (colok) {
-          const float2 Dv = __ldg(&Dm[(size_t)kr * Wp + cc]);
-          const float2 Sv = __ldg(&Sh[(size_t)kr * Wp + cc]);
-          const float2 yu = cur[e];
-          const float2 bv = make_float2(Dv.x * Sv.x + Dv.y * Sv.y + rho * yu.x,
-                                        Dv.x * Sv.y - Dv.y * Sv.x + rho * yu.y);
-          float d = rho;
-          if (grd) d = wg * (gw_col + 2.f - 2.f * __ldg(&P.twH[kr]).x) + rho;
-          const float id = 1.f / d;
-          const float2 cb = num[e];
-          // x = (b - conj(D) cb) / d
-          xo.x = (bv.x - (Dv.x * cb.x + Dv.y * cb.y)) * id;
-          xo.y = (bv.y - (Dv.x * cb.y - Dv.y * cb.x)) * id;
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        const int kr = t + i * g;
+        if (kr < H) {
+          const int sl = slot(kr) * T + cc;
+          float2 xo = make_float2(0.f, 0.f);
+          if (colok) {
+            const float2 Dv = dbuf[sl];
+            const float2 Sv = __ldg(&Sh[(size_t)kr * Wp + cc]);
+            const float2 yu = cur[sl];
+            const float2 bv = make_float2(Dv.x * Sv.x + Dv.y * Sv.y + rho * yu.x,
+                                          Dv.x * Sv.y - Dv.y * Sv.x + rho * yu.y);
+            const float id = inv_d(wg, kr);
+            const float2 cb = num[i];
+            xo.x = (bv.x - (Dv.x * cb.x + Dv.y * cb.y)) * id;
+            xo.y = (bv.y - (Dv.x * cb.y - Dv.y * cb.x)) * id;
+          }
+          cur[sl] = make_float2(xo.x, -xo.y);  // conj: inverse via forward FFT
         }
-        cur[e] = make_float2(xo.x, -xo.y);  // conj: inverse via forward FFT
       }
       __syncthreads();
-      fft_any<NH, T>(cur + cc, P.ph, P.twH, t, g);
+      fft_any<NH, T, RM>(cur + cc, P.ph, P.twH, t, g);
       float2* dst = Fi + (size_t)m * H * Wp + c0;
       if (colok) {
-        for (int e = tid; e < E; e += NT) {
-          const int kr = e / T;
-          const float2 v = cur[e];
-          dst[(size_t)kr * Wp + cc] = make_float2(v.x, -v.y);
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+          const int kr = t + i * g;
+          if (kr < H) {
+            const float2 v = cur[slot(kr) * T + cc];
+            dst[(size_t)kr * Wp + cc] = make_float2(v.x, -v.y);
+          }
         }
       }
       __syncthreads();
     }
     cp_async_wait<0>();
   }
+}
+
+// Sum over the maps of |Df_m|^2 for every frequency (setup of COL_SOLVE).
+__global__ void psum_kernel(const float2* __restrict__ Dh, float* __restrict__ Psum, int M,
+                            size_t plane) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= plane) return;
+  float s = 0.f;
+  for (int m = 0; m < M; ++m) {
+    const float2 d = __ldg(&Dh[(size_t)m * plane + i]);
+    s += d.x * d.x + d.y * d.y;
+  }
+  Psum[i] = s;
 }
 
 // ============================================================== finalize ==

@@ -109,7 +109,7 @@ static int group_size(int n) {
 }
 
 // Transform lengths with compile-time FFT plans (all benchmark sizes).
-#define SC_SPEC_ROW(X) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096) \
+#define SC_SPEC_ROW(X) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) \
   X(48) X(96) X(192) X(384) X(768) X(1536)
 #define SC_SPEC_COL(X) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) \
   X(48) X(96) X(192) X(384) X(768) X(1536)
@@ -139,7 +139,7 @@ struct Plan {
   int colg_g, colg_NT;
   size_t colg_smem;
   int max_iter;
-  size_t off_U, off_F, off_Dh, off_Sh, off_twW, off_twH, off_part, off_st, off_it,
+  size_t off_U, off_F, off_Dh, off_Sh, off_Ps, off_twW, off_twH, off_part, off_st, off_it,
       off_xi, off_ndone, total;
 };
 
@@ -167,24 +167,26 @@ static int plan_geometry(int B, int M, int H, int W, Plan* pl) {
   g.Wp = (g.Wf + 3) & ~3;
   if (make_fft_plan(W, &pl->pw) || make_fft_plan(H, &pl->ph))
     return set_status(SC_ERR_UNSUPPORTED, "cannot factor %d or %d", W, H);
-  pl->row_g = spec_row(W) ? ct_threads(W) : group_size(W);
+  const bool srow = spec_row(W), scol = spec_col(H);
+  const int zlen = srow ? ct_padded(W, SC_ROW_RADIX) : W;
+  pl->row_g = srow ? ct_threads(W, SC_ROW_RADIX) : group_size(W);
   const int S = SC_ROW_THREADS / pl->row_g;
   const long rows = (long)M * H;
   const long npairs = (rows + 1) / 2;
   long want = (npairs + S - 1) / S;
   long cap = std::max(1L, (long)num_sms() * 8 / B);
   pl->row_nblk = (int)std::min(want, cap);
-  pl->row_smem = (size_t)S * row_slot_bytes(ROW_ITER, W, g.Wp);
-  pl->row_smem_fix = (size_t)S * row_slot_bytes(ROW_FIXUP, W, g.Wp);
+  pl->row_smem = (size_t)S * row_slot_bytes(ROW_ITER, zlen, W, g.Wp);
+  pl->row_smem_fix = (size_t)S * row_slot_bytes(ROW_FIXUP, zlen, W, g.Wp);
   pl->rowg_g = group_size(W);
-  pl->rowg_smem = (size_t)(SC_ROW_THREADS / pl->rowg_g) * row_slot_bytes(ROW_FWD_REAL, W, g.Wp);
+  pl->rowg_smem = (size_t)(SC_ROW_THREADS / pl->rowg_g) * row_slot_bytes(ROW_FWD_REAL, W, W, g.Wp);
 
   pl->Hs = H + 1;
   pl->col_ntiles = (g.Wf + SC_COL_TILE - 1) / SC_COL_TILE;
-  pl->col_g = spec_col(H) ? ct_threads(H) : group_size(H);
+  pl->col_g = scol ? ct_threads(H, col_radix(H)) : group_size(H);
   pl->col_NT = SC_COL_TILE * pl->col_g;
   pl->col_G = std::min(8, M);
-  pl->col_smem = col_smem_bytes(COL_SOLVE, H);
+  pl->col_smem = col_smem_bytes(COL_SOLVE, scol ? ct_padded(H, col_radix(H)) : H);
   pl->colg_g = group_size(H);
   pl->colg_NT = SC_COL_TILE * pl->colg_g;
   pl->colg_smem = col_smem_bytes(COL_FWD, H);
@@ -208,6 +210,7 @@ static int plan_problem(const sc_problem* p, const sc_options* o, Plan* pl) {
   pl->off_F = take(sizeof(float2) * spec_img * g.B);
   pl->off_Dh = take(sizeof(float2) * spec_img);
   pl->off_Sh = take(sizeof(float2) * (size_t)g.H * g.Wp * g.B);
+  pl->off_Ps = take(sizeof(float) * (size_t)g.H * g.Wp);
   pl->off_twW = take(sizeof(float2) * g.W);
   pl->off_twH = take(sizeof(float2) * g.H);
   pl->off_part = take(sizeof(double) * 5 * (size_t)pl->row_nblk * g.B);
@@ -242,7 +245,7 @@ static RowFn row_fn(int W) {
 template <int MODE>
 static ColFn col_fn(int H) {
 #define SC_COL_CASE(n) case n: return col_kernel<MODE, n>;
-  if constexpr (MODE == COL_SOLVE) {
+  if constexpr (MODE == COL_SOLVE || MODE == COL_SOLVE_W) {
     switch (H) { SC_SPEC_COL(SC_COL_CASE) default: break; }
   }
 #undef SC_COL_CASE
@@ -279,7 +282,9 @@ static int launch_row(const Plan& pl, RowParams rp, int B, cudaStream_t s, int n
   dim3 grid(rp.nblk, B);
   const size_t smem = MODE == ROW_ITER ? pl.row_smem
                      : MODE == ROW_FIXUP ? pl.row_smem_fix : pl.rowg_smem;
-  fn<<<grid, SC_ROW_THREADS, smem, s>>>(rp);
+  // one slot (row pair in flight) per rp.gsz threads
+  const int threads = (SC_ROW_THREADS / rp.gsz) * rp.gsz;
+  fn<<<grid, threads, smem, s>>>(rp);
   CU_TRY(cudaGetLastError());
   ++g_launches;
   return SC_OK;
@@ -288,8 +293,8 @@ static int launch_row(const Plan& pl, RowParams rp, int B, cudaStream_t s, int n
 template <int MODE>
 static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s) {
   cp.Hs = pl.Hs;
-  if (MODE == COL_SOLVE) {
-    ColFn fn = col_fn<COL_SOLVE>(cp.g.H);
+  if (MODE == COL_SOLVE || MODE == COL_SOLVE_W) {
+    ColFn fn = col_fn<MODE>(cp.g.H);
     int st = prepare_fn((const void*)fn, true);
     if (st) return st;
     cp.gsz = pl.col_g;
@@ -391,6 +396,9 @@ extern "C" int sc_cbpdn_solve(const sc_problem* p, const sc_options* o, void* wo
 
   float* U; float2 *F, *Dh, *Sh, *twW, *twH; double *part, *it, *xi; ImgState* sts; int* ndone;
   carve(pl, (unsigned char*)workspace, &U, &F, &Dh, &Sh, &twW, &twH, &part, &sts, &it, &xi, &ndone);
+  float* Psum = (float*)((unsigned char*)workspace + pl.off_Ps);
+  // one d for every map unless GradWeight differs between maps
+  const bool per_map_d = p->grd && !p->wgrd_uniform;
 
   twiddle_kernel<<<(g.W + 255) / 256, 256, 0, s>>>(twW, g.W);
   twiddle_kernel<<<(g.H + 255) / 256, 256, 0, s>>>(twH, g.H);
@@ -407,6 +415,10 @@ extern "C" int sc_cbpdn_solve(const sc_problem* p, const sc_options* o, void* wo
     ColParams cp = {};
     cp.g = g; cp.g.B = 1; cp.ph = pl.ph; cp.twH = twH; cp.twW = twW; cp.F = Dh;
     if ((st = launch_col<COL_FWD>(pl, cp, 1, s))) return st;
+    const size_t plane = (size_t)g.H * g.Wp;
+    psum_kernel<<<(unsigned)((plane + 255) / 256), 256, 0, s>>>(Dh, Psum, g.M, plane);
+    CU_TRY(cudaGetLastError());
+    ++g_launches;
   }
   // Signal spectra (B images, one map each).
   {
@@ -437,7 +449,7 @@ extern "C" int sc_cbpdn_solve(const sc_problem* p, const sc_options* o, void* wo
   rp.partials = part; rp.st = sts;
   ColParams cp = {};
   cp.g = g; cp.ph = pl.ph; cp.twH = twH; cp.twW = twW; cp.F = F; cp.Dh = Dh; cp.Sh = Sh;
-  cp.grd = p->grd; cp.mu = p->mu; cp.wgrd = p->wgrd; cp.st = sts;
+  cp.grd = p->grd; cp.mu = p->mu; cp.wgrd = p->wgrd; cp.Psum = Psum; cp.st = sts;
   FinParams fp = {};
   fp.max_iter = o->max_iter;
   fp.auto_rho = o->auto_rho; fp.period = std::max(1, o->auto_rho_period);
@@ -483,7 +495,11 @@ extern "C" int sc_cbpdn_solve(const sc_problem* p, const sc_options* o, void* wo
     int chunk = o->max_iter - done_iters;
     if (o->check_every > 0 && can_stop) chunk = std::min(chunk, o->check_every);
     for (int i = 0; i < chunk; ++i) {
-      if ((st = timed(0, [&] { return launch_col<COL_SOLVE>(pl, cp, g.B, s); }))) return st;
+      if ((st = timed(0, [&] {
+             return per_map_d ? launch_col<COL_SOLVE_W>(pl, cp, g.B, s)
+                              : launch_col<COL_SOLVE>(pl, cp, g.B, s);
+           })))
+        return st;
       if ((st = timed(1, [&] { return launch_row<ROW_ITER>(pl, rp, g.B, s); }))) return st;
       if ((st = timed(2, [&]() -> int {
              finalize_kernel<<<g.B, 256, 0, s>>>(part, pl.row_nblk, sts, fp);

@@ -320,6 +320,7 @@ def prepare_device(Dm, S, lmbda, opt, mu=0.0, grd=False, l1=1.0, gw=1.0, mask=No
             raise ValueError("GradWeight must be a scalar or have M entries")
         keep["gw"] = g.contiguous()
         prob.wgrd = keep["gw"].data_ptr()
+        prob.wgrd_uniform = int(bool(torch.all(keep["gw"] == keep["gw"][0]).item()))
     l1a = l1.detach().float() if torch.is_tensor(l1) else np.asarray(l1, dtype=F32)
     l1n = l1a.numel() if torch.is_tensor(l1a) else l1a.size
     if l1n == 1:

@@ -459,8 +459,9 @@ col_kernel(ColParams P) {
     };
 
     // ---------------------------------------------------------------- pass 1
-    // forward column FFT of the row spectra of Y - U; accumulate
-    // num = sum_m Df b / d (and sum_m |Df|^2 / d for per-map d); write the
+    // Forward column FFT of the row spectra of Y - U; accumulate
+    //   acc = sum_m Df_m (Y-U)^_m / d_m   (and sden = sum_m |Df_m|^2 / d_m for
+    // per-map d), so that sum_m Df_m b_m / d_m = S^ sden + rho acc; write the
     // column-transformed (Y - U)^ back in place for pass 2.
     float2 num[EPT];
     float sden[SDEN ? EPT : 1];
@@ -468,20 +469,19 @@ col_kernel(ColParams P) {
     for (int i = 0; i < EPT; ++i) num[i] = make_float2(0.f, 0.f);
 #pragma unroll
     for (int i = 0; i < (SDEN ? EPT : 1); ++i) sden[i] = 0.f;
-    if (m0 < m1) issue_tile(Fi + (size_t)m0 * H * Wp, fbuf[0]);
+    if (m0 < m1) {
+      issue_tile(Fi + (size_t)m0 * H * Wp, fbuf[0]);
+      issue_tile(P.Dh + (size_t)m0 * H * Wp, dbuf);
+    }
     cp_async_commit();
     int it = 0;
     for (int m = m0; m < m1; ++m, ++it) {
       float2* cur = fbuf[it & 1];
-      issue_tile(P.Dh + (size_t)m * H * Wp, dbuf);
-      cp_async_commit();
       if (m + 1 < m1) issue_tile(Fi + (size_t)(m + 1) * H * Wp, fbuf[(it + 1) & 1]);
       cp_async_commit();
-      cp_async_wait<2>();
+      cp_async_wait<1>();  // F(m) and D(m)
       __syncthreads();
       fft_any<NH, T, RM>(cur + cc, P.ph, P.twH, t, g);
-      cp_async_wait<1>();
-      __syncthreads();
       const float wg = grd ? mu * P.wgrd[m] : 0.f;
       float2* fout = Fi + (size_t)m * H * Wp + c0;
       if (colok) {
@@ -491,27 +491,29 @@ col_kernel(ColParams P) {
           if (kr < H) {
             const int sl = slot(kr) * T + cc;
             const float2 Dv = dbuf[sl];
-            const float2 Sv = __ldg(&Sh[(size_t)kr * Wp + cc]);
             const float2 yu = cur[sl];
             fout[(size_t)kr * Wp + cc] = yu;
-            // b = conj(D) S + rho (Y - U)^
-            const float2 bv = make_float2(Dv.x * Sv.x + Dv.y * Sv.y + rho * yu.x,
-                                          Dv.x * Sv.y - Dv.y * Sv.x + rho * yu.y);
             const float id = inv_d(wg, kr);
-            num[i].x += (Dv.x * bv.x - Dv.y * bv.y) * id;
-            num[i].y += (Dv.x * bv.y + Dv.y * bv.x) * id;
+            num[i].x += (Dv.x * yu.x - Dv.y * yu.y) * id;
+            num[i].y += (Dv.x * yu.y + Dv.y * yu.x) * id;
             if constexpr (SDEN) sden[i] += (Dv.x * Dv.x + Dv.y * Dv.y) * id;
           }
         }
       }
       __syncthreads();
+      // the dictionary tile of the next map lands during its FFT
+      if (m + 1 < m1) issue_tile(P.Dh + (size_t)(m + 1) * H * Wp, dbuf);
+      cp_async_commit();
     }
-    // prefetch the first tile of pass 2 into F0 while [F1][D] hosts the
-    // reduction over the maps
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    // prefetch the first spectrum tile of pass 2 into F0 while [F1][D] hosts
+    // the reduction over the maps
     if (m0 < m1) issue_tile(Fi + (size_t)m0 * H * Wp, fbuf[0]);
     cp_async_commit();
     // ------------------------------------------------- reduce over the maps
-    // cb = sum_m Df b / d / (1 + sum_m |Df|^2 / d)
+    // cb = (S^ sden + rho acc) / (1 + sden); pass 2 keeps SC = S^ - cb
     const int E = T * H;
     float2* xn = fbuf[1];                                  // [E] complex
     float* xd = reinterpret_cast<float*>(xn + E);          // [E] real
@@ -530,6 +532,15 @@ col_kernel(ColParams P) {
         }
         return __ldg(&P.Psum[(size_t)kr * Wp + k]) * id;
       }
+    };
+    auto s_minus_cb = [&](int kr, int c, float2 acc, float ds) -> float2 {
+      const int k = c0 + c;
+      if (k >= Wf) return make_float2(0.f, 0.f);
+      const float2 Sv = __ldg(&Sh[(size_t)kr * Wp + c]);
+      const float sd = denom(kr, c, ds);
+      const float q = 1.f / (1.f + sd);
+      const float2 cb = make_float2((Sv.x * sd + rho * acc.x) * q, (Sv.y * sd + rho * acc.y) * q);
+      return make_float2(Sv.x - cb.x, Sv.y - cb.y);
     };
 #pragma unroll
     for (int i = 0; i < EPT; ++i) {
@@ -553,8 +564,7 @@ col_kernel(ColParams P) {
           ns.y += v.y;
           if constexpr (SDEN) ds += cluster.map_shared_rank(xd, r)[e];
         }
-        const float q = 1.f / (1.f + denom(e / T, e % T, ds));
-        xn[e] = make_float2(ns.x * q, ns.y * q);
+        xn[e] = s_minus_cb(e / T, e % T, ns, ds);
       }
       cluster.sync();
 #pragma unroll
@@ -571,22 +581,21 @@ col_kernel(ColParams P) {
 #pragma unroll
       for (int i = 0; i < EPT; ++i) {
         const int kr = t + i * g;
-        const float q = 1.f / (1.f + denom(kr, cc, SDEN ? sden[SDEN ? i : 0] : 0.f));
-        num[i] = make_float2(num[i].x * q, num[i].y * q);
+        if (kr < H) num[i] = s_minus_cb(kr, cc, num[i], SDEN ? sden[SDEN ? i : 0] : 0.f);
       }
       __syncthreads();
     }
-    // num[i] now holds cb for this thread's elements
+    // num[i] now holds SC = S^ - cb for this thread's elements
+    if (m0 < m1) issue_tile(P.Dh + (size_t)m0 * H * Wp, dbuf);
+    cp_async_commit();
     // ---------------------------------------------------------------- pass 2
-    // x = (b - conj(Df) cb) / d from the stored (Y - U)^, inverse column FFT
+    // x = (conj(Df) SC + rho (Y - U)^) / d, inverse column FFT
     it = 0;
     for (int m = m0; m < m1; ++m, ++it) {
       float2* cur = fbuf[it & 1];
-      issue_tile(P.Dh + (size_t)m * H * Wp, dbuf);
-      cp_async_commit();
       if (m + 1 < m1) issue_tile(Fi + (size_t)(m + 1) * H * Wp, fbuf[(it + 1) & 1]);
       cp_async_commit();
-      cp_async_wait<1>();
+      cp_async_wait<1>();  // F(m) and D(m)
       __syncthreads();
       const float wg = grd ? mu * P.wgrd[m] : 0.f;
 #pragma unroll
@@ -597,19 +606,19 @@ col_kernel(ColParams P) {
           float2 xo = make_float2(0.f, 0.f);
           if (colok) {
             const float2 Dv = dbuf[sl];
-            const float2 Sv = __ldg(&Sh[(size_t)kr * Wp + cc]);
             const float2 yu = cur[sl];
-            const float2 bv = make_float2(Dv.x * Sv.x + Dv.y * Sv.y + rho * yu.x,
-                                          Dv.x * Sv.y - Dv.y * Sv.x + rho * yu.y);
+            const float2 sc = num[i];
             const float id = inv_d(wg, kr);
-            const float2 cb = num[i];
-            xo.x = (bv.x - (Dv.x * cb.x + Dv.y * cb.y)) * id;
-            xo.y = (bv.y - (Dv.x * cb.y - Dv.y * cb.x)) * id;
+            xo.x = (Dv.x * sc.x + Dv.y * sc.y + rho * yu.x) * id;
+            xo.y = (Dv.x * sc.y - Dv.y * sc.x + rho * yu.y) * id;
           }
           cur[sl] = make_float2(xo.x, -xo.y);  // conj: inverse via forward FFT
         }
       }
       __syncthreads();
+      // the dictionary tile of the next map lands during this inverse FFT
+      if (m + 1 < m1) issue_tile(P.Dh + (size_t)(m + 1) * H * Wp, dbuf);
+      cp_async_commit();
       fft_any<NH, T, RM>(cur + cc, P.ph, P.twH, t, g);
       float2* dst = Fi + (size_t)m * H * Wp + c0;
       if (colok) {
@@ -624,6 +633,7 @@ col_kernel(ColParams P) {
       }
       __syncthreads();
     }
+    cp_async_commit();
     cp_async_wait<0>();
   }
 }

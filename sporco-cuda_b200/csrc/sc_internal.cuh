@@ -110,12 +110,12 @@ __host__ __device__ inline size_t sc_align16(size_t x) { return (x + 15) & ~(siz
 
 // Shared memory of one row-pass slot (one row pair in flight); zlen is the
 // (padded) number of shared-memory slots of one row transform.  The
-// iteration mode double-buffers the pair's two spectrum rows and stages the
-// pair's Y and U rows: [z: zlen complex][F: 2 x 2Wp complex][Y: 2W][U: 2W].
+// iteration mode stages the next pair's two spectrum rows and the pair's Y
+// and U rows: [z: zlen complex][F: 2Wp complex][Y: 2W][U: 2W].
 __host__ __device__ inline size_t row_slot_bytes(int mode, int zlen, int W, int Wp) {
   size_t z = sc_align16((size_t)zlen * 8);
   if (mode != ROW_ITER) return z;
-  return z + 2 * (size_t)(2 * Wp) * 8 + 2 * sc_align16((size_t)(2 * W) * 4);
+  return z + (size_t)(2 * Wp) * 8 + 2 * sc_align16((size_t)(2 * W) * 4);
 }
 
 // Shared memory of one column-pass CTA; hlen is the (padded) number of

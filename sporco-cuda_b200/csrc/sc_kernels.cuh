@@ -117,7 +117,7 @@ __device__ __forceinline__ float2 pack_inverse(const float2* a, const float2* bb
 // NW > 0: row length W known at compile time (specialised FFT plan);
 // NW == 0: any W (runtime FFT plan).
 template <int MODE, int NW>
-__global__ void __launch_bounds__(SC_ROW_THREADS, 2)
+__global__ void __launch_bounds__(SC_ROW_THREADS, 3)
 row_kernel(RowParams P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red_scratch[(SC_ROW_THREADS / 32) * 5];
@@ -158,19 +158,18 @@ row_kernel(RowParams P) {
   if constexpr (MODE == ROW_ITER) {
     // --------------------------------------------------------- iteration
     float2* fst = reinterpret_cast<float2*>(slot + sc_align16((size_t)zlen * 8));
-    float* ysm = reinterpret_cast<float*>(fst + 2 * 2 * (size_t)Wp);
+    float* ysm = reinterpret_cast<float*>(fst + 2 * (size_t)Wp);
     float* usm = ysm + sc_align16((size_t)(2 * W) * 4) / 4;
     const float* Yi = P.Y + (size_t)b * img_real;
     const float* Ui = P.U + (size_t)b * img_real;
     const bool vec = (W & 3) == 0;
 
-    auto issue_F = [&](long p, int stage) {
+    auto issue_F = [&](long p) {
       if (p < npairs) {
         const int nrow = (2 * p + 1 < rows) ? 2 : 1;
         const float2* src = Fi + 2 * p * Wp;
-        float2* dst = fst + stage * 2 * Wp;
         const int nch = nrow * Wp / 2;
-        for (int q = t; q < nch; q += g) cp_async16(dst + 2 * q, src + 2 * q);
+        for (int q = t; q < nch; q += g) cp_async16(fst + 2 * q, src + 2 * q);
       }
     };
     auto issue_YU = [&](long p) {
@@ -196,28 +195,45 @@ row_kernel(RowParams P) {
     const int32_t* mk = P.mask ? P.mask + (size_t)b * H * W : nullptr;
     const float a = P.relax, a1 = 1.f - P.relax;
     const bool relax = P.relax != 1.f;
+    // one element of the epilogue: returns y - u, accumulates the residual
+    // partial sums in f[] (single precision within a row pair)
+    auto elem = [&](float x, float yo, float uo, bool ams, int mval, float tw, float* y_out,
+                    float* u_out, float* f) -> float {
+      const float xr = relax ? a * x + a1 * yo : x;
+      const float v = xr + uo;
+      const float y = ams ? (float)(1 - mval) * v : soft_threshold(v, tw);
+      const float u = v - y;
+      *y_out = y;
+      *u_out = u;
+      const float dxy = x - y, dyy = yo - y;
+      f[0] += x * x;
+      f[1] += y * y;
+      f[2] += u * u;
+      f[3] += dxy * dxy;
+      f[4] += dyy * dyy;
+      return y - u;
+    };
 
-    issue_F((long)blockIdx.x * S + s, 0);
+    long p0 = (long)blockIdx.x * S + s;
+    issue_F(p0);
     cp_async_commit();
-    int it = 0;
-    for (long pb = (long)blockIdx.x * S; pb < npairs; pb += pstride, ++it) {
+    issue_YU(p0);
+    cp_async_commit();
+    for (long pb = (long)blockIdx.x * S; pb < npairs; pb += pstride) {
       const long p = pb + s;
       const bool valid = p < npairs;
       const long r0 = 2 * p, r1 = 2 * p + 1;
       const bool has1 = valid && (r1 < rows);
-      issue_YU(p);
-      cp_async_commit();
-      issue_F(p + pstride, (it + 1) & 1);
-      cp_async_commit();
-      cp_async_wait<2>();
+      cp_async_wait<1>();  // F(p)
       __syncthreads();
       if (valid) {
-        const float2* fa = fst + (it & 1) * 2 * Wp;
-        for (int k = t; k < W; k += g) z[zs(k)] = pack_inverse(fa, fa + Wp, has1, k, W, Wf);
+        for (int k = t; k < W; k += g) z[zs(k)] = pack_inverse(fst, fst + Wp, has1, k, W, Wf);
       }
       __syncthreads();
+      issue_F(p + pstride);  // lands during this pair's transforms
+      cp_async_commit();
       fft_any<NW, 1, RM>(z, P.pw, P.twW, t, g);
-      cp_async_wait<1>();
+      cp_async_wait<1>();  // Y(p), U(p)
       __syncthreads();
       if (valid) {
         const int m0 = (int)(r0 / H), h0 = (int)(r0 - (long)m0 * H);
@@ -229,51 +245,45 @@ row_kernel(RowParams P) {
         const float* wr0 = P.l1_kind == 2 ? P.l1w + ((size_t)m0 * H + h0) * W : nullptr;
         const float* wr1 = (P.l1_kind == 2 && has1) ? P.l1w + ((size_t)m1 * H + h1) * W : nullptr;
         const bool ams0 = mk && m0 == 0, ams1 = mk && m1 == 0;
-        for (int k = t; k < W; k += g) {
-          const float2 zz = z[zs(k)];
-          float yu0, yu1 = 0.f;
-          {
-            const float x = zz.x * P.invN;
-            const float yo = ysm[k], uo = usm[k] * uscale;
-            const float xr = relax ? a * x + a1 * yo : x;
-            const float v = xr + uo;
-            float y;
-            if (ams0) y = (float)(1 - mk[h0 * W + k]) * v;
-            else y = soft_threshold(v, thr * (wr0 ? wr0[k] : w0));
-            const float u = v - y;
+        const float t0 = thr * w0, t1 = thr * w1;
+        float f[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+        if (!ams0 && !ams1 && !wr0 && !wr1 && has1) {
+          // common case: two rows, scalar thresholds
+          for (int k = t; k < W; k += g) {
+            const float2 zz = z[zs(k)];
+            float y, u;
+            const float yu0 = elem(zz.x * P.invN, ysm[k], usm[k] * uscale, false, 0, t0, &y, &u, f);
             Y0[k] = y;
             U0[k] = u;
-            yu0 = y - u;
-            const float dxy = x - y, dyy = yo - y;
-            acc[0] += (double)(x * x);
-            acc[1] += (double)(y * y);
-            acc[2] += (double)(u * u);
-            acc[3] += (double)(dxy * dxy);
-            acc[4] += (double)(dyy * dyy);
-          }
-          if (has1) {
-            const float x = -zz.y * P.invN;
-            const float yo = ysm[W + k], uo = usm[W + k] * uscale;
-            const float xr = relax ? a * x + a1 * yo : x;
-            const float v = xr + uo;
-            float y;
-            if (ams1) y = (float)(1 - mk[h1 * W + k]) * v;
-            else y = soft_threshold(v, thr * (wr1 ? wr1[k] : w1));
-            const float u = v - y;
+            const float yu1 =
+                elem(-zz.y * P.invN, ysm[W + k], usm[W + k] * uscale, false, 0, t1, &y, &u, f);
             Y0[W + k] = y;
             U0[W + k] = u;
-            yu1 = y - u;
-            const float dxy = x - y, dyy = yo - y;
-            acc[0] += (double)(x * x);
-            acc[1] += (double)(y * y);
-            acc[2] += (double)(u * u);
-            acc[3] += (double)(dxy * dxy);
-            acc[4] += (double)(dyy * dyy);
+            z[zs(k)] = make_float2(yu0, yu1);
           }
-          z[zs(k)] = make_float2(yu0, yu1);
+        } else {
+          for (int k = t; k < W; k += g) {
+            const float2 zz = z[zs(k)];
+            float y, u, yu1 = 0.f;
+            const float yu0 = elem(zz.x * P.invN, ysm[k], usm[k] * uscale, ams0,
+                                   ams0 ? mk[h0 * W + k] : 0, thr * (wr0 ? wr0[k] : w0), &y, &u, f);
+            Y0[k] = y;
+            U0[k] = u;
+            if (has1) {
+              yu1 = elem(-zz.y * P.invN, ysm[W + k], usm[W + k] * uscale, ams1,
+                         ams1 ? mk[h1 * W + k] : 0, thr * (wr1 ? wr1[k] : w1), &y, &u, f);
+              Y0[W + k] = y;
+              U0[W + k] = u;
+            }
+            z[zs(k)] = make_float2(yu0, yu1);
+          }
         }
+#pragma unroll
+        for (int i = 0; i < 5; ++i) acc[i] += (double)f[i];
       }
       __syncthreads();
+      issue_YU(p + pstride);  // Y/U staging is free again
+      cp_async_commit();
       fft_any<NW, 1, RM>(z, P.pw, P.twW, t, g);
       if (valid) {
         float2* fa = Fi + r0 * Wp;

@@ -328,9 +328,10 @@ def prepare_device(Dm, S, lmbda, opt, mu=0.0, grd=False, l1=1.0, gw=1.0, mask=No
         prob.l1_scalar = float(np.asarray(_np(l1a), dtype=F32).ravel()[0])
     else:
         t = torch.as_tensor(l1a, dtype=torch.float32, device=dev)
-        if t.ndim == 1 and t.numel() == M:
+        if t.numel() == M and all(d == 1 for d in t.shape[1:]):
+            # one weight per map, e.g. (M,) or (M, 1, 1)
             prob.l1_kind = _lib.SC_L1_PER_MAP
-            keep["l1"] = t.contiguous()
+            keep["l1"] = t.reshape(M).contiguous()
         else:
             while t.ndim < 3:
                 t = t.unsqueeze(0)

@@ -175,6 +175,17 @@ int sc_rfft2(const float *x, void *xf, int count, int H, int W, void *stream);
 /* Inverse of sc_rfft2 (numpy irfft2, normalised by 1/(H W)). */
 int sc_irfft2(const void *xf, float *x, int count, int H, int W, void *stream);
 
+/* sc_rfft2 without any device-memory allocation (no counterpart in the
+ * reference).  For callers that must not allocate device memory -- code
+ * running under a memory budget owned by another allocator, or
+ * real-time callers that must not call into the allocator on their
+ * critical path: its scratch (W + H twiddles) lives in a 64 KiB static
+ * device array that every GPU loading this library holds until the process
+ * exits.  Rejects H + W > 8192 with SC_ERR_UNSUPPORTED.  The first call on a
+ * device looks up that array's device address; make it before any stream
+ * capture.  All calls share the array, so calls that overlap on the GPU race. */
+int sc_rfft2_noalloc(const float *x, void *xf, int count, int H, int W, void *stream);
+
 /* Per-kernel device time of the last solve run with options.profile set:
  * index 0 column pass, 1 row pass, 2 finalize, 3 rho fix-up. */
 typedef struct sc_profile {

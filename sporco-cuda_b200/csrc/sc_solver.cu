@@ -622,3 +622,70 @@ extern "C" int sc_irfft2(const void* xf, float* x, int count, int H, int W, void
   CU_TRY(cudaFreeAsync(tw, s));
   return SC_OK;
 }
+
+// ------------------------------------------------- allocation-free rfft2 --
+// sc_rfft2 takes its scratch (the two twiddle tables) from the stream-ordered
+// allocator.  sc_rfft2_noalloc is the same transform with that scratch in a
+// file-scope device array instead, for callers that must not allocate device
+// memory.  The array is SC_NOALLOC_TWIDDLES complex entries (64 KiB) and
+// holds the W + H twiddles of one call; every GPU that loads this library
+// keeps it until the process exits.  All calls share it: each call rewrites
+// the entries it uses before reading them (nothing has to start at zero),
+// and calls that overlap on the GPU (e.g. on two streams) race on it.
+#define SC_NOALLOC_TWIDDLES 8192
+#define SC_NOALLOC_MAX_DEVICES 64
+static __device__ __align__(256) float2 sc_noalloc_tw[SC_NOALLOC_TWIDDLES];
+// Device address of sc_noalloc_tw per device (the host-side symbol is only a
+// stand-in for it), looked up once per device by the first call there.
+static float2* g_noalloc_tw[SC_NOALLOC_MAX_DEVICES] = {};
+
+extern "C" int sc_rfft2_noalloc(const float* x, void* xf, int count, int H, int W, void* stream) {
+  set_status(SC_OK, nullptr);
+  (void)cudaGetLastError();
+  if (!x || !xf) return set_status(SC_ERR_INVALID, "null pointer");
+  if (count < 1 || H < 1 || W < 1)
+    return set_status(SC_ERR_INVALID, "sizes must be positive (count=%d H=%d W=%d)", count, H, W);
+  if (H + W > SC_NOALLOC_TWIDDLES)
+    return set_status(SC_ERR_UNSUPPORTED,
+                      "H + W = %d twiddles exceed the %d the static scratch holds", H + W,
+                      SC_NOALLOC_TWIDDLES);
+  Plan pl;
+  int st = plan_geometry(count, 1, H, W, &pl);
+  if (st) return st;
+  int dev = 0;
+  CU_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= SC_NOALLOC_MAX_DEVICES)
+    return set_status(SC_ERR_UNSUPPORTED, "device %d beyond the %d this entry point tracks", dev,
+                      SC_NOALLOC_MAX_DEVICES);
+  if (!g_noalloc_tw[dev]) {
+    void* addr = nullptr;
+    CU_TRY(cudaGetSymbolAddress(&addr, sc_noalloc_tw));
+    g_noalloc_tw[dev] = (float2*)addr;
+  }
+  float2* tw = g_noalloc_tw[dev];
+  cudaStream_t s = (cudaStream_t)stream;
+  pl.g.Wp = pl.g.Wf;  // dense numpy layout
+  twiddle_kernel<<<(W + 255) / 256, 256, 0, s>>>(tw, W);
+  twiddle_kernel<<<(H + 255) / 256, 256, 0, s>>>(tw + W, H);
+  CU_TRY(cudaGetLastError());
+  RowParams rp = {};
+  rp.g = pl.g; rp.pw = pl.pw; rp.twW = tw; rp.F = (float2*)xf; rp.src = x;
+  rp.gsz = pl.rowg_g;
+  rp.nblk = pl.row_nblk;
+  CU_TRY(cudaFuncSetAttribute(row_kernel<ROW_FWD_REAL, 0>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.rowg_smem));
+  row_kernel<ROW_FWD_REAL, 0><<<dim3(rp.nblk, count), (SC_ROW_THREADS / rp.gsz) * rp.gsz,
+                                 pl.rowg_smem, s>>>(rp);
+  CU_TRY(cudaGetLastError());
+  ColParams cp = {};
+  cp.g = pl.g; cp.ph = pl.ph; cp.twH = tw + W; cp.twW = tw; cp.F = (float2*)xf;
+  cp.gsz = pl.colg_g;
+  cp.Hs = pl.Hs;
+  cp.G = 1;
+  CU_TRY(cudaFuncSetAttribute(col_kernel<COL_FWD, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)pl.colg_smem));
+  col_kernel<COL_FWD, 0><<<dim3(1, pl.col_ntiles, count), pl.colg_NT, pl.colg_smem, s>>>(cp);
+  CU_TRY(cudaGetLastError());
+  g_launches += 4;
+  return SC_OK;
+}

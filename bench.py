@@ -45,6 +45,8 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
+F32 = np.float32
+
 METRIC = ("ADMM iters/s & HBM GB/s (plain vs batched vs fwd+adjoint), "
           "rel err ≤1e-4 vs FP64")
 
@@ -58,6 +60,11 @@ CONFIGS = {
     4: dict(workload="cbpdn 2048x2048 M=256 16x16, 100 iterations, AutoRho",
             H=2048, W=2048, M=256, K=16, density=0.01, lmbda=0.02, mu=0.0,
             variants=["cbpdn"], iters=100, autorho=True, mask_p=None),
+    2: dict(workload="batched cbpdnmsk: 64 images, sides from {128..1024} (H, W independent), "
+                     "M=64 12x12, per-image masks and lambda, AutoRho, RelStopTol 1e-4, cap 1000",
+            H=None, W=None, M=64, K=12, density=0.005, lmbda=None, mu=0.0,
+            variants=["cbpdnmsk"], iters=1000, autorho=True, mask_p=None, nimg=64,
+            sides=(128, 192, 256, 384, 512, 768, 1024)),
     # small 2048x2048 case for kernel profiles (2 GB on the device)
     9: dict(workload="cbpdn 2048x2048 M=24 16x16, 20 iterations, AutoRho (profiling case)",
             H=2048, W=2048, M=24, K=16, density=0.01, lmbda=0.02, mu=0.0,
@@ -369,6 +376,144 @@ def run_ours(args, cfg, rank, world, local_rank):
     return out
 
 
+def synth_images(cfg, seed, device):
+    """Config 2: uneven images from one dictionary, masks, lambdas."""
+    import torch
+    from sporco_cuda import _lib
+    rng = np.random.default_rng(seed)
+    M, K = cfg["M"], cfg["K"]
+    g = torch.Generator(device=device).manual_seed(seed)
+    D = torch.randn((M, K, K), generator=g, device=device)
+    D /= torch.sqrt(torch.sum(D * D, dim=(1, 2), keepdim=True))
+    imgs, masks = [], []
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for _ in range(cfg["nimg"]):
+        H, W = (int(rng.choice(cfg["sides"])) for _ in range(2))
+        Dp = torch.zeros((M, H, W), device=device)
+        Dp[:, :K, :K] = D
+        X0 = (torch.rand((M, H, W), generator=g, device=device) < cfg["density"]).float() * \
+            torch.randn((M, H, W), generator=g, device=device)
+        Wf = W // 2 + 1
+        Df = torch.empty((M, H, Wf), dtype=torch.complex64, device=device)
+        Xf = torch.empty((M, H, Wf), dtype=torch.complex64, device=device)
+        _lib.check(_lib.sc_rfft2(C.c_void_p(Dp.data_ptr()), C.c_void_p(Df.data_ptr()), M, H, W, st))
+        _lib.check(_lib.sc_rfft2(C.c_void_p(X0.data_ptr()), C.c_void_p(Xf.data_ptr()), M, H, W, st))
+        Sf = torch.sum(Df * Xf, dim=0).contiguous()
+        S = torch.empty((1, H, W), device=device)
+        _lib.check(_lib.sc_irfft2(C.c_void_p(Sf.data_ptr()), C.c_void_p(S.data_ptr()), 1, H, W, st))
+        S = S[0] + 0.01 * torch.randn((H, W), generator=g, device=device)
+        S = S - S.mean()
+        p = float(rng.uniform(0.5, 0.9))
+        mk = (torch.rand((H, W), generator=g, device=device) < p).float()
+        imgs.append((S * mk).contiguous())
+        masks.append(mk)
+    lam = rng.uniform(0.02, 0.1, cfg["nimg"]).astype(np.float32)
+    return D.contiguous(), imgs, masks, lam
+
+
+def run_batched(args, cfg, rank, world, local_rank):
+    """Config 2: image-iterations/s of the batched solver, and of a loop of
+    single solves over the same images."""
+    import torch
+    import sporco_cuda.cbpdn as cb
+    from sporco_cuda import _lib
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    D, imgs, masks, lam = synth_images(cfg, 12345 + args.config + rank, dev)
+    Dk = D.permute(1, 2, 0).contiguous()
+    opt = {"MaxMainIter": cfg["iters"], "RelStopTol": 1e-4, "AbsStopTol": 0.0,
+           "RelaxParam": 1.8, "L1Weight": 1.0,
+           "AutoRho": {"Enabled": True, "Period": 1, "Scaling": 1000.0, "RsdlRatio": 1.2,
+                       "RsdlTarget": None, "AutoScaling": True, "StdResiduals": False}}
+
+    def step():
+        _, iters = cb.cbpdn_batched(Dk, imgs, lam, opt, W_list=masks, return_info=True)
+        return iters
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    n0 = _lib.sc_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    total_it = 0
+    with ClockSampler(local_rank) as clk:
+        ev0.record()
+        for _ in range(args.steps):
+            total_it += sum(step())
+        ev1.record()
+        barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = _lib.sc_launch_count() - n0
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+        t = torch.tensor([total_it], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t)
+        total_it = int(t.item())
+    value = total_it / (ms / 1e3)
+    # loop of single solves over the same images (device inputs)
+    Di = torch.cat((torch.zeros((1, cfg["K"], cfg["K"]), device=dev), D), 0)
+    Di[0, 0, 0] = 1.0  # the AMS impulse filter, as cbpdnmsk prepends it
+    l1 = np.concatenate(([0.0], np.ones(cfg["M"]))).astype(F32)
+    t0 = time.perf_counter()
+    loop_it = 0
+    for S, mk, lm in zip(imgs, masks, lam):
+        ds = cb.prepare_device(Di, S[None], float(lm), opt, l1=l1, mask=mk.to(torch.int32)[None])
+        ds.run()
+        loop_it += ds.state()["iterations"][0]
+    torch.cuda.synchronize()
+    loop_ms = (time.perf_counter() - t0) * 1e3
+    loop_value = loop_it / (loop_ms / 1e3)
+    # end to end through the public API with numpy host buffers
+    Dn = Dk.cpu().numpy()
+    In = [x.cpu().numpy() for x in imgs]
+    Wn = [x.cpu().numpy() for x in masks]
+    barrier()
+    t0 = time.perf_counter()
+    out, e_iters = cb.cbpdn_batched(Dn, In, lam, opt, W_list=Wn, return_info=True)
+    barrier()
+    e_ms = (time.perf_counter() - t0) * 1e3
+    e_value = sum(e_iters) / (e_ms / 1e3)
+    h2d = 4 * Dn.size + sum(4 * x.size for x in In) + sum(4 * x.size for x in Wn) + 4 * len(lam)
+    d2h = sum(4 * x.size for x in out)
+    peak, peak_kind = measured_peaks()
+    bytes_total = 0.0
+    it_per_img = step()  # iteration counts per image (same data, same counts)
+    for S, k in zip(imgs, it_per_img):
+        bytes_total += algorithmic_bytes(S.shape[0], S.shape[1], cfg["M"] + 1) * k
+    achieved = bytes_total * args.steps / (ms / 1e3) / 1e9
+    if rank != 0:
+        return None
+    shapes = sorted(set(tuple(x.shape) for x in imgs))
+    return {
+        "metric": METRIC, "value": value, "unit": "image-iter/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": cfg["workload"], "images": cfg["nimg"], "M": cfg["M"],
+                   "K": cfg["K"], "buckets": len(shapes),
+                   "parallelism": "replicas%d" % world if world > 1 else "single",
+                   "l2": "working set larger than L2 (no flush)"},
+        "loop_of_single_solves": {"value": loop_value, "unit": "image-iter/s",
+                                  "speedup_batched_over_loop": value / loop_value},
+        "e2e": {"value": e_value, "unit": "image-iter/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "kernel": "batched solve (all buckets, all kernels)",
+                     "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None},
+        "iterations": {"mean": float(np.mean(it_per_img)), "max": int(np.max(it_per_img))},
+        "cpu_baseline": None,
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+
+
 def run_reference(args, cfg, rank):
     """The reference algorithm on the host cores (FP64 restatement)."""
     if rank != 0:
@@ -435,7 +580,10 @@ def main():
         import torch
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    out = run_ours(args, cfg, rank, world, local_rank)
+    if args.config == 2:
+        out = run_batched(args, cfg, rank, world, local_rank)
+    else:
+        out = run_ours(args, cfg, rank, world, local_rank)
     if out is not None:
         print(json.dumps(out), flush=True)
     if world > 1:

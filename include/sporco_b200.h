@@ -164,6 +164,15 @@ void sc_options_from_algopt(const AlgOpt *a, sc_options *o);
 int sc_cbpdn_solve(const sc_problem *p, const sc_options *o, void *workspace,
                    size_t workspace_bytes, sc_result *res, void *stream);
 
+/* Several batches of different image sizes solved together (no reference
+ * counterpart): problem i uses workspaces[i] (workspace_bytes[i]) and
+ * streams[i] (NULL array: the legacy default stream for all).  Iterations of
+ * all problems are launched in turn, each on its own stream, and every
+ * problem stops on its own; res may be NULL or hold nprob results. */
+int sc_cbpdn_solve_batch(const sc_problem *probs, int nprob, const sc_options *o,
+                         void *const *workspaces, const size_t *workspace_bytes,
+                         sc_result *res, void *const *streams);
+
 /* Per-image iteration counts / final rho / itstat after a solve, copied from
  * the workspace of that solve (host pointers; itstat may be NULL). */
 int sc_read_state(const sc_problem *p, const sc_options *o, const void *workspace,

@@ -374,90 +374,191 @@ extern "C" void sc_options_from_algopt(const AlgOpt* a, sc_options* o) {
   o->check_every = 32;
 }
 
+// One solve of a batch of equal-sized images: set-up, iteration launches in
+// chunks, host polling of the "finished" counter between chunks, results.
+// sc_cbpdn_solve drives one; sc_cbpdn_solve_batch interleaves several on
+// their own streams.
+struct Solve {
+  const sc_problem* p = nullptr;
+  const sc_options* o = nullptr;
+  Plan pl;
+  cudaStream_t s = nullptr;
+  float* U = nullptr;
+  float2 *F = nullptr, *Dh = nullptr, *Sh = nullptr, *twW = nullptr, *twH = nullptr;
+  double *part = nullptr, *it = nullptr, *xi = nullptr;
+  ImgState* sts = nullptr;
+  int* ndone = nullptr;
+  float* Psum = nullptr;
+  bool per_map_d = false, can_stop = false, finished = false;
+  int done_iters = 0;
+  RowParams rp = {};
+  ColParams cp = {};
+  FinParams fp = {};
+
+  int setup(const sc_problem* p_, const sc_options* o_, void* workspace, size_t workspace_bytes,
+            cudaStream_t stream) {
+    p = p_;
+    o = o_;
+    s = stream;
+    if (!p || !o) return set_status(SC_ERR_INVALID, "null problem or options");
+    int st = plan_problem(p, o, &pl);
+    if (st) return st;
+    if (!workspace || workspace_bytes < pl.total)
+      return set_status(SC_ERR_WORKSPACE, "workspace of %zu bytes needed", pl.total);
+    if (((uintptr_t)workspace) & 255)
+      return set_status(SC_ERR_WORKSPACE, "workspace not 256-byte aligned");
+    if (!p->D || !p->S || !p->lmbda || !p->rho0 || !p->Y)
+      return set_status(SC_ERR_INVALID, "null device pointer");
+    if (p->grd && !p->wgrd) return set_status(SC_ERR_INVALID, "grd problem without GradWeight");
+    if (p->l1_kind != SC_L1_SCALAR && !p->l1w)
+      return set_status(SC_ERR_INVALID, "missing L1Weight");
+    if ((p->W % 4) == 0 && (((uintptr_t)p->Y) & 15))
+      return set_status(SC_ERR_INVALID, "Y must be 16-byte aligned");
+    const Geom& g = pl.g;
+    carve(pl, (unsigned char*)workspace, &U, &F, &Dh, &Sh, &twW, &twH, &part, &sts, &it, &xi,
+          &ndone);
+    Psum = (float*)((unsigned char*)workspace + pl.off_Ps);
+    // one d for every map unless GradWeight differs between maps
+    per_map_d = p->grd && !p->wgrd_uniform;
+
+    twiddle_kernel<<<(g.W + 255) / 256, 256, 0, s>>>(twW, g.W);
+    twiddle_kernel<<<(g.H + 255) / 256, 256, 0, s>>>(twH, g.H);
+    CU_TRY(cudaGetLastError());
+    g_launches += 2;
+
+    // Dictionary spectrum: rfft2 of the zero-padded filters (cuda_Pad_Dict +
+    // R2C, cbpdn.cu:277-289), computed without materialising the padding.
+    {
+      RowParams r = {};
+      r.g = g; r.g.B = 1;
+      r.pw = pl.pw; r.twW = twW; r.F = Dh; r.D = p->D; r.Kr = p->Kr; r.Kc = p->Kc;
+      if ((st = launch_row<ROW_FWD_DICT>(pl, r, 1, s))) return st;
+      ColParams c = {};
+      c.g = g; c.g.B = 1; c.ph = pl.ph; c.twH = twH; c.twW = twW; c.F = Dh;
+      if ((st = launch_col<COL_FWD>(pl, c, 1, s))) return st;
+      const size_t plane = (size_t)g.H * g.Wp;
+      psum_kernel<<<(unsigned)((plane + 255) / 256), 256, 0, s>>>(Dh, Psum, g.M, plane);
+      CU_TRY(cudaGetLastError());
+      ++g_launches;
+    }
+    // Signal spectra (B images, one map each).
+    {
+      RowParams r = {};
+      r.g = g; r.g.M = 1;
+      r.pw = pl.pw; r.twW = twW; r.F = Sh; r.src = p->S;
+      const long npairs = ((long)g.H + 1) / 2;
+      const int S = SC_ROW_THREADS / pl.rowg_g;
+      const int nb = (int)std::max(1L, std::min((npairs + S - 1) / S, (long)num_sms()));
+      if ((st = launch_row<ROW_FWD_REAL>(pl, r, g.B, s, nb))) return st;
+      ColParams c = {};
+      c.g = g; c.g.M = 1; c.ph = pl.ph; c.twH = twH; c.twW = twW; c.F = Sh;
+      if ((st = launch_col<COL_FWD>(pl, c, g.B, s))) return st;
+    }
+    const size_t real_all = (size_t)g.B * g.M * g.H * g.W;
+    CU_TRY(cudaMemsetAsync(p->Y, 0, sizeof(float) * real_all, s));
+    CU_TRY(cudaMemsetAsync(U, 0, sizeof(float) * real_all, s));
+    CU_TRY(cudaMemsetAsync(F, 0, sizeof(float2) * (size_t)g.B * g.M * g.H * g.Wp, s));
+    init_state_kernel<<<(g.B + 127) / 128, 128, 0, s>>>(sts, p->rho0, g.B, ndone);
+    xi_kernel<<<(g.B + 127) / 128, 128, 0, s>>>(xi, p->lmbda, g.B, o->rsdl_target,
+                                                 o->std_residuals);
+    CU_TRY(cudaGetLastError());
+    g_launches += 2;
+
+    rp.g = g; rp.pw = pl.pw; rp.twW = twW; rp.F = F; rp.Y = p->Y; rp.U = U;
+    rp.lam = p->lmbda; rp.l1_kind = p->l1_kind; rp.l1_scalar = p->l1_scalar; rp.l1w = p->l1w;
+    rp.mask = p->mask; rp.relax = o->relax; rp.invN = (float)(1.0 / ((double)g.H * g.W));
+    rp.partials = part; rp.st = sts;
+    cp.g = g; cp.ph = pl.ph; cp.twH = twH; cp.twW = twW; cp.F = F; cp.Dh = Dh; cp.Sh = Sh;
+    cp.grd = p->grd; cp.mu = p->mu; cp.wgrd = p->wgrd; cp.Psum = Psum; cp.st = sts;
+    fp.max_iter = o->max_iter;
+    fp.auto_rho = o->auto_rho; fp.period = std::max(1, o->auto_rho_period);
+    fp.auto_scaling = o->auto_scaling; fp.std_residuals = o->std_residuals;
+    fp.rho_scaling = o->rho_scaling; fp.rsdl_ratio = o->rsdl_ratio;
+    fp.abs_tol = o->abs_tol; fp.rel_tol = o->rel_tol;
+    fp.nelem = (double)g.M * g.H * g.W;
+    fp.xi = xi; fp.itstat = o->record_itstat ? it : nullptr; fp.ndone = ndone;
+    // Without a stopping tolerance only a non-finite residual can end the
+    // solve early; the host then never waits on the device mid-solve.
+    can_stop = o->rel_tol > 0.f || o->abs_tol > 0.f;
+    finished = o->max_iter <= 0;
+    return SC_OK;
+  }
+
+  // Iterations to launch before the next poll.
+  int chunk() const {
+    int c = o->max_iter - done_iters;
+    if (o->check_every > 0 && can_stop) c = std::min(c, o->check_every);
+    return c;
+  }
+
+  // Launch n ADMM iterations; timed(kind, launch) wraps every launch.
+  template <typename Timed>
+  int launch(int n, Timed&& timed) {
+    const int B = pl.g.B;
+    int st;
+    for (int i = 0; i < n; ++i) {
+      if ((st = timed(0, [&] {
+             return per_map_d ? launch_col<COL_SOLVE_W>(pl, cp, B, s)
+                              : launch_col<COL_SOLVE>(pl, cp, B, s);
+           })))
+        return st;
+      if ((st = timed(1, [&] { return launch_row<ROW_ITER>(pl, rp, B, s); }))) return st;
+      if ((st = timed(2, [&]() -> int {
+             finalize_kernel<<<B, 256, 0, s>>>(part, pl.row_nblk, sts, fp);
+             CU_TRY(cudaGetLastError());
+             ++g_launches;
+             return SC_OK;
+           })))
+        return st;
+      if (o->auto_rho) {
+        if ((st = timed(3, [&] { return launch_row<ROW_FIXUP>(pl, rp, B, s); }))) return st;
+      }
+    }
+    done_iters += n;
+    if (done_iters >= o->max_iter) finished = true;
+    return SC_OK;
+  }
+
+  // Wait for the launched iterations and stop when every image is finished.
+  int poll() {
+    if (finished) return SC_OK;
+    int nd = 0;
+    CU_TRY(cudaMemcpyAsync(&nd, ndone, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CU_TRY(cudaStreamSynchronize(s));
+    if (nd >= pl.g.B) finished = true;
+    return SC_OK;
+  }
+
+  int result(sc_result* res) {
+    if (!res) return SC_OK;
+    const int B = pl.g.B;
+    ImgState h0;
+    CU_TRY(cudaMemcpyAsync(&h0, sts, sizeof(ImgState), cudaMemcpyDeviceToHost, s));
+    CU_TRY(cudaStreamSynchronize(s));
+    res->iterations = h0.k;
+    res->rho = h0.rho;
+    res->r = h0.r;
+    res->s = h0.s;
+    if (B > 1) {
+      std::vector<ImgState> hs(B);
+      CU_TRY(cudaMemcpy(hs.data(), sts, sizeof(ImgState) * B, cudaMemcpyDeviceToHost));
+      for (auto& x : hs) res->iterations = std::max(res->iterations, x.k);
+      for (auto& x : hs)
+        if (x.status) return set_status(x.status, "non-finite residual");
+    }
+    if (h0.status) return set_status(h0.status, "non-finite residual");
+    return SC_OK;
+  }
+};
+
 extern "C" int sc_cbpdn_solve(const sc_problem* p, const sc_options* o, void* workspace,
                               size_t workspace_bytes, sc_result* res, void* stream) {
   set_status(SC_OK, nullptr);
   (void)cudaGetLastError();  // do not report an earlier call's error as ours
-  if (!p || !o) return set_status(SC_ERR_INVALID, "null problem or options");
-  Plan pl;
-  int st = plan_problem(p, o, &pl);
-  if (st) return st;
-  if (!workspace || workspace_bytes < pl.total)
-    return set_status(SC_ERR_WORKSPACE, "workspace of %zu bytes needed", pl.total);
-  if (((uintptr_t)workspace) & 255) return set_status(SC_ERR_WORKSPACE, "workspace not 256-byte aligned");
-  if (!p->D || !p->S || !p->lmbda || !p->rho0 || !p->Y)
-    return set_status(SC_ERR_INVALID, "null device pointer");
-  if (p->grd && !p->wgrd) return set_status(SC_ERR_INVALID, "grd problem without GradWeight");
-  if (p->l1_kind != SC_L1_SCALAR && !p->l1w) return set_status(SC_ERR_INVALID, "missing L1Weight");
-  if ((p->W % 4) == 0 && (((uintptr_t)p->Y) & 15))
-    return set_status(SC_ERR_INVALID, "Y must be 16-byte aligned");
+  Solve sv;
   cudaStream_t s = (cudaStream_t)stream;
-  const Geom& g = pl.g;
-
-  float* U; float2 *F, *Dh, *Sh, *twW, *twH; double *part, *it, *xi; ImgState* sts; int* ndone;
-  carve(pl, (unsigned char*)workspace, &U, &F, &Dh, &Sh, &twW, &twH, &part, &sts, &it, &xi, &ndone);
-  float* Psum = (float*)((unsigned char*)workspace + pl.off_Ps);
-  // one d for every map unless GradWeight differs between maps
-  const bool per_map_d = p->grd && !p->wgrd_uniform;
-
-  twiddle_kernel<<<(g.W + 255) / 256, 256, 0, s>>>(twW, g.W);
-  twiddle_kernel<<<(g.H + 255) / 256, 256, 0, s>>>(twH, g.H);
-  CU_TRY(cudaGetLastError());
-  g_launches += 2;
-
-  // Dictionary spectrum: rfft2 of the zero-padded filters (cuda_Pad_Dict +
-  // R2C, cbpdn.cu:277-289), computed without materialising the padding.
-  {
-    RowParams rp = {};
-    rp.g = g; rp.g.B = 1;
-    rp.pw = pl.pw; rp.twW = twW; rp.F = Dh; rp.D = p->D; rp.Kr = p->Kr; rp.Kc = p->Kc;
-    if ((st = launch_row<ROW_FWD_DICT>(pl, rp, 1, s))) return st;
-    ColParams cp = {};
-    cp.g = g; cp.g.B = 1; cp.ph = pl.ph; cp.twH = twH; cp.twW = twW; cp.F = Dh;
-    if ((st = launch_col<COL_FWD>(pl, cp, 1, s))) return st;
-    const size_t plane = (size_t)g.H * g.Wp;
-    psum_kernel<<<(unsigned)((plane + 255) / 256), 256, 0, s>>>(Dh, Psum, g.M, plane);
-    CU_TRY(cudaGetLastError());
-    ++g_launches;
-  }
-  // Signal spectra (B images, one map each).
-  {
-    RowParams rp = {};
-    rp.g = g; rp.g.M = 1;
-    rp.pw = pl.pw; rp.twW = twW; rp.F = Sh; rp.src = p->S;
-    const long npairs = ((long)g.H + 1) / 2;
-    const int S = SC_ROW_THREADS / pl.rowg_g;
-    const int nb = (int)std::max(1L, std::min((npairs + S - 1) / S, (long)num_sms()));
-    if ((st = launch_row<ROW_FWD_REAL>(pl, rp, g.B, s, nb))) return st;
-    ColParams cp = {};
-    cp.g = g; cp.g.M = 1; cp.ph = pl.ph; cp.twH = twH; cp.twW = twW; cp.F = Sh;
-    if ((st = launch_col<COL_FWD>(pl, cp, g.B, s))) return st;
-  }
-  const size_t real_all = (size_t)g.B * g.M * g.H * g.W;
-  CU_TRY(cudaMemsetAsync(p->Y, 0, sizeof(float) * real_all, s));
-  CU_TRY(cudaMemsetAsync(U, 0, sizeof(float) * real_all, s));
-  CU_TRY(cudaMemsetAsync(F, 0, sizeof(float2) * (size_t)g.B * g.M * g.H * g.Wp, s));
-  init_state_kernel<<<(g.B + 127) / 128, 128, 0, s>>>(sts, p->rho0, g.B, ndone);
-  xi_kernel<<<(g.B + 127) / 128, 128, 0, s>>>(xi, p->lmbda, g.B, o->rsdl_target, o->std_residuals);
-  CU_TRY(cudaGetLastError());
-  g_launches += 2;
-
-  RowParams rp = {};
-  rp.g = g; rp.pw = pl.pw; rp.twW = twW; rp.F = F; rp.Y = p->Y; rp.U = U;
-  rp.lam = p->lmbda; rp.l1_kind = p->l1_kind; rp.l1_scalar = p->l1_scalar; rp.l1w = p->l1w;
-  rp.mask = p->mask; rp.relax = o->relax; rp.invN = (float)(1.0 / ((double)g.H * g.W));
-  rp.partials = part; rp.st = sts;
-  ColParams cp = {};
-  cp.g = g; cp.ph = pl.ph; cp.twH = twH; cp.twW = twW; cp.F = F; cp.Dh = Dh; cp.Sh = Sh;
-  cp.grd = p->grd; cp.mu = p->mu; cp.wgrd = p->wgrd; cp.Psum = Psum; cp.st = sts;
-  FinParams fp = {};
-  fp.max_iter = o->max_iter;
-  fp.auto_rho = o->auto_rho; fp.period = std::max(1, o->auto_rho_period);
-  fp.auto_scaling = o->auto_scaling; fp.std_residuals = o->std_residuals;
-  fp.rho_scaling = o->rho_scaling; fp.rsdl_ratio = o->rsdl_ratio;
-  fp.abs_tol = o->abs_tol; fp.rel_tol = o->rel_tol;
-  fp.nelem = (double)g.M * g.H * g.W;
-  fp.xi = xi; fp.itstat = o->record_itstat ? it : nullptr; fp.ndone = ndone;
+  int st = sv.setup(p, o, workspace, workspace_bytes, s);
+  if (st) return st;
 
   // Per-kernel event timing (profile mode only); events come from a
   // grow-only pool so that profiling adds no per-launch host allocation.
@@ -487,38 +588,9 @@ extern "C" int sc_cbpdn_solve(const sc_problem* p, const sc_options* o, void* wo
     evs.push_back(e);
     return r;
   };
-  // Without a stopping tolerance only a non-finite residual can end the
-  // solve early; the host then never waits on the device mid-solve.
-  const bool can_stop = o->rel_tol > 0.f || o->abs_tol > 0.f;
-  int done_iters = 0;
-  while (done_iters < o->max_iter) {
-    int chunk = o->max_iter - done_iters;
-    if (o->check_every > 0 && can_stop) chunk = std::min(chunk, o->check_every);
-    for (int i = 0; i < chunk; ++i) {
-      if ((st = timed(0, [&] {
-             return per_map_d ? launch_col<COL_SOLVE_W>(pl, cp, g.B, s)
-                              : launch_col<COL_SOLVE>(pl, cp, g.B, s);
-           })))
-        return st;
-      if ((st = timed(1, [&] { return launch_row<ROW_ITER>(pl, rp, g.B, s); }))) return st;
-      if ((st = timed(2, [&]() -> int {
-             finalize_kernel<<<g.B, 256, 0, s>>>(part, pl.row_nblk, sts, fp);
-             CU_TRY(cudaGetLastError());
-             ++g_launches;
-             return SC_OK;
-           })))
-        return st;
-      if (o->auto_rho) {
-        if ((st = timed(3, [&] { return launch_row<ROW_FIXUP>(pl, rp, g.B, s); }))) return st;
-      }
-    }
-    done_iters += chunk;
-    if (done_iters < o->max_iter) {
-      int nd = 0;
-      CU_TRY(cudaMemcpyAsync(&nd, ndone, sizeof(int), cudaMemcpyDeviceToHost, s));
-      CU_TRY(cudaStreamSynchronize(s));
-      if (nd >= g.B) break;
-    }
+  while (!sv.finished) {
+    if ((st = sv.launch(sv.chunk(), timed))) return st;
+    if ((st = sv.poll())) return st;
   }
   if (o->profile) {
     CU_TRY(cudaStreamSynchronize(s));
@@ -530,23 +602,37 @@ extern "C" int sc_cbpdn_solve(const sc_problem* p, const sc_options* o, void* wo
       g_profile.count[e.kind] += 1;
     }
   }
-  if (res) {
-    ImgState h0;
-    CU_TRY(cudaMemcpyAsync(&h0, sts, sizeof(ImgState), cudaMemcpyDeviceToHost, s));
-    CU_TRY(cudaStreamSynchronize(s));
-    res->iterations = h0.k;
-    res->rho = h0.rho;
-    res->r = h0.r;
-    res->s = h0.s;
-    if (g.B > 1) {
-      std::vector<ImgState> hs(g.B);
-      CU_TRY(cudaMemcpy(hs.data(), sts, sizeof(ImgState) * g.B, cudaMemcpyDeviceToHost));
-      for (auto& x : hs) res->iterations = std::max(res->iterations, x.k);
-      for (auto& x : hs)
-        if (x.status) return set_status(x.status, "non-finite residual");
-    }
-    if (h0.status) return set_status(h0.status, "non-finite residual");
+  return sv.result(res);
+}
+
+extern "C" int sc_cbpdn_solve_batch(const sc_problem* probs, int nprob, const sc_options* o,
+                                    void* const* workspaces, const size_t* workspace_bytes,
+                                    sc_result* res, void* const* streams) {
+  set_status(SC_OK, nullptr);
+  (void)cudaGetLastError();
+  if (!probs || nprob < 1 || !o || !workspaces || !workspace_bytes)
+    return set_status(SC_ERR_INVALID, "invalid batch arguments");
+  if (o->profile) return set_status(SC_ERR_INVALID, "profiling is per single solve");
+  std::vector<Solve> sv(nprob);
+  int st;
+  for (int i = 0; i < nprob; ++i) {
+    cudaStream_t s = streams ? (cudaStream_t)streams[i] : nullptr;
+    if ((st = sv[i].setup(&probs[i], o, workspaces[i], workspace_bytes[i], s))) return st;
   }
+  auto untimed = [](int, auto&& launch) -> int { return launch(); };
+  for (;;) {
+    bool any = false;
+    for (auto& x : sv) {
+      if (x.finished) continue;
+      any = true;
+      if ((st = x.launch(x.chunk(), untimed))) return st;
+    }
+    if (!any) break;
+    for (auto& x : sv)
+      if ((st = x.poll())) return st;
+  }
+  for (int i = 0; i < nprob; ++i)
+    if ((st = sv[i].result(res ? &res[i] : nullptr))) return st;
   return SC_OK;
 }
 

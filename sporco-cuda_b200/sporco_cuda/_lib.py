@@ -134,6 +134,10 @@ sc_options_from_algopt = _proto("sc_options_from_algopt", None,
 sc_cbpdn_solve = _proto("sc_cbpdn_solve", C.c_int,
                         [C.POINTER(ScProblem), C.POINTER(ScOptions), C.c_void_p, C.c_size_t,
                          C.POINTER(ScResult), C.c_void_p])
+sc_cbpdn_solve_batch = _proto("sc_cbpdn_solve_batch", C.c_int,
+                              [C.POINTER(ScProblem), C.c_int, C.POINTER(ScOptions),
+                               C.POINTER(C.c_void_p), C.POINTER(C.c_size_t),
+                               C.POINTER(ScResult), C.POINTER(C.c_void_p)])
 sc_read_state = _proto("sc_read_state", C.c_int,
                        [C.POINTER(ScProblem), C.POINTER(ScOptions), C.c_void_p, IP,
                         C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p])
@@ -154,7 +158,7 @@ EXPORTED = [
     "cuda_wrapper_CBPDN", "cuda_wrapper_CBPDN_GR", "clear_opts", "default_opts",
     "check_cuda_req", "get_device_count", "get_current_device", "set_current_device",
     "get_memory_info", "get_device_name", "sc_workspace_size", "sc_options_from_algopt",
-    "sc_cbpdn_solve", "sc_read_state", "sc_rfft2", "sc_irfft2", "sc_rfft2_noalloc",
+    "sc_cbpdn_solve", "sc_cbpdn_solve_batch", "sc_read_state", "sc_rfft2", "sc_irfft2", "sc_rfft2_noalloc",
     "sc_last_profile",
     "sc_launch_count", "sc_last_status", "sc_last_error", "sc_version",
 ]

@@ -450,3 +450,83 @@ def cbpdngrdmsk(D, S, W, lmbda, mu, opt, dev=0):
     X = _host_solve(np.ascontiguousarray(np.rollaxis(Di, 2, 0)), np.ascontiguousarray(S),
                     np.ascontiguousarray(W, dtype=np.int32), lmbda, mu, opt, l1, g, dev, True)
     return np.rollaxis(X, 0, 3)[..., 1:]
+
+
+# ------------------------------------------------------------- batched form --
+
+def cbpdn_batched(D, S_list, lmbda, opt, W_list=None, mu=0.0, grd=False, streams=True,
+                  return_info=False):
+    """Solve many images of possibly different sizes with one dictionary.
+
+    No counterpart in the reference (which solves one image per call).
+    ``D``: (Kr, Kc, M) float32 (numpy or CUDA tensor); ``S_list``: sequence of
+    (H_i, W_i) float32 images; ``lmbda``: scalar or one value per image;
+    ``W_list``: optional per-image AMS masks (then the impulse filter is
+    prepended and map 0 dropped, as in ``cbpdnmsk``); ``grd``/``mu``: gradient
+    regularisation as in ``cbpdngrd``.  Every image keeps its own rho,
+    residuals and stopping state.  Images are grouped into buckets of equal
+    (H, W) (no padding: the circular-boundary problem is unchanged); each
+    bucket is one batched solve on its own CUDA stream, and the iterations
+    of all buckets are launched in turn by one host driver
+    (``sc_cbpdn_solve_batch``).  Returns a list of (H_i, W_i, M) results of
+    the input's array type (and, with ``return_info``, per-image iteration
+    counts)."""
+    import torch
+    n = len(S_list)
+    lam = np.broadcast_to(np.asarray(lmbda, dtype=F32), (n,))
+    as_torch = _is_torch(D)
+    dev = D.device if as_torch else torch.device("cuda", torch.cuda.current_device())
+    Dt = torch.as_tensor(D, device=dev).float()
+    ams = W_list is not None
+    M = Dt.shape[2]
+    if ams:
+        d0 = torch.zeros((Dt.shape[0], Dt.shape[1], 1), device=dev)
+        d0[0, 0] = 1.0
+        Dt = torch.cat((d0, Dt), dim=2)
+    Dm = Dt.permute(2, 0, 1).contiguous()
+    Mi = Dm.shape[0]
+    l1 = _opt_get(opt, "L1Weight")
+    gw = _opt_get(opt, "GradWeight") if grd else 1.0
+    if ams:
+        l1, gw = _ams_weights(None, Mi, {"L1Weight": _np(l1), "GradWeight": _np(gw)}, grd)
+    if hasattr(l1, "ndim") and np.ndim(l1) == 3:
+        l1 = np.ascontiguousarray(np.rollaxis(_np(l1), 2, 0))
+    buckets = {}
+    for i, s in enumerate(S_list):
+        buckets.setdefault(tuple(s.shape), []).append(i)
+    solves, order = [], []
+    for shape, idx in buckets.items():
+        S = torch.stack([torch.as_tensor(S_list[i], device=dev).float() for i in idx])
+        mask = None
+        if ams:
+            mask = torch.stack([torch.as_tensor(np.asarray(_np(W_list[i])), device=dev)
+                                .to(torch.int32) for i in idx])
+        ds = prepare_device(Dm, S, lam[idx], opt, mu=mu, grd=grd, l1=l1, gw=gw, mask=mask)
+        solves.append(ds)
+        order.append(idx)
+    k = len(solves)
+    probs = (_lib.ScProblem * k)(*[ds.prob for ds in solves])
+    wss = (C.c_void_p * k)(*[ds.ws.data_ptr() for ds in solves])
+    wsb = (C.c_size_t * k)(*[ds.ws.numel() for ds in solves])
+    res = (_lib.ScResult * k)()
+    strm = [torch.cuda.Stream(device=dev) if streams else torch.cuda.current_stream(dev)
+            for _ in range(k)]
+    cur = torch.cuda.current_stream(dev)
+    for st in strm:
+        st.wait_stream(cur)
+    sp = (C.c_void_p * k)(*[st.cuda_stream for st in strm])
+    _lib.check(_lib.sc_cbpdn_solve_batch(probs, k, C.byref(solves[0].opts), wss, wsb, res, sp))
+    for st in strm:
+        cur.wait_stream(st)
+    out = [None] * n
+    iters = [0] * n
+    for ds, idx in zip(solves, order):
+        Y = ds.keep["Y"]
+        info = ds.state()
+        for j, i in enumerate(idx):
+            X = Y[j].permute(1, 2, 0)
+            if ams:
+                X = X[..., 1:]
+            out[i] = X if as_torch else X.contiguous().cpu().numpy()
+            iters[i] = info["iterations"][j]
+    return (out, iters) if return_info else out

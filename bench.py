@@ -65,6 +65,10 @@ CONFIGS = {
             H=None, W=None, M=64, K=12, density=0.005, lmbda=None, mu=0.0,
             variants=["cbpdnmsk"], iters=1000, autorho=True, mask_p=None, nimg=64,
             sides=(128, 192, 256, 384, 512, 768, 1024)),
+    3: dict(workload="differentiable cbpdn: 16 images 256x256, M=32 11x11, 200 unrolled "
+                     "iterations, loss ||D*X - S_clean||^2 + 0.01||X||_1, backward to D and S",
+            H=256, W=256, M=32, K=11, density=0.01, lmbda=0.05, mu=0.0, nimg=16,
+            variants=["cbpdn"], iters=200, autorho=False, mask_p=None),
     # small 2048x2048 case for kernel profiles (2 GB on the device)
     9: dict(workload="cbpdn 2048x2048 M=24 16x16, 20 iterations, AutoRho (profiling case)",
             H=2048, W=2048, M=24, K=16, density=0.01, lmbda=0.02, mu=0.0,
@@ -514,6 +518,95 @@ def run_batched(args, cfg, rank, world, local_rank):
     }
 
 
+def run_adjoint(args, cfg, rank, world, local_rank):
+    """Config 3: forward + backward of the unrolled solve; image-iterations/s
+    of forward+backward, and the backward/forward time ratio."""
+    import torch
+    import sporco_cuda.adjoint as adj
+    import sporco_cuda.cbpdn as cb
+    from sporco_cuda import _lib
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    B = cfg["nimg"]
+    imgs = []
+    D = None
+    for b in range(B):
+        Db, Sb, _ = synth(cfg, 12345 + args.config + 100 * b + rank, dev)
+        if D is None:
+            D = Db
+        imgs.append(Sb)
+    # one dictionary for the batch: re-synthesise every clean image from D
+    g = torch.Generator(device=dev).manual_seed(777 + rank)
+    H, W, M, K = cfg["H"], cfg["W"], cfg["M"], cfg["K"]
+    X0 = (torch.rand((B, H, W, M), generator=g, device=dev) < cfg["density"]).float() * \
+        torch.randn((B, H, W, M), generator=g, device=dev)
+    Dk = D.permute(1, 2, 0).contiguous()
+    with torch.no_grad():
+        Sc = adj.reconstruct(Dk, X0)
+        Sc = Sc - Sc.mean(dim=(1, 2), keepdim=True)
+    S = Sc + 0.05 * torch.randn((B, H, W), generator=g, device=dev)
+    opt = {"MaxMainIter": cfg["iters"], "RelStopTol": 0.0, "RelaxParam": 1.8, "rho": None,
+           "AutoRho": {"Enabled": False}}
+
+    def fwd_bwd():
+        Dg = Dk.clone().requires_grad_(True)
+        Sg = S.clone().requires_grad_(True)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t2 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        X = adj.cbpdn_unrolled(Dg, Sg, cfg["lmbda"], opt)
+        R = adj.reconstruct(Dg, X)
+        L = torch.sum((R - Sc) ** 2) + 0.01 * torch.sum(torch.abs(X))
+        t1.record()
+        L.backward()
+        t2.record()
+        torch.cuda.synchronize()
+        return t0.elapsed_time(t1), t1.elapsed_time(t2)
+
+    for _ in range(args.warmup):
+        fwd_bwd()
+    torch.cuda.synchronize()
+    n0 = _lib.sc_launch_count()
+    f_ms = b_ms = 0.0
+    with ClockSampler(local_rank) as clk:
+        for _ in range(args.steps):
+            f, b_ = fwd_bwd()
+            f_ms += f
+            b_ms += b_
+    launches = _lib.sc_launch_count() - n0
+    ms = f_ms + b_ms
+    value = world * B * cfg["iters"] * args.steps / (ms / 1e3)
+    # the fused solver on the same batch, for reference
+    ds = cb.prepare_device(D, S, cfg["lmbda"], opt)
+    ds.run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ds.run()
+    e1.record()
+    torch.cuda.synchronize()
+    fused_ms = e0.elapsed_time(e1)
+    peak, peak_kind = measured_peaks()
+    if rank != 0:
+        return None
+    return {
+        "metric": METRIC, "value": value, "unit": "image-iter/s (forward+backward)",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "images": B, "H": H, "W": W, "M": M, "K": K,
+                   "iterations": cfg["iters"], "checkpoints": "every ceil(sqrt(K)) iterations",
+                   "l2": "working set larger than L2 (no flush)"},
+        "forward_ms": f_ms / args.steps, "backward_ms": b_ms / args.steps,
+        "backward_over_forward": b_ms / f_ms,
+        "fused_forward_solve_ms": fused_ms,
+        "backward_over_fused_forward": (b_ms / args.steps) / fused_ms,
+        "e2e": None, "roofline": None, "cpu_baseline": None, "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+
+
 def run_reference(args, cfg, rank):
     """The reference algorithm on the host cores (FP64 restatement)."""
     if rank != 0:
@@ -582,6 +675,8 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     if args.config == 2:
         out = run_batched(args, cfg, rank, world, local_rank)
+    elif args.config == 3:
+        out = run_adjoint(args, cfg, rank, world, local_rank)
     else:
         out = run_ours(args, cfg, rank, world, local_rank)
     if out is not None:

@@ -206,6 +206,22 @@ int sc_last_profile(sc_profile *out);
 /* Number of kernels this library has launched since it was loaded. */
 unsigned long long sc_launch_count(void);
 
+/* Building blocks of the adjoint of the unrolled cbpdn iteration (no
+ * counterpart in the reference; plain cbpdn, fixed rho).  Spectra are dense
+ * (count, H, W/2+1) complex64, maps (B, M, H, W) float32, device pointers.
+ * sc_adj_freq mode 0: io = Z^ -> X^ = A^{-1}(conj(Df) S^ + rho Z^);
+ *             mode 1: io = gX^ -> Q^ = A^{-1} gX^, accumulating gD^ (M, H, W/2+1)
+ *             and gS^ (B, H, W/2+1) from X^ (the step's forward solution).
+ * sc_adj_elem mode 0: out = Y - U; 1: (Y, U) <- y/u step from X;
+ *             2: from gY', gU' and the step's X, Y, U: out = gX, gY <- (1-a) gV,
+ *                gU <- gV;  3: gY += rho Q, gU -= rho Q with Q in X. */
+int sc_adj_freq(int mode, int B, int M, int H, int W, float rho, const void *Dh,
+                const void *Sh, void *io, const void *Xh, void *gDh, void *gSh, void *stream);
+int sc_adj_elem(int mode, int B, int M, int H, int W, float rho, float alpha,
+                const float *lam, int l1_kind, float l1_scalar, const float *l1w,
+                const float *X, float *Y, float *U, float *gY, float *gU, float *out,
+                void *stream);
+
 /* Last status / message recorded on the calling thread. */
 int sc_last_status(void);
 const char *sc_last_error(void);

@@ -1,0 +1,107 @@
+"""Gradients of the unrolled CBPDN solve (hand-written adjoint) against torch
+autograd of an FP64 unrolled reference and FP64 central finite differences."""
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from oracle import adjoint_oracle as A
+from oracle import cbpdn_oracle as O
+
+F32 = np.float32
+
+
+def _problem(B=2, H=24, W=20, M=3, K=5, seed=0):
+    rng = np.random.default_rng(seed)
+    D = rng.standard_normal((K, K, M))
+    D /= np.sqrt(np.sum(D * D, axis=(0, 1), keepdims=True))
+    Sc = rng.standard_normal((B, H, W)) * 0.5
+    S = Sc + 0.05 * rng.standard_normal((B, H, W))
+    return D.astype(F32), S.astype(F32), Sc.astype(F32)
+
+
+LAM, BETA, ITERS = 0.05, 0.01, 12
+
+
+def _opt():
+    return {"MaxMainIter": ITERS, "RelStopTol": 0.0, "RelaxParam": 1.8, "rho": None,
+            "AutoRho": {"Enabled": False}}
+
+
+def _consts():
+    lam = float(F32(LAM))
+    return lam, float(F32(50 * lam + 1)), float(F32(1.8))
+
+
+def test_fp64_reference_gradient_matches_finite_differences():
+    D, S, Sc, = _problem()
+    lam, rho, alpha = _consts()
+    Dt = torch.tensor(D, dtype=torch.float64, requires_grad=True)
+    St = torch.tensor(S, dtype=torch.float64, requires_grad=True)
+    L = A.loss(Dt, St, torch.tensor(Sc, dtype=torch.float64), lam, rho, alpha, ITERS, BETA)
+    L.backward()
+    rng = np.random.default_rng(5)
+    for G, base, which in ((Dt.grad, D, "D"), (St.grad, S, "S")):
+        dirn = rng.standard_normal(base.shape)
+        eps = 1e-6
+
+        def f(x):
+            d = torch.tensor(D, dtype=torch.float64) if which == "S" else x
+            s = torch.tensor(S, dtype=torch.float64) if which == "D" else x
+            return float(A.loss(d, s, torch.tensor(Sc, dtype=torch.float64), lam, rho, alpha,
+                                ITERS, BETA))
+        x0 = torch.tensor(base, dtype=torch.float64)
+        dd = torch.tensor(dirn)
+        fd = (f(x0 + eps * dd) - f(x0 - eps * dd)) / (2 * eps)
+        an = float(torch.sum(G * dd))
+        assert abs(fd - an) <= 1e-5 * max(1.0, abs(an)), (which, fd, an)
+
+
+@pytest.mark.gpu
+def test_unrolled_forward_matches_oracle():
+    import sporco_cuda.adjoint as adj
+    D, S, _ = _problem()
+    X = adj.cbpdn_unrolled(torch.tensor(D, device="cuda"), torch.tensor(S, device="cuda"),
+                           LAM, _opt())
+    for b in range(S.shape[0]):
+        Xo = O.cbpdn(D, S[b], LAM, _opt())
+        rel = np.linalg.norm(X[b].cpu().numpy() - Xo) / np.linalg.norm(Xo)
+        assert rel < 1e-4
+
+
+@pytest.mark.gpu
+def test_unrolled_gradients_match_fp64_autograd_and_fd():
+    import sporco_cuda.adjoint as adj
+    D, S, Sc = _problem()
+    lam, rho, alpha = _consts()
+    Dg = torch.tensor(D, device="cuda", requires_grad=True)
+    Sg = torch.tensor(S, device="cuda", requires_grad=True)
+    X = adj.cbpdn_unrolled(Dg, Sg, LAM, _opt())
+    R = adj.reconstruct(Dg, X)
+    L = torch.sum((R - torch.tensor(Sc, device="cuda")) ** 2) + BETA * torch.sum(torch.abs(X))
+    L.backward()
+    Dt = torch.tensor(D, dtype=torch.float64, requires_grad=True)
+    St = torch.tensor(S, dtype=torch.float64, requires_grad=True)
+    Lr = A.loss(Dt, St, torch.tensor(Sc, dtype=torch.float64), lam, rho, alpha, ITERS, BETA)
+    Lr.backward()
+    assert abs(float(L) - float(Lr)) / float(Lr) < 1e-5
+    for g, r in ((Dg.grad, Dt.grad), (Sg.grad, St.grad)):
+        g = g.double().cpu()
+        rel = float(torch.linalg.norm(g - r) / torch.linalg.norm(r))
+        assert rel < 1e-4, rel
+    # directional finite differences of the FP64 loss against the GPU gradient
+    rng = np.random.default_rng(7)
+    eps = 1e-6
+    for g, base, which in ((Dg.grad, D, "D"), (Sg.grad, S, "S")):
+        dd = rng.standard_normal(base.shape)
+
+        def f(x):
+            d = torch.tensor(D, dtype=torch.float64) if which == "S" else x
+            s = torch.tensor(S, dtype=torch.float64) if which == "D" else x
+            return float(A.loss(d, s, torch.tensor(Sc, dtype=torch.float64), lam, rho, alpha,
+                                ITERS, BETA))
+        x0 = torch.tensor(base, dtype=torch.float64)
+        fd = (f(x0 + eps * torch.tensor(dd)) - f(x0 - eps * torch.tensor(dd))) / (2 * eps)
+        an = float(np.sum(g.double().cpu().numpy() * dd))
+        assert abs(fd - an) <= 1e-4 * max(1.0, abs(fd)), (which, fd, an)

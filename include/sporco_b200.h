@@ -146,6 +146,9 @@ typedef struct sc_problem {
   const int32_t *mask;   /* (B, H, W) AMS mask, map 0 is the impulse; NULL: none */
   float *Y;              /* (B, M, H, W) output; also the Y iterate */
   int wgrd_uniform;      /* grd only: 1 when all M GradWeight entries are equal */
+  const float *U0;       /* (B, M, H, W) or NULL: start from Y (as given) and U0
+                            instead of Y = U = 0 */
+  float *U_out;          /* (B, M, H, W) or NULL: receives the final U */
 } sc_problem;
 
 typedef struct sc_result {
@@ -210,7 +213,8 @@ unsigned long long sc_launch_count(void);
  * counterpart in the reference; plain cbpdn, fixed rho).  Spectra are dense
  * (count, H, W/2+1) complex64, maps (B, M, H, W) float32, device pointers.
  * sc_adj_freq mode 0: io = Z^ -> X^ = A^{-1}(conj(Df) S^ + rho Z^);
- *             mode 1: io = gX^ -> Q^ = A^{-1} gX^, accumulating gD^ (M, H, W/2+1)
+ *             mode 1: io = gX^ -> Q^ = A^{-1} gX^, accumulating gD^ per image
+ *             (B, M, H, W/2+1; sum over the images for the dictionary gradient)
  *             and gS^ (B, H, W/2+1) from X^ (the step's forward solution).
  * sc_adj_elem mode 0: out = Y - U; 1: (Y, U) <- y/u step from X;
  *             2: from gY', gU' and the step's X, Y, U: out = gX, gY <- (1-a) gV,

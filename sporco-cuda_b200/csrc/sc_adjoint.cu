@@ -33,8 +33,6 @@ int fail(cudaError_t e, const char* what) {
   return sc_set_status_external(e == cudaErrorMemoryAllocation ? SC_ERR_OOM : SC_ERR_CUDA, b);
 }
 
-constexpr int ADJ_BCHUNK = 16;  // images handled per register block
-
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
@@ -43,94 +41,67 @@ __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
   return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
 
-// One thread per frequency f of the (H, W/2+1) grid, all images and maps.
+// One thread per (frequency f of the (H, W/2+1) grid, image b), all maps.
 //  mode 0: io holds Z^ = rfft2(Y - U); replaced by X^ = A^{-1}(conj(Df) S^ + rho Z^)
-//  mode 1: io holds gX^; replaced by Q^ = A^{-1} gX^; gD^ and gS^ accumulate
+//  mode 1: io holds gX^; replaced by Q^ = A^{-1} gX^; the image's part of gD^
+//          accumulates in gDh[b] (B, M, H, W/2+1), gS^ in gSh[b]
 __global__ void adj_freq_kernel(int mode, int B, int M, int Fn, float rho,
                                 const float2* __restrict__ Dh, const float2* __restrict__ Sh,
                                 float2* io, const float2* __restrict__ Xh, float2* gDh,
                                 float2* gSh) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y;
   if (f >= Fn) return;
   const size_t plane = (size_t)Fn;
+  const size_t ib = (size_t)b * M * plane + f;
+  const float2 Sv = __ldg(&Sh[(size_t)b * plane + f]);
   float sden = 0.f;
+  // dot = sum_m Df_m v_m, v = conj(Df) S + rho Z (mode 0) or gX (mode 1)
+  float2 dot = make_float2(0.f, 0.f), DX = make_float2(0.f, 0.f);
   for (int m = 0; m < M; ++m) {
     const float2 d = __ldg(&Dh[m * plane + f]);
     sden += d.x * d.x + d.y * d.y;
+    float2 vm = io[ib + m * plane];
+    if (mode == 0) {
+      const float2 ds = cmulc(Sv, d);  // conj(Df) S
+      vm = make_float2(ds.x + rho * vm.x, ds.y + rho * vm.y);
+    } else {
+      const float2 dx = cmul(d, __ldg(&Xh[ib + m * plane]));
+      DX.x += dx.x;
+      DX.y += dx.y;
+    }
+    const float2 p = cmul(d, vm);
+    dot.x += p.x;
+    dot.y += p.y;
   }
-  const float inv = 1.f / (rho + sden);
-  const float irho = 1.f / rho;
-  for (int b0 = 0; b0 < B; b0 += ADJ_BCHUNK) {
-    const int nb = min(ADJ_BCHUNK, B - b0);
-    float2 DX[ADJ_BCHUNK], DQ[ADJ_BCHUNK], Sv[ADJ_BCHUNK];
-#pragma unroll
-    for (int j = 0; j < ADJ_BCHUNK; ++j) {
-      DX[j] = DQ[j] = Sv[j] = make_float2(0.f, 0.f);
-      if (j < nb) Sv[j] = __ldg(&Sh[(size_t)(b0 + j) * plane + f]);
+  const float inv = 1.f / (rho + sden), irho = 1.f / rho;
+  const float2 c = make_float2(dot.x * inv, dot.y * inv);
+  float2 DQ = make_float2(0.f, 0.f);
+  for (int m = 0; m < M; ++m) {
+    const float2 d = __ldg(&Dh[m * plane + f]);
+    float2 vm = io[ib + m * plane];
+    if (mode == 0) {
+      const float2 ds = cmulc(Sv, d);
+      vm = make_float2(ds.x + rho * vm.x, ds.y + rho * vm.y);
     }
-#pragma unroll
-    for (int j = 0; j < ADJ_BCHUNK; ++j) {
-      if (j >= nb) break;
-      const int b = b0 + j;
-      float2* v = io + (size_t)b * M * plane + f;
-      // dot = sum_m Df_m v_m, v = conj(Df) S + rho Z (mode 0) or gX (mode 1)
-      float2 dot = make_float2(0.f, 0.f);
-      for (int m = 0; m < M; ++m) {
-        const float2 d = __ldg(&Dh[m * plane + f]);
-        float2 vm = v[m * plane];
-        if (mode == 0) {
-          const float2 ds = cmulc(Sv[j], d);  // conj(Df) S
-          vm = make_float2(ds.x + rho * vm.x, ds.y + rho * vm.y);
-        } else {
-          const float2 x = __ldg(&Xh[(size_t)b * M * plane + m * plane + f]);
-          const float2 dx = cmul(d, x);
-          DX[j].x += dx.x;
-          DX[j].y += dx.y;
-        }
-        const float2 p = cmul(d, vm);
-        dot.x += p.x;
-        dot.y += p.y;
-      }
-      const float2 c = make_float2(dot.x * inv, dot.y * inv);
-      for (int m = 0; m < M; ++m) {
-        const float2 d = __ldg(&Dh[m * plane + f]);
-        float2 vm = v[m * plane];
-        if (mode == 0) {
-          const float2 ds = cmulc(Sv[j], d);
-          vm = make_float2(ds.x + rho * vm.x, ds.y + rho * vm.y);
-        }
-        const float2 dc = cmulc(c, d);  // conj(Df) c
-        const float2 out = make_float2((vm.x - dc.x) * irho, (vm.y - dc.y) * irho);
-        v[m * plane] = out;
-        if (mode == 1) {
-          const float2 dq = cmul(d, out);
-          DQ[j].x += dq.x;
-          DQ[j].y += dq.y;
-        }
-      }
-      if (mode == 1) {
-        float2* gs = gSh + (size_t)b * plane + f;
-        *gs = make_float2(gs->x + DQ[j].x, gs->y + DQ[j].y);
-      }
-    }
+    const float2 dc = cmulc(c, d);  // conj(Df) c
+    const float2 out = make_float2((vm.x - dc.x) * irho, (vm.y - dc.y) * irho);
+    io[ib + m * plane] = out;
     if (mode == 1) {
-      for (int m = 0; m < M; ++m) {
-        float2 acc = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int j = 0; j < ADJ_BCHUNK; ++j) {
-          if (j >= nb) break;
-          const size_t i = (size_t)(b0 + j) * M * plane + m * plane + f;
-          const float2 q = io[i];
-          const float2 x = __ldg(&Xh[i]);
-          const float2 t1 = cmulc(Sv[j], q);
-          const float2 t2 = cmulc(DX[j], q);
-          const float2 t3 = cmulc(DQ[j], x);
-          acc.x += t1.x - t2.x - t3.x;
-          acc.y += t1.y - t2.y - t3.y;
-        }
-        float2* g = gDh + m * plane + f;
-        *g = make_float2(g->x + acc.x, g->y + acc.y);
-      }
+      const float2 dq = cmul(d, out);
+      DQ.x += dq.x;
+      DQ.y += dq.y;
+    }
+  }
+  if (mode == 1) {
+    float2* gs = gSh + (size_t)b * plane + f;
+    *gs = make_float2(gs->x + DQ.x, gs->y + DQ.y);
+    for (int m = 0; m < M; ++m) {
+      const float2 q = io[ib + m * plane];
+      const float2 x = __ldg(&Xh[ib + m * plane]);
+      const float2 t1 = cmulc(Sv, q), t2 = cmulc(DX, q), t3 = cmulc(DQ, x);
+      float2* g = gDh + ib + m * plane;
+      *g = make_float2(g->x + t1.x - t2.x - t3.x, g->y + t1.y - t2.y - t3.y);
     }
   }
 }
@@ -192,7 +163,7 @@ extern "C" int sc_adj_freq(int mode, int B, int M, int H, int W, float rho, cons
       !Sh || !io || (mode == 1 && (!Xh || !gDh || !gSh)))
     return sc_set_status_external(SC_ERR_INVALID, "sc_adj_freq: invalid arguments");
   const int Fn = H * (W / 2 + 1);
-  adj_freq_kernel<<<(Fn + 127) / 128, 128, 0, (cudaStream_t)stream>>>(
+  adj_freq_kernel<<<dim3((Fn + 127) / 128, B), 128, 0, (cudaStream_t)stream>>>(
       mode, B, M, Fn, rho, (const float2*)Dh, (const float2*)Sh, (float2*)io, (const float2*)Xh,
       (float2*)gDh, (float2*)gSh);
   cudaError_t e = cudaGetLastError();

@@ -100,7 +100,10 @@ struct ColParams {
   ImgState* st;
 };
 
-enum RowMode { ROW_ITER = 0, ROW_FWD_REAL = 1, ROW_FWD_DICT = 2, ROW_INV_REAL = 3, ROW_FIXUP = 4 };
+enum RowMode {
+  ROW_ITER = 0, ROW_FWD_REAL = 1, ROW_FWD_DICT = 2, ROW_INV_REAL = 3, ROW_FIXUP = 4,
+  ROW_FWD_YU = 5  // row spectra of Y - U (start from given iterates)
+};
 // COL_SOLVE: all maps share d (cbpdn, or cbpdngrd with one GradWeight), so
 // sum_m |Df_m|^2 / d comes from the precomputed Psum; COL_SOLVE_W: per-map
 // d_m = mu w_m |G|^2 + rho, the sum is accumulated over the maps.

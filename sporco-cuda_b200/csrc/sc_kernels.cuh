@@ -346,6 +346,11 @@ row_kernel(RowParams P) {
         } else if constexpr (MODE == ROW_FIXUP) {
           const float* U0 = P.U + (size_t)b * img_real + (size_t)r0 * W;
           for (int k = t; k < W; k += g) z[zs(k)] = make_float2(U0[k], has1 ? U0[W + k] : 0.f);
+        } else if constexpr (MODE == ROW_FWD_YU) {
+          const float* Y0 = P.Y + (size_t)b * img_real + (size_t)r0 * W;
+          const float* U0 = P.U + (size_t)b * img_real + (size_t)r0 * W;
+          for (int k = t; k < W; k += g)
+            z[zs(k)] = make_float2(Y0[k] - U0[k], has1 ? Y0[W + k] - U0[W + k] : 0.f);
         }
       }
       __syncthreads();
@@ -757,4 +762,12 @@ __global__ void twiddle_kernel(float2* tw, int n) {
   double s, c;
   sincospi(-2.0 * (double)j / (double)n, &s, &c);
   tw[j] = make_float2((float)c, (float)s);
+}
+
+// out = U scaled to the value the next iteration would read (U * uscale).
+__global__ void export_u_kernel(const float* __restrict__ U, float* __restrict__ out,
+                                const ImgState* __restrict__ st, size_t per_img, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = U[i] * (float)st[i / per_img].uscale;
 }

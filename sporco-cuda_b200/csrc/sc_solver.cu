@@ -455,9 +455,18 @@ struct Solve {
       if ((st = launch_col<COL_FWD>(pl, c, g.B, s))) return st;
     }
     const size_t real_all = (size_t)g.B * g.M * g.H * g.W;
-    CU_TRY(cudaMemsetAsync(p->Y, 0, sizeof(float) * real_all, s));
-    CU_TRY(cudaMemsetAsync(U, 0, sizeof(float) * real_all, s));
-    CU_TRY(cudaMemsetAsync(F, 0, sizeof(float2) * (size_t)g.B * g.M * g.H * g.Wp, s));
+    if (p->U0) {
+      // start from the given iterates: U from U0, Y as given, F = rowFFT(Y - U)
+      CU_TRY(cudaMemcpyAsync(U, p->U0, sizeof(float) * real_all, cudaMemcpyDeviceToDevice, s));
+      CU_TRY(cudaMemsetAsync(F, 0, sizeof(float2) * (size_t)g.B * g.M * g.H * g.Wp, s));
+      RowParams r = {};
+      r.g = g; r.pw = pl.pw; r.twW = twW; r.F = F; r.Y = p->Y; r.U = U;
+      if ((st = launch_row<ROW_FWD_YU>(pl, r, g.B, s))) return st;
+    } else {
+      CU_TRY(cudaMemsetAsync(p->Y, 0, sizeof(float) * real_all, s));
+      CU_TRY(cudaMemsetAsync(U, 0, sizeof(float) * real_all, s));
+      CU_TRY(cudaMemsetAsync(F, 0, sizeof(float2) * (size_t)g.B * g.M * g.H * g.Wp, s));
+    }
     init_state_kernel<<<(g.B + 127) / 128, 128, 0, s>>>(sts, p->rho0, g.B, ndone);
     xi_kernel<<<(g.B + 127) / 128, 128, 0, s>>>(xi, p->lmbda, g.B, o->rsdl_target,
                                                  o->std_residuals);
@@ -529,7 +538,19 @@ struct Solve {
     return SC_OK;
   }
 
+  int export_u() {
+    if (!p->U_out) return SC_OK;
+    const size_t per = (size_t)pl.g.M * pl.g.H * pl.g.W, n = per * pl.g.B;
+    export_u_kernel<<<(unsigned)std::min<size_t>((n + 255) / 256, 4096), 256, 0, s>>>(
+        U, p->U_out, sts, per, n);
+    CU_TRY(cudaGetLastError());
+    ++g_launches;
+    return SC_OK;
+  }
+
   int result(sc_result* res) {
+    int st = export_u();
+    if (st) return st;
     if (!res) return SC_OK;
     const int B = pl.g.B;
     ImgState h0;
@@ -659,6 +680,32 @@ extern "C" int sc_read_state(const sc_problem* p, const sc_options* o, const voi
 }
 
 // --------------------------------------------------------------- rfft2 tools --
+// Twiddle tables of the FFT tool entry points, kept per (device, W, H) for
+// the life of the process (a handful of sizes in practice).
+struct TwEntry {
+  int dev, W, H;
+  float2* tw;
+};
+static std::vector<TwEntry> g_tw_cache;
+
+static int tool_twiddles(int W, int H, cudaStream_t s, float2** out) {
+  int dev = 0;
+  CU_TRY(cudaGetDevice(&dev));
+  for (auto& e : g_tw_cache)
+    if (e.dev == dev && e.W == W && e.H == H) {
+      *out = e.tw;
+      return SC_OK;
+    }
+  float2* tw = nullptr;
+  CU_TRY(cudaMalloc((void**)&tw, sizeof(float2) * (W + H)));
+  twiddle_kernel<<<(W + 255) / 256, 256, 0, s>>>(tw, W);
+  twiddle_kernel<<<(H + 255) / 256, 256, 0, s>>>(tw + W, H);
+  CU_TRY(cudaGetLastError());
+  g_tw_cache.push_back({dev, W, H, tw});
+  *out = tw;
+  return SC_OK;
+}
+
 extern "C" int sc_rfft2(const float* x, void* xf, int count, int H, int W, void* stream) {
   set_status(SC_OK, nullptr);
   (void)cudaGetLastError();
@@ -668,16 +715,13 @@ extern "C" int sc_rfft2(const float* x, void* xf, int count, int H, int W, void*
   cudaStream_t s = (cudaStream_t)stream;
   pl.g.Wp = pl.g.Wf;  // dense numpy layout
   float2* tw = nullptr;
-  CU_TRY(cudaMallocAsync((void**)&tw, sizeof(float2) * (W + H), s));
-  twiddle_kernel<<<(W + 255) / 256, 256, 0, s>>>(tw, W);
-  twiddle_kernel<<<(H + 255) / 256, 256, 0, s>>>(tw + W, H);
+  if ((st = tool_twiddles(W, H, s, &tw))) return st;
   RowParams rp = {};
   rp.g = pl.g; rp.pw = pl.pw; rp.twW = tw; rp.F = (float2*)xf; rp.src = x;
   if ((st = launch_row<ROW_FWD_REAL>(pl, rp, count, s))) return st;
   ColParams cp = {};
   cp.g = pl.g; cp.ph = pl.ph; cp.twH = tw + W; cp.twW = tw; cp.F = (float2*)xf;
   if ((st = launch_col<COL_FWD>(pl, cp, count, s))) return st;
-  CU_TRY(cudaFreeAsync(tw, s));
   return SC_OK;
 }
 
@@ -692,11 +736,9 @@ extern "C" int sc_irfft2(const void* xf, float* x, int count, int H, int W, void
   float2* tw = nullptr;
   float2* tmp = nullptr;
   const size_t nspec = (size_t)count * H * pl.g.Wf;
-  CU_TRY(cudaMallocAsync((void**)&tw, sizeof(float2) * (W + H), s));
+  if ((st = tool_twiddles(W, H, s, &tw))) return st;
   CU_TRY(cudaMallocAsync((void**)&tmp, sizeof(float2) * nspec, s));
   CU_TRY(cudaMemcpyAsync(tmp, xf, sizeof(float2) * nspec, cudaMemcpyDeviceToDevice, s));
-  twiddle_kernel<<<(W + 255) / 256, 256, 0, s>>>(tw, W);
-  twiddle_kernel<<<(H + 255) / 256, 256, 0, s>>>(tw + W, H);
   ColParams cp = {};
   cp.g = pl.g; cp.ph = pl.ph; cp.twH = tw + W; cp.twW = tw; cp.F = tmp;
   if ((st = launch_col<COL_INV>(pl, cp, count, s))) return st;
@@ -705,7 +747,6 @@ extern "C" int sc_irfft2(const void* xf, float* x, int count, int H, int W, void
   rp.invN = (float)(1.0 / ((double)H * W));
   if ((st = launch_row<ROW_INV_REAL>(pl, rp, count, s))) return st;
   CU_TRY(cudaFreeAsync(tmp, s));
-  CU_TRY(cudaFreeAsync(tw, s));
   return SC_OK;
 }
 

@@ -96,6 +96,7 @@ class ScProblem(C.Structure):
         ("grd", C.c_int), ("mu", C.c_float), ("wgrd", C.c_void_p),
         ("l1_kind", C.c_int), ("l1_scalar", C.c_float), ("l1w", C.c_void_p),
         ("mask", C.c_void_p), ("Y", C.c_void_p), ("wgrd_uniform", C.c_int),
+        ("U0", C.c_void_p), ("U_out", C.c_void_p),
     ]
 
 

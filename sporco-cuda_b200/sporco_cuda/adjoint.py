@@ -25,7 +25,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .cbpdn import F32, _opt_get, resolve_options
+from .cbpdn import F32, _opt_get, prepare_device, resolve_options
 
 __all__ = ["cbpdn_unrolled", "reconstruct", "rfft2", "irfft2"]
 
@@ -128,10 +128,18 @@ class _Unrolled(torch.autograd.Function):
         U = torch.zeros_like(Y)
         seg = max(1, int(math.ceil(math.sqrt(c.K))))
         ckpt = []
-        for k in range(c.K):
-            if k % seg == 0:
-                ckpt.append((k, Y.clone(), U.clone()))
-            c.step(Y, U)
+        # the fused solver, run segment by segment from each checkpoint
+        fopt = dict(opt)
+        fopt.update({"RelStopTol": 0.0, "AbsStopTol": 0.0, "rho": c.rho,
+                     "AutoRho": {"Enabled": False}})
+        l1 = c.l1w if c.l1w is not None else c.l1_scalar
+        ds = prepare_device(Dm, Sb, lmbda, fopt, l1=l1, Y=Y, check_every=0)
+        ds.prob.U_out = U.data_ptr()
+        for k0 in range(0, c.K, seg):
+            ckpt.append((k0, Y.clone(), U.clone()))
+            ds.opts.max_iter = min(seg, c.K - k0)
+            ds.prob.U0 = U.data_ptr() if k0 > 0 else None
+            ds.run()
         ctx.c, ctx.seg, ctx.ckpt = c, seg, ckpt
         ctx.dshape = D.shape
         return Y.permute(0, 2, 3, 1).contiguous()
@@ -142,7 +150,7 @@ class _Unrolled(torch.autograd.Function):
         gY = gX.detach().permute(0, 3, 1, 2).contiguous().float()
         gU = torch.zeros_like(gY)
         Wf = c.W // 2 + 1
-        gDh = torch.zeros((c.M, c.H, Wf), dtype=torch.complex64, device=gY.device)
+        gDh = torch.zeros((c.B, c.M, c.H, Wf), dtype=torch.complex64, device=gY.device)
         gSh = torch.zeros((c.B, c.H, Wf), dtype=torch.complex64, device=gY.device)
         gXs = torch.empty_like(gY)
         for k0, Yc, Uc in reversed(ctx.ckpt):
@@ -161,7 +169,7 @@ class _Unrolled(torch.autograd.Function):
                 c.elem(3, X=Q, gY=gY, gU=gU)
             del steps
         gS = irfft2(gSh, c.H, c.W)
-        gDfull = irfft2(gDh, c.H, c.W)
+        gDfull = irfft2(torch.sum(gDh, dim=0), c.H, c.W)
         gD = gDfull[:, :c.Kr, :c.Kc].permute(1, 2, 0).contiguous()
         return gD.reshape(ctx.dshape), gS, None, None
 

@@ -137,7 +137,7 @@ struct Plan {
   int col_g, col_G, col_ntiles, col_NT, Hs;
   size_t col_smem;
   int colg_g, colg_NT;
-  size_t colg_smem;
+  size_t colg_smem, colt_smem;
   int max_iter;
   size_t off_U, off_F, off_Dh, off_Sh, off_Ps, off_twW, off_twH, off_part, off_st, off_it,
       off_xi, off_ndone, total;
@@ -190,6 +190,7 @@ static int plan_geometry(int B, int M, int H, int W, Plan* pl) {
   pl->colg_g = group_size(H);
   pl->colg_NT = SC_COL_TILE * pl->colg_g;
   pl->colg_smem = col_smem_bytes(COL_FWD, H);
+  pl->colt_smem = col_smem_bytes(COL_FWD, scol ? ct_padded(H, col_radix(H)) : H);
   return SC_OK;
 }
 
@@ -232,10 +233,18 @@ extern "C" size_t sc_workspace_size(const sc_problem* p, const sc_options* o) {
 typedef void (*RowFn)(RowParams);
 typedef void (*ColFn)(ColParams);
 
+// Row modes with compile-time FFT plans: the iteration, the rho fix-up and
+// the 2-D FFT tools (used inside the adjoint); set-up modes use the runtime
+// plan.
+template <int MODE>
+constexpr bool row_specialised() {
+  return MODE == ROW_ITER || MODE == ROW_FIXUP || MODE == ROW_FWD_REAL || MODE == ROW_INV_REAL;
+}
+
 template <int MODE>
 static RowFn row_fn(int W) {
 #define SC_ROW_CASE(n) case n: return row_kernel<MODE, n>;
-  if constexpr (MODE == ROW_ITER || MODE == ROW_FIXUP) {
+  if constexpr (row_specialised<MODE>()) {
     switch (W) { SC_SPEC_ROW(SC_ROW_CASE) default: break; }
   }
 #undef SC_ROW_CASE
@@ -245,9 +254,7 @@ static RowFn row_fn(int W) {
 template <int MODE>
 static ColFn col_fn(int H) {
 #define SC_COL_CASE(n) case n: return col_kernel<MODE, n>;
-  if constexpr (MODE == COL_SOLVE || MODE == COL_SOLVE_W) {
-    switch (H) { SC_SPEC_COL(SC_COL_CASE) default: break; }
-  }
+  switch (H) { SC_SPEC_COL(SC_COL_CASE) default: break; }
 #undef SC_COL_CASE
   return col_kernel<MODE, 0>;
 }
@@ -273,15 +280,14 @@ static int prepare_fn(const void* fn, bool cluster) {
 // length has one; the setup modes always use the runtime plan.
 template <int MODE>
 static int launch_row(const Plan& pl, RowParams rp, int B, cudaStream_t s, int nblk = 0) {
-  const bool hot = MODE == ROW_ITER || MODE == ROW_FIXUP;
+  const bool hot = row_specialised<MODE>() && spec_row(rp.g.W);
   RowFn fn = row_fn<MODE>(rp.g.W);
   int st = prepare_fn((const void*)fn, false);
   if (st) return st;
   rp.gsz = hot ? pl.row_g : pl.rowg_g;
   rp.nblk = nblk > 0 ? nblk : pl.row_nblk;
   dim3 grid(rp.nblk, B);
-  const size_t smem = MODE == ROW_ITER ? pl.row_smem
-                     : MODE == ROW_FIXUP ? pl.row_smem_fix : pl.rowg_smem;
+  const size_t smem = MODE == ROW_ITER ? pl.row_smem : hot ? pl.row_smem_fix : pl.rowg_smem;
   // one slot (row pair in flight) per rp.gsz threads
   const int threads = (SC_ROW_THREADS / rp.gsz) * rp.gsz;
   fn<<<grid, threads, smem, s>>>(rp);
@@ -318,10 +324,11 @@ static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s) {
     ColFn fn = col_fn<MODE>(cp.g.H);
     int st = prepare_fn((const void*)fn, false);
     if (st) return st;
-    cp.gsz = pl.colg_g;
+    const bool hot = spec_col(cp.g.H);
+    cp.gsz = hot ? pl.col_g : pl.colg_g;
     cp.G = std::min(8, cp.g.M);
     dim3 grid(cp.G, pl.col_ntiles, B);
-    fn<<<grid, pl.colg_NT, pl.colg_smem, s>>>(cp);
+    fn<<<grid, hot ? pl.col_NT : pl.colg_NT, hot ? pl.colt_smem : pl.colg_smem, s>>>(cp);
     CU_TRY(cudaGetLastError());
     ++g_launches;
   }

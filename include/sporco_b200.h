@@ -209,22 +209,26 @@ int sc_last_profile(sc_profile *out);
 /* Number of kernels this library has launched since it was loaded. */
 unsigned long long sc_launch_count(void);
 
-/* Building blocks of the adjoint of the unrolled cbpdn iteration (no
- * counterpart in the reference; plain cbpdn, fixed rho).  Spectra are dense
- * (count, H, W/2+1) complex64, maps (B, M, H, W) float32, device pointers.
- * sc_adj_freq mode 0: io = Z^ -> X^ = A^{-1}(conj(Df) S^ + rho Z^);
- *             mode 1: io = gX^ -> Q^ = A^{-1} gX^, accumulating gD^ per image
- *             (B, M, H, W/2+1; sum over the images for the dictionary gradient)
- *             and gS^ (B, H, W/2+1) from X^ (the step's forward solution).
- * sc_adj_elem mode 0: out = Y - U; 1: (Y, U) <- y/u step from X;
- *             2: from gY', gU' and the step's X, Y, U: out = gX, gY <- (1-a) gV,
- *                gU <- gV;  3: gY += rho Q, gU -= rho Q with Q in X. */
-int sc_adj_freq(int mode, int B, int M, int H, int W, float rho, const void *Dh,
-                const void *Sh, void *io, const void *Xh, void *gDh, void *gSh, void *stream);
-int sc_adj_elem(int mode, int B, int M, int H, int W, float rho, float alpha,
-                const float *lam, int l1_kind, float l1_scalar, const float *l1w,
-                const float *X, float *Y, float *U, float *gY, float *gU, float *out,
-                void *stream);
+/* Differentiable unrolled cbpdn (no counterpart in the reference): exactly
+ * o->max_iter = K plain-cbpdn ADMM iterations at the fixed rho p->rho0 (no
+ * stopping test, no adaptive rho; p->grd = 0, p->mask = NULL, p->U0 = p->U_out
+ * = NULL), and the reverse pass of those iterations.
+ *   sc_unrolled_forward writes Y_K to p->Y and keeps (Y, U) every seg
+ *     iterations in the workspace (seg: 1..K; ceil(sqrt(K)) balances memory
+ *     against the one recomputation of each segment in the backward pass).
+ *   sc_unrolled_backward, after a forward call with the same problem,
+ *     options, seg and workspace, takes gY = dLoss/dY_K (B, M, H, W) and
+ *     writes dLoss/dD to gD (M, Kr, Kc) and dLoss/dS to gS (B, H, W).
+ * The workspace (sc_unrolled_workspace_size bytes, 256-byte aligned) holds
+ * the solver's own workspace, the checkpoints, one segment's Y and x^ of
+ * every step, and the gradient spectra.  Returns 0 when the problem is not
+ * a plain fixed-rho cbpdn problem or seg is out of range. */
+size_t sc_unrolled_workspace_size(const sc_problem *p, const sc_options *o, int seg);
+int sc_unrolled_forward(const sc_problem *p, const sc_options *o, int seg, void *workspace,
+                        size_t workspace_bytes, void *stream);
+int sc_unrolled_backward(const sc_problem *p, const sc_options *o, int seg, void *workspace,
+                         size_t workspace_bytes, const float *gY, float *gD, float *gS,
+                         void *stream);
 
 /* Last status / message recorded on the calling thread. */
 int sc_last_status(void);

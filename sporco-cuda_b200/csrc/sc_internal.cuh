@@ -65,6 +65,7 @@ struct RowParams {
   float2* F;               // (B, M, H, Wp) spectra
   float* Y;                // (B, M, H, W)
   float* U;                // (B, M, H, W)
+  float* Yo;               // ROW_ITER writes Y here (== Y unless a trace is kept)
   // epilogue
   const float* lam;        // (B,)
   int l1_kind;
@@ -80,6 +81,10 @@ struct RowParams {
   const float* D;          // (M, Kr, Kc) for ROW_FWD_DICT
   int Kr, Kc;
   float* dst;              // real rows out for ROW_INV_REAL
+  // adjoint (ROW_ADJ)
+  float* gV;               // (B, M, H, W) gradient w.r.t. V of the step, in place
+  const float* Ymask;      // (B, M, H, W) Y the step produced (nonzero: shrinkage active)
+  int first;               // 1: gV holds dLoss/dY of the last iterate, no Q yet
 };
 
 struct ColParams {
@@ -98,26 +103,43 @@ struct ColParams {
   const float* wgrd;       // (M,)
   const float* Psum;       // (H, Wp) sum_m |Df_m|^2 (solve with one d for all maps)
   ImgState* st;
+  float2* Xtr;             // COL_SOLVE_X: x^ also written here (B, M, H, Wp)
+  // adjoint (COL_ADJ)
+  const float2* Xh;        // (B, M, H, Wp) x^ of the step
+  float2* gDh;             // (B, M, H, Wp) dictionary-gradient spectra, accumulated
+  float2* gSh;             // (B, H, Wp) signal-gradient spectra, accumulated
 };
 
 enum RowMode {
   ROW_ITER = 0, ROW_FWD_REAL = 1, ROW_FWD_DICT = 2, ROW_INV_REAL = 3, ROW_FIXUP = 4,
-  ROW_FWD_YU = 5  // row spectra of Y - U (start from given iterates)
+  ROW_FWD_YU = 5, // row spectra of Y - U (start from given iterates)
+  ROW_ADJ = 6     // adjoint step: Q = row IFFT, gV update, row FFT of relax * gV
 };
 // COL_SOLVE: all maps share d (cbpdn, or cbpdngrd with one GradWeight), so
 // sum_m |Df_m|^2 / d comes from the precomputed Psum; COL_SOLVE_W: per-map
 // d_m = mu w_m |G|^2 + rho, the sum is accumulated over the maps.
-enum ColMode { COL_SOLVE = 0, COL_FWD = 1, COL_INV = 2, COL_SOLVE_W = 3 };
+// COL_SOLVE_X: COL_SOLVE that also writes x^ to ColParams::Xtr (the
+// recomputation inside the adjoint).  COL_ADJ: adjoint of the plain cbpdn
+// solve (one d = rho): column FFT, Q^ = A^{-1} G^, gradient accumulation,
+// inverse column FFT.
+enum ColMode {
+  COL_SOLVE = 0, COL_FWD = 1, COL_INV = 2, COL_SOLVE_W = 3, COL_ADJ = 4, COL_SOLVE_X = 5
+};
+// Modes that launch as a cluster over the maps of one column tile.
+__host__ __device__ constexpr bool col_clustered(int mode) {
+  return mode == COL_SOLVE || mode == COL_SOLVE_W || mode == COL_SOLVE_X || mode == COL_ADJ;
+}
 
 __host__ __device__ inline size_t sc_align16(size_t x) { return (x + 15) & ~(size_t)15; }
 
 // Shared memory of one row-pass slot (one row pair in flight); zlen is the
 // (padded) number of shared-memory slots of one row transform.  The
 // iteration mode stages the next pair's two spectrum rows and the pair's Y
-// and U rows: [z: zlen complex][F: 2Wp complex][Y: 2W][U: 2W].
+// and U rows: [z: zlen complex][F: 2Wp complex][Y: 2W][U: 2W]; the adjoint
+// step stages gV and the shrinkage mask source in the Y and U places.
 __host__ __device__ inline size_t row_slot_bytes(int mode, int zlen, int W, int Wp) {
   size_t z = sc_align16((size_t)zlen * 8);
-  if (mode != ROW_ITER) return z;
+  if (mode != ROW_ITER && mode != ROW_ADJ) return z;
   return z + (size_t)(2 * Wp) * 8 + 2 * sc_align16((size_t)(2 * W) * 4);
 }
 
@@ -127,5 +149,5 @@ __host__ __device__ inline size_t row_slot_bytes(int mode, int zlen, int W, int 
 // the dictionary tile: [F0][F1][D]; the cluster reduction reuses [F1][D].
 __host__ __device__ inline size_t col_smem_bytes(int mode, int hlen) {
   const size_t tile = (size_t)SC_COL_TILE * hlen * 8;
-  return (mode == COL_SOLVE || mode == COL_SOLVE_W) ? 3 * tile : tile;
+  return col_clustered(mode) ? 3 * tile : tile;
 }

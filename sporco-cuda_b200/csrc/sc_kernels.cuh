@@ -135,13 +135,15 @@ row_kernel(RowParams P) {
   float2* z = reinterpret_cast<float2*>(slot);
   auto zs = [](int k) { return fft_slot<NW, RM>(k); };
 
-  float thr = 0.f, rsf_c = 0.f, uscale = 1.f;
-  if constexpr (MODE == ROW_ITER || MODE == ROW_FIXUP) {
+  float thr = 0.f, rsf_c = 0.f, uscale = 1.f, rho = 0.f;
+  if constexpr (MODE == ROW_ITER || MODE == ROW_FIXUP || MODE == ROW_ADJ) {
     const ImgState& st = P.st[b];
     if (st.done) return;
     if constexpr (MODE == ROW_ITER) {
       thr = (float)((double)P.lam[b] / st.rho);
       uscale = (float)st.uscale;
+    } else if constexpr (MODE == ROW_ADJ) {
+      rho = (float)st.rho;
     } else {
       if (st.rsf == 1.0) return;
       rsf_c = (float)(1.0 - 1.0 / st.rsf);
@@ -155,13 +157,15 @@ row_kernel(RowParams P) {
   float2* Fi = P.F + (size_t)b * img_spec;
   const long pstride = (long)gridDim.x * S;
 
-  if constexpr (MODE == ROW_ITER) {
-    // --------------------------------------------------------- iteration
+  if constexpr (MODE == ROW_ITER || MODE == ROW_ADJ) {
+    // ------------------------------------------ iteration / adjoint step
+    constexpr bool ADJ = MODE == ROW_ADJ;
     float2* fst = reinterpret_cast<float2*>(slot + sc_align16((size_t)zlen * 8));
     float* ysm = reinterpret_cast<float*>(fst + 2 * (size_t)Wp);
     float* usm = ysm + sc_align16((size_t)(2 * W) * 4) / 4;
-    const float* Yi = P.Y + (size_t)b * img_real;
-    const float* Ui = P.U + (size_t)b * img_real;
+    // staged per row pair: Y and U (iteration), gV and the mask source (adjoint)
+    const float* Yi = (ADJ ? P.gV : P.Y) + (size_t)b * img_real;
+    const float* Ui = (ADJ ? P.Ymask : P.U) + (size_t)b * img_real;
     const bool vec = (W & 3) == 0;
 
     auto issue_F = [&](long p) {
@@ -235,10 +239,35 @@ row_kernel(RowParams P) {
       fft_any<NW, 1, RM>(z, P.pw, P.twW, t, g);
       cp_async_wait<1>();  // Y(p), U(p)
       __syncthreads();
-      if (valid) {
+      if (ADJ && valid) {
+        // Q = IFFT(Q^) (zero before the first step); gradients w.r.t. Y and U
+        // of this step, gY = (1 - a) gV + rho Q, gU = gV - rho Q; gV of the
+        // step before: gY where its shrinkage was active (Y != 0), else gU.
+        float* gv = P.gV + (size_t)b * img_real + (size_t)r0 * W;
+        const bool first = P.first != 0;
+        for (int k = t; k < W; k += g) {
+          const float2 zz = z[zs(k)];
+          const float q0 = first ? 0.f : zz.x * P.invN;
+          const float q1 = first ? 0.f : -zz.y * P.invN;
+          const float v0 = ysm[k];
+          const float gy0 = first ? v0 : a1 * v0 + rho * q0;
+          const float gu0 = first ? 0.f : v0 - rho * q0;
+          const float n0 = usm[k] != 0.f ? gy0 : gu0;
+          gv[k] = n0;
+          float n1 = 0.f;
+          if (has1) {
+            const float v1 = ysm[W + k];
+            const float gy1 = first ? v1 : a1 * v1 + rho * q1;
+            const float gu1 = first ? 0.f : v1 - rho * q1;
+            n1 = usm[W + k] != 0.f ? gy1 : gu1;
+            gv[W + k] = n1;
+          }
+          z[zs(k)] = make_float2(a * n0, a * n1);
+        }
+      } else if (valid) {
         const int m0 = (int)(r0 / H), h0 = (int)(r0 - (long)m0 * H);
         const int m1 = (int)(r1 / H), h1 = (int)(r1 - (long)m1 * H);
-        float* Y0 = P.Y + (size_t)b * img_real + (size_t)r0 * W;
+        float* Y0 = P.Yo + (size_t)b * img_real + (size_t)r0 * W;
         float* U0 = P.U + (size_t)b * img_real + (size_t)r0 * W;
         float w0 = P.l1_scalar, w1 = P.l1_scalar;
         if (P.l1_kind == 1) { w0 = P.l1w[m0]; w1 = has1 ? P.l1w[m1] : 0.f; }
@@ -298,6 +327,7 @@ row_kernel(RowParams P) {
       __syncthreads();
     }
     cp_async_wait<0>();
+    if constexpr (ADJ) return;
     block_sum<5>(acc, red_scratch);
     if (threadIdx.x == 0) {
       double* out = P.partials + ((size_t)b * P.nblk + blockIdx.x) * 5;
@@ -413,7 +443,7 @@ col_kernel(ColParams P) {
   auto slot = [](int kr) { return fft_slot<NH, RM>(kr); };
 
   float rho = 0.f;
-  if constexpr (MODE == COL_SOLVE || MODE == COL_SOLVE_W) {
+  if constexpr (col_clustered(MODE)) {
     const ImgState& st = P.st[b];
     if (st.done) return;  // uniform over the cluster (same image)
     rho = (float)st.rho;
@@ -449,6 +479,195 @@ col_kernel(ColParams P) {
       __syncthreads();
     }
     return;
+  } else if constexpr (MODE == COL_ADJ) {
+    // Adjoint of the plain cbpdn solve, A = rho I + conj(Df) Df^T per
+    // frequency (one d = rho for every map).  F holds the row spectra of
+    // a gV; G^ is their column FFT and
+    //   cb = sum_m Df_m G^_m / (rho + Psum),   Q^_m = (G^_m - conj(Df_m) cb) / rho,
+    //   sum_m Df_m Q^_m = cb,                  gS^ += cb,
+    //   gD^_m += (S^ - sum_j Df_j X^_j) conj(Q^_m) - cb conj(X^_m);
+    // F receives the inverse column FFT of Q^.
+    float2* fbuf[2] = {stg, stg + TL};
+    float2* dbuf = stg + 2 * TL;
+    auto issue_tile = [&](const float2* base, float2* dst) {
+      for (int q = tid; q < 2 * H; q += NT) {
+        const int kr = q >> 1, h = q & 1;
+        cp_async16(dst + slot(kr) * T + 2 * h, base + (size_t)kr * Wp + c0 + 2 * h);
+      }
+    };
+    const size_t plane = (size_t)H * Wp;
+    const float2* Xb = P.Xh + (size_t)b * M * plane + c0;
+    float2* gDb = P.gDh + (size_t)b * M * plane + c0;
+    const float2* Sh = P.Sh + (size_t)b * plane + c0;
+    float2* gSb = P.gSh + (size_t)b * plane + c0;
+    const bool colok = c0 + cc < Wf;
+    const float irho = 1.f / rho;
+
+    // pass 1: G^, sum_m Df_m G^_m and sum_m Df_m X^_m; G^ written back in place
+    float2 dg[EPT], dx[EPT];
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) dg[i] = dx[i] = make_float2(0.f, 0.f);
+    if (m0 < m1) {
+      issue_tile(Fi + (size_t)m0 * plane, fbuf[0]);
+      issue_tile(P.Dh + (size_t)m0 * plane, dbuf);
+    }
+    cp_async_commit();
+    int it = 0;
+    for (int m = m0; m < m1; ++m, ++it) {
+      float2* cur = fbuf[it & 1];
+      if (m + 1 < m1) issue_tile(Fi + (size_t)(m + 1) * plane, fbuf[(it + 1) & 1]);
+      cp_async_commit();
+      cp_async_wait<1>();  // F(m) and D(m)
+      __syncthreads();
+      fft_any<NH, T, RM>(cur + cc, P.ph, P.twH, t, g);
+      float2* fout = Fi + (size_t)m * plane + c0;
+      const float2* xin = Xb + (size_t)m * plane;
+      if (colok) {
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+          const int kr = t + i * g;
+          if (kr < H) {
+            const int sl = slot(kr) * T + cc;
+            const float2 Dv = dbuf[sl];
+            const float2 gv = cur[sl];
+            const float2 xv = __ldg(&xin[(size_t)kr * Wp + cc]);
+            fout[(size_t)kr * Wp + cc] = gv;
+            dg[i].x += Dv.x * gv.x - Dv.y * gv.y;
+            dg[i].y += Dv.x * gv.y + Dv.y * gv.x;
+            dx[i].x += Dv.x * xv.x - Dv.y * xv.y;
+            dx[i].y += Dv.x * xv.y + Dv.y * xv.x;
+          }
+        }
+      }
+      __syncthreads();
+      if (m + 1 < m1) issue_tile(P.Dh + (size_t)(m + 1) * plane, dbuf);
+      cp_async_commit();
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    if (m0 < m1) issue_tile(Fi + (size_t)m0 * plane, fbuf[0]);
+    cp_async_commit();
+    // reduce over the maps: dg -> cb, dx -> S^ - sum Df X^; the owner of an
+    // element also accumulates gS^ there
+    const int E = T * H;
+    float2* xn = fbuf[1];  // [E] complex
+    float2* xx = xn + E;   // [E] complex
+    auto finish = [&](int e, float2 sdg, float2 sdx, float2* cb_out, float2* a_out) {
+      const int kr = e / T, c = e - (e / T) * T;
+      float2 cbv = make_float2(0.f, 0.f), av = make_float2(0.f, 0.f);
+      if (c0 + c < Wf) {
+        const float q = 1.f / (rho + __ldg(&P.Psum[(size_t)kr * Wp + c0 + c]));
+        cbv = make_float2(sdg.x * q, sdg.y * q);
+        const float2 Sv = __ldg(&Sh[(size_t)kr * Wp + c]);
+        av = make_float2(Sv.x - sdx.x, Sv.y - sdx.y);
+        float2* gs = gSb + (size_t)kr * Wp + c;
+        const float2 o = *gs;
+        *gs = make_float2(o.x + cbv.x, o.y + cbv.y);
+      }
+      *cb_out = cbv;
+      *a_out = av;
+    };
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) {
+      const int kr = t + i * g;
+      if (kr < H) {
+        xn[kr * T + cc] = dg[i];
+        xx[kr * T + cc] = dx[i];
+      }
+    }
+    if (P.G > 1) {
+      cg::cluster_group cluster = cg::this_cluster();
+      cluster.sync();
+      const int sl = (E + P.G - 1) / P.G;
+      const int e0 = rank * sl, e1 = min(E, e0 + sl);
+      for (int e = e0 + tid; e < e1; e += NT) {
+        float2 s1 = make_float2(0.f, 0.f), s2 = make_float2(0.f, 0.f);
+        for (int r = 0; r < P.G; ++r) {
+          const float2 v = cluster.map_shared_rank(xn, r)[e];
+          const float2 w = cluster.map_shared_rank(xx, r)[e];
+          s1.x += v.x;
+          s1.y += v.y;
+          s2.x += w.x;
+          s2.y += w.y;
+        }
+        finish(e, s1, s2, &s1, &s2);
+        xn[e] = s1;
+        xx[e] = s2;
+      }
+      cluster.sync();
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        const int kr = t + i * g;
+        if (kr < H) {
+          const int e = kr * T + cc;
+          const int owner = e / sl;
+          dg[i] = owner == rank ? xn[e] : cluster.map_shared_rank(xn, owner)[e];
+          dx[i] = owner == rank ? xx[e] : cluster.map_shared_rank(xx, owner)[e];
+        }
+      }
+      cluster.sync();
+    } else {
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        const int kr = t + i * g;
+        if (kr < H) finish(kr * T + cc, dg[i], dx[i], &dg[i], &dx[i]);
+      }
+      __syncthreads();
+    }
+    // dg[i] = cb, dx[i] = S^ - sum_j Df_j X^_j for this thread's elements
+    if (m0 < m1) issue_tile(P.Dh + (size_t)m0 * plane, dbuf);
+    cp_async_commit();
+    // pass 2: Q^, the dictionary gradient, inverse column FFT of Q^
+    it = 0;
+    for (int m = m0; m < m1; ++m, ++it) {
+      float2* cur = fbuf[it & 1];
+      if (m + 1 < m1) issue_tile(Fi + (size_t)(m + 1) * plane, fbuf[(it + 1) & 1]);
+      cp_async_commit();
+      cp_async_wait<1>();  // F(m) and D(m)
+      __syncthreads();
+      const float2* xin = Xb + (size_t)m * plane;
+      float2* gd = gDb + (size_t)m * plane;
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        const int kr = t + i * g;
+        if (kr < H) {
+          const int sl = slot(kr) * T + cc;
+          float2 qv = make_float2(0.f, 0.f);
+          if (colok) {
+            const float2 Dv = dbuf[sl];
+            const float2 gv = cur[sl];
+            const float2 cb = dg[i], av = dx[i];
+            qv.x = (gv.x - (Dv.x * cb.x + Dv.y * cb.y)) * irho;
+            qv.y = (gv.y - (Dv.x * cb.y - Dv.y * cb.x)) * irho;
+            const float2 xv = __ldg(&xin[(size_t)kr * Wp + cc]);
+            float2* gp = gd + (size_t)kr * Wp + cc;
+            const float2 o = *gp;
+            *gp = make_float2(o.x + av.x * qv.x + av.y * qv.y - (cb.x * xv.x + cb.y * xv.y),
+                              o.y + av.y * qv.x - av.x * qv.y - (cb.y * xv.x - cb.x * xv.y));
+          }
+          cur[sl] = make_float2(qv.x, -qv.y);  // conj: inverse via forward FFT
+        }
+      }
+      __syncthreads();
+      if (m + 1 < m1) issue_tile(P.Dh + (size_t)(m + 1) * plane, dbuf);
+      cp_async_commit();
+      fft_any<NH, T, RM>(cur + cc, P.ph, P.twH, t, g);
+      float2* dst = Fi + (size_t)m * plane + c0;
+      if (colok) {
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+          const int kr = t + i * g;
+          if (kr < H) {
+            const float2 v = cur[slot(kr) * T + cc];
+            dst[(size_t)kr * Wp + cc] = make_float2(v.x, -v.y);
+          }
+        }
+      }
+      __syncthreads();
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
   } else {
     constexpr bool SDEN = MODE == COL_SOLVE_W;  // accumulate sum |Df|^2 / d_m
     float2* fbuf[2] = {stg, stg + TL};
@@ -604,7 +823,9 @@ col_kernel(ColParams P) {
     if (m0 < m1) issue_tile(P.Dh + (size_t)m0 * H * Wp, dbuf);
     cp_async_commit();
     // ---------------------------------------------------------------- pass 2
-    // x = (conj(Df) SC + rho (Y - U)^) / d, inverse column FFT
+    // x = (conj(Df) SC + rho (Y - U)^) / d (kept in P.Xtr by COL_SOLVE_X),
+    // inverse column FFT
+    float2* xtr = MODE == COL_SOLVE_X ? P.Xtr + (size_t)b * M * H * Wp + c0 : nullptr;
     it = 0;
     for (int m = m0; m < m1; ++m, ++it) {
       float2* cur = fbuf[it & 1];
@@ -626,6 +847,7 @@ col_kernel(ColParams P) {
             const float id = inv_d(wg, kr);
             xo.x = (Dv.x * sc.x + Dv.y * sc.y + rho * yu.x) * id;
             xo.y = (Dv.x * sc.y - Dv.y * sc.x + rho * yu.y) * id;
+            if constexpr (MODE == COL_SOLVE_X) xtr[(size_t)m * H * Wp + (size_t)kr * Wp + cc] = xo;
           }
           cur[sl] = make_float2(xo.x, -xo.y);  // conj: inverse via forward FFT
         }

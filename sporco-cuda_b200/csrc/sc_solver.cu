@@ -238,7 +238,8 @@ typedef void (*ColFn)(ColParams);
 // plan.
 template <int MODE>
 constexpr bool row_specialised() {
-  return MODE == ROW_ITER || MODE == ROW_FIXUP || MODE == ROW_FWD_REAL || MODE == ROW_INV_REAL;
+  return MODE == ROW_ITER || MODE == ROW_FIXUP || MODE == ROW_FWD_REAL || MODE == ROW_INV_REAL ||
+         MODE == ROW_ADJ;
 }
 
 template <int MODE>
@@ -287,7 +288,8 @@ static int launch_row(const Plan& pl, RowParams rp, int B, cudaStream_t s, int n
   rp.gsz = hot ? pl.row_g : pl.rowg_g;
   rp.nblk = nblk > 0 ? nblk : pl.row_nblk;
   dim3 grid(rp.nblk, B);
-  const size_t smem = MODE == ROW_ITER ? pl.row_smem : hot ? pl.row_smem_fix : pl.rowg_smem;
+  const size_t smem = (MODE == ROW_ITER || MODE == ROW_ADJ) ? pl.row_smem
+                      : hot ? pl.row_smem_fix : pl.rowg_smem;
   // one slot (row pair in flight) per rp.gsz threads
   const int threads = (SC_ROW_THREADS / rp.gsz) * rp.gsz;
   fn<<<grid, threads, smem, s>>>(rp);
@@ -299,7 +301,7 @@ static int launch_row(const Plan& pl, RowParams rp, int B, cudaStream_t s, int n
 template <int MODE>
 static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s) {
   cp.Hs = pl.Hs;
-  if (MODE == COL_SOLVE || MODE == COL_SOLVE_W) {
+  if (col_clustered(MODE)) {
     ColFn fn = col_fn<MODE>(cp.g.H);
     int st = prepare_fn((const void*)fn, true);
     if (st) return st;
@@ -480,7 +482,7 @@ struct Solve {
     CU_TRY(cudaGetLastError());
     g_launches += 2;
 
-    rp.g = g; rp.pw = pl.pw; rp.twW = twW; rp.F = F; rp.Y = p->Y; rp.U = U;
+    rp.g = g; rp.pw = pl.pw; rp.twW = twW; rp.F = F; rp.Y = p->Y; rp.Yo = p->Y; rp.U = U;
     rp.lam = p->lmbda; rp.l1_kind = p->l1_kind; rp.l1_scalar = p->l1_scalar; rp.l1w = p->l1w;
     rp.mask = p->mask; rp.relax = o->relax; rp.invN = (float)(1.0 / ((double)g.H * g.W));
     rp.partials = part; rp.st = sts;
@@ -661,6 +663,231 @@ extern "C" int sc_cbpdn_solve_batch(const sc_problem* probs, int nprob, const sc
   }
   for (int i = 0; i < nprob; ++i)
     if ((st = sv[i].result(res ? &res[i] : nullptr))) return st;
+  return SC_OK;
+}
+
+// ------------------------------------------------ unrolled solve + adjoint --
+// Workspace of the unrolled solve: the solver's own workspace first, then
+//   ckY, ckU (nseg, B, M, H, W)  Y and U at the start of every segment
+//   Ytr      (seg, B, M, H, W)   Y after each step of the segment being reversed
+//   Xtr      (seg, B, M, H, Wp)  x^ of each of those steps
+//   gV       (B, M, H, W)        gradient w.r.t. V of the step being reversed
+//   Fb       (B, M, H, Wp)       spectra of the reverse steps
+//   gDh      (B, M, H, Wp), gSh (B, H, Wp)  gradient spectra, per image
+//   gDr      (M, H, W)           dictionary gradient before the crop
+struct Unrolled {
+  sc_problem p;   // the caller's problem with the solver-owned fields cleared
+  sc_options o;   // fixed rho, no stopping test, no statistics
+  Plan pl;
+  int K = 0, seg = 0, nseg = 0;
+  size_t R = 0, C = 0;  // floats of a real array, complex entries of a spectrum array
+  size_t ckY = 0, ckU = 0, Ytr = 0, Xtr = 0, gV = 0, Fb = 0, gDh = 0, gSh = 0, gDr = 0;
+  size_t total = 0;
+};
+
+static int unrolled_plan(const sc_problem* p, const sc_options* o, int seg, Unrolled* u) {
+  if (!p || !o) return set_status(SC_ERR_INVALID, "null problem or options");
+  if (p->grd || p->mask || p->U0 || p->U_out)
+    return set_status(SC_ERR_UNSUPPORTED,
+                      "the unrolled solve is plain cbpdn (no gradient term, mask or warm start)");
+  if (o->max_iter < 1) return set_status(SC_ERR_INVALID, "max_iter must be >= 1");
+  if (seg < 1 || seg > o->max_iter)
+    return set_status(SC_ERR_INVALID, "segment length %d outside 1..%d", seg, o->max_iter);
+  u->p = *p;
+  u->o = *o;
+  u->o.rel_tol = 0.f;
+  u->o.abs_tol = 0.f;
+  u->o.auto_rho = 0;
+  u->o.record_itstat = 0;
+  u->o.check_every = 0;
+  u->o.profile = 0;
+  int st = plan_problem(&u->p, &u->o, &u->pl);
+  if (st) return st;
+  const Geom& g = u->pl.g;
+  u->K = o->max_iter;
+  u->seg = seg;
+  u->nseg = (u->K + seg - 1) / seg;
+  u->R = (size_t)g.B * g.M * g.H * g.W;
+  u->C = (size_t)g.B * g.M * g.H * g.Wp;
+  size_t off = u->pl.total;
+  auto take = [&](size_t bytes) { size_t r = off; off = align256(off + bytes); return r; };
+  u->ckY = take(sizeof(float) * u->R * u->nseg);
+  u->ckU = take(sizeof(float) * u->R * u->nseg);
+  u->Ytr = take(sizeof(float) * u->R * seg);
+  u->Xtr = take(sizeof(float2) * u->C * seg);
+  u->gV = take(sizeof(float) * u->R);
+  u->Fb = take(sizeof(float2) * u->C);
+  u->gDh = take(sizeof(float2) * u->C);
+  u->gSh = take(sizeof(float2) * (size_t)g.B * g.H * g.Wp);
+  u->gDr = take(sizeof(float) * (size_t)g.M * g.H * g.W);
+  u->total = off;
+  return SC_OK;
+}
+
+extern "C" size_t sc_unrolled_workspace_size(const sc_problem* p, const sc_options* o, int seg) {
+  Unrolled u;
+  if (unrolled_plan(p, o, seg, &u)) return 0;
+  return u.total;
+}
+
+static int unrolled_begin(const sc_problem* p, const sc_options* o, int seg, void* ws,
+                          size_t bytes, Unrolled* u) {
+  set_status(SC_OK, nullptr);
+  (void)cudaGetLastError();
+  int st = unrolled_plan(p, o, seg, u);
+  if (st) return st;
+  if (!ws || bytes < u->total)
+    return set_status(SC_ERR_WORKSPACE, "workspace of %zu bytes needed", u->total);
+  return SC_OK;
+}
+
+static auto untimed = [](int, auto&& launch) -> int { return launch(); };
+
+extern "C" int sc_unrolled_forward(const sc_problem* p, const sc_options* o, int seg, void* ws,
+                                   size_t bytes, void* stream) {
+  Unrolled u;
+  int st = unrolled_begin(p, o, seg, ws, bytes, &u);
+  if (st) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned char* w = (unsigned char*)ws;
+  Solve sv;
+  if ((st = sv.setup(&u.p, &u.o, ws, u.pl.total, s))) return st;
+  for (int j = 0; j < u.nseg; ++j) {
+    CU_TRY(cudaMemcpyAsync(w + u.ckY + sizeof(float) * u.R * j, u.p.Y, sizeof(float) * u.R,
+                           cudaMemcpyDeviceToDevice, s));
+    CU_TRY(cudaMemcpyAsync(w + u.ckU + sizeof(float) * u.R * j, sv.U, sizeof(float) * u.R,
+                           cudaMemcpyDeviceToDevice, s));
+    if ((st = sv.launch(std::min(u.seg, u.K - j * u.seg), untimed))) return st;
+  }
+  sc_result res;
+  return sv.result(&res);
+}
+
+// gDh[0] <- sum over the images of gDh[b] (per: complex entries of one image)
+__global__ void sum_images_kernel(float2* g, int B, size_t per) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < per;
+       i += (size_t)gridDim.x * blockDim.x) {
+    float2 a = g[i];
+    for (int b = 1; b < B; ++b) {
+      const float2 v = g[(size_t)b * per + i];
+      a.x += v.x;
+      a.y += v.y;
+    }
+    g[i] = a;
+  }
+}
+
+// gD (M, Kr, Kc) <- the filter support of src (M, H, W)
+__global__ void crop_kernel(const float* src, float* dst, int M, int H, int W, int Kr, int Kc) {
+  const int n = M * Kr * Kc;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int m = i / (Kr * Kc), r = (i / Kc) % Kr, c = i % Kc;
+    dst[i] = src[((size_t)m * H + r) * W + c];
+  }
+}
+
+// Reverse pass.  Step k of the forward pass maps (Y_k, U_k) to (Y_k+1, U_k+1)
+// through X_k = A^{-1}(D^T S + rho (Y_k - U_k)), V_k = a X_k + (1 - a) Y_k + U_k,
+// Y_k+1 = soft(V_k), U_k+1 = V_k - Y_k+1.  Its reverse: gV_k from the
+// gradients w.r.t. Y_k+1 and U_k+1 and the shrinkage mask (Y_k+1 != 0), then
+// (COL_ADJ) Q_k = A^{-1} a gV_k with the dictionary and signal gradients, then
+// (ROW_ADJ) the gradients w.r.t. Y_k and U_k, which give gV_k-1.  Segments are
+// reversed last to first, each after recomputing its forward steps from its
+// checkpoint with Y and x^ of every step kept.
+extern "C" int sc_unrolled_backward(const sc_problem* p, const sc_options* o, int seg, void* ws,
+                                    size_t bytes, const float* gY, float* gD, float* gS,
+                                    void* stream) {
+  Unrolled u;
+  int st = unrolled_begin(p, o, seg, ws, bytes, &u);
+  if (st) return st;
+  if (!gY || !gD || !gS) return set_status(SC_ERR_INVALID, "null gradient pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned char* w = (unsigned char*)ws;
+  float* ckY = (float*)(w + u.ckY);
+  float* ckU = (float*)(w + u.ckU);
+  float* Ytr = (float*)(w + u.Ytr);
+  float2* Xtr = (float2*)(w + u.Xtr);
+  float* gV = (float*)(w + u.gV);
+  float2* Fb = (float2*)(w + u.Fb);
+  float2* gDh = (float2*)(w + u.gDh);
+  float2* gSh = (float2*)(w + u.gSh);
+  float* gDr = (float*)(w + u.gDr);
+  const Geom& g = u.pl.g;
+  const Plan& pl = u.pl;
+  const int B = g.B;
+  // set-up writes zeros to the problem's Y: give it a trace slot instead of
+  // the caller's result
+  u.p.Y = Ytr;
+  Solve sv;
+  if ((st = sv.setup(&u.p, &u.o, ws, pl.total, s))) return st;
+  CU_TRY(cudaMemsetAsync(gDh, 0, sizeof(float2) * u.C, s));
+  CU_TRY(cudaMemsetAsync(gSh, 0, sizeof(float2) * (size_t)B * g.H * g.Wp, s));
+  CU_TRY(cudaMemcpyAsync(gV, gY, sizeof(float) * u.R, cudaMemcpyDeviceToDevice, s));
+
+  RowParams ra = sv.rp;
+  ra.F = Fb; ra.gV = gV; ra.first = 1;
+  ColParams ca = sv.cp;
+  ca.F = Fb; ca.gDh = gDh; ca.gSh = gSh; ca.Xtr = nullptr;
+  for (int j = u.nseg - 1; j >= 0; --j) {
+    const int n = std::min(u.seg, u.K - j * u.seg);
+    // Y of step i of this segment: i = 0 is the checkpoint
+    auto Yat = [&](int i) { return i == 0 ? ckY + u.R * j : Ytr + u.R * (i - 1); };
+    // recompute the segment
+    CU_TRY(cudaMemcpyAsync(sv.U, ckU + u.R * j, sizeof(float) * u.R, cudaMemcpyDeviceToDevice, s));
+    {
+      RowParams rf = sv.rp;
+      rf.Y = Yat(0);
+      if ((st = launch_row<ROW_FWD_YU>(pl, rf, B, s))) return st;
+    }
+    for (int i = 0; i < n; ++i) {
+      ColParams cf = sv.cp;
+      cf.Xtr = Xtr + u.C * i;
+      if ((st = launch_col<COL_SOLVE_X>(pl, cf, B, s))) return st;
+      RowParams rr = sv.rp;
+      rr.Y = Yat(i);
+      rr.Yo = Yat(i + 1);
+      if ((st = launch_row<ROW_ITER>(pl, rr, B, s))) return st;
+    }
+    // reverse it
+    ra.Ymask = Yat(n);
+    if ((st = launch_row<ROW_ADJ>(pl, ra, B, s))) return st;
+    ra.first = 0;
+    for (int i = n - 1; i >= 0; --i) {
+      ca.Xh = Xtr + u.C * i;
+      if ((st = launch_col<COL_ADJ>(pl, ca, B, s))) return st;
+      if (i > 0) {
+        ra.Ymask = Yat(i);
+        if ((st = launch_row<ROW_ADJ>(pl, ra, B, s))) return st;
+      }
+    }
+  }
+  // dictionary gradient: sum over the images, inverse FFT, crop to the filters
+  const size_t per = (size_t)g.M * g.H * g.Wp;
+  sum_images_kernel<<<(unsigned)std::min<size_t>((per + 255) / 256, 4096), 256, 0, s>>>(gDh, B,
+                                                                                       per);
+  CU_TRY(cudaGetLastError());
+  ++g_launches;
+  {
+    ColParams ci = sv.cp;
+    ci.g.B = 1; ci.F = gDh;
+    if ((st = launch_col<COL_INV>(pl, ci, 1, s))) return st;
+    RowParams ri = sv.rp;
+    ri.g.B = 1; ri.F = gDh; ri.dst = gDr;
+    if ((st = launch_row<ROW_INV_REAL>(pl, ri, 1, s))) return st;
+    const int n = g.M * u.p.Kr * u.p.Kc;
+    crop_kernel<<<(n + 255) / 256, 256, 0, s>>>(gDr, gD, g.M, g.H, g.W, u.p.Kr, u.p.Kc);
+    CU_TRY(cudaGetLastError());
+    ++g_launches;
+  }
+  // signal gradient
+  {
+    ColParams ci = sv.cp;
+    ci.g.M = 1; ci.F = gSh;
+    if ((st = launch_col<COL_INV>(pl, ci, B, s))) return st;
+    RowParams ri = sv.rp;
+    ri.g.M = 1; ri.F = gSh; ri.dst = gS;
+    if ((st = launch_row<ROW_INV_REAL>(pl, ri, B, s))) return st;
+  }
   return SC_OK;
 }
 

@@ -149,12 +149,12 @@ sc_irfft2 = _proto("sc_irfft2", C.c_int,
 sc_rfft2_noalloc = _proto("sc_rfft2_noalloc", C.c_int,
                           [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p])
 VP = C.c_void_p
-sc_adj_freq = _proto("sc_adj_freq", C.c_int,
-                     [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, VP, VP, VP, VP,
-                      VP, VP, VP])
-sc_adj_elem = _proto("sc_adj_elem", C.c_int,
-                     [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, VP,
-                      C.c_int, C.c_float, VP, VP, VP, VP, VP, VP, VP, VP])
+PP, PO = C.POINTER(ScProblem), C.POINTER(ScOptions)
+sc_unrolled_workspace_size = _proto("sc_unrolled_workspace_size", C.c_size_t, [PP, PO, C.c_int])
+sc_unrolled_forward = _proto("sc_unrolled_forward", C.c_int,
+                             [PP, PO, C.c_int, VP, C.c_size_t, VP])
+sc_unrolled_backward = _proto("sc_unrolled_backward", C.c_int,
+                              [PP, PO, C.c_int, VP, C.c_size_t, VP, VP, VP, VP])
 sc_last_profile = _proto("sc_last_profile", C.c_int, [C.POINTER(ScProfile)])
 sc_launch_count = _proto("sc_launch_count", C.c_ulonglong, [])
 sc_last_status = _proto("sc_last_status", C.c_int, [])
@@ -167,7 +167,8 @@ EXPORTED = [
     "check_cuda_req", "get_device_count", "get_current_device", "set_current_device",
     "get_memory_info", "get_device_name", "sc_workspace_size", "sc_options_from_algopt",
     "sc_cbpdn_solve", "sc_cbpdn_solve_batch", "sc_read_state", "sc_rfft2", "sc_irfft2",
-    "sc_rfft2_noalloc", "sc_adj_freq", "sc_adj_elem", "sc_last_profile", "sc_launch_count",
+    "sc_rfft2_noalloc", "sc_unrolled_workspace_size", "sc_unrolled_forward",
+    "sc_unrolled_backward", "sc_last_profile", "sc_launch_count",
     "sc_last_status", "sc_last_error", "sc_version",
 ]
 

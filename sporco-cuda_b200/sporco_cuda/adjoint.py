@@ -4,13 +4,15 @@ No counterpart in the reference.  ``cbpdn_unrolled(D, S, lmbda, opt)`` runs a
 fixed number of plain-cbpdn ADMM iterations (``opt['MaxMainIter']``, fixed
 rho: adaptive rho and early stopping are not differentiated) and returns the
 coefficient maps; its backward pass returns dLoss/dD and dLoss/dS through all
-iterations.  The backward pass is hand-written (``csrc/sc_adjoint.cu``): the
-shrinkage subgradient mask, the transposed Sherman-Morrison solve (the
-system is Hermitian, so it is the forward solve again), the dictionary and
-signal gradients accumulated in the frequency domain, and FFTs by this
-package's own kernels.  Memory: (Y, U) checkpoints every ceil(sqrt(K))
-iterations; each segment is recomputed forward once during the backward pass
-and its steps kept while they are reversed.
+iterations.  Both passes are single calls into the native library
+(``sc_unrolled_forward`` / ``sc_unrolled_backward``): the forward pass is the
+solver's own fused iteration, keeping (Y, U) every ceil(sqrt(K)) iterations;
+the backward pass recomputes each segment once from its checkpoint (keeping
+Y and the coefficient spectra of every step) and reverses it with fused
+kernels of the same shape as the forward ones: the shrinkage subgradient
+mask, the transposed Sherman-Morrison solve (the system is Hermitian, so it
+is the forward solve again) and the dictionary and signal gradients
+accumulated in the frequency domain.
 
 Shapes: D (Kr, Kc, M), S (B, H, W) or (H, W) float32 CUDA tensors; the result
 is (B, H, W, M) (or (H, W, M)).
@@ -63,59 +65,16 @@ def _dict_spectrum(Dm, H, W):
     return rfft2(P)
 
 
-class _Ctx:
-    """Per-call constants of the unrolled solve."""
-
-    def __init__(self, Dm, S, lmbda, opt):
-        self.B, self.H, self.W = S.shape
-        self.M = Dm.shape[0]
-        self.Kr, self.Kc = Dm.shape[1:]
-        r = resolve_options(opt, float(np.asarray(lmbda).ravel()[0]))
-        self.K = int(r["MaxMainIter"])
-        self.alpha = float(r["RelaxParam"])
-        lam = np.broadcast_to(np.asarray(lmbda, dtype=F32), (self.B,))
-        self.lam = torch.as_tensor(lam.copy(), device=S.device)
-        rho = _opt_get(opt, "rho")
-        self.rho = float(F32(5e1 * float(lam[0]) + 1.0)) if rho is None else float(F32(rho))
-        w = _opt_get(opt, "L1Weight")
-        self.l1_kind, self.l1_scalar, self.l1w = _lib.SC_L1_SCALAR, float(F32(1.0)), None
-        if hasattr(w, "ndim") and np.asarray(w).size > 1:
-            w = np.asarray(w, dtype=F32)
-            if w.size == self.M:
-                self.l1_kind, self.l1w = _lib.SC_L1_PER_MAP, torch.as_tensor(
-                    w.ravel().copy(), device=S.device)
-            else:
-                self.l1_kind = _lib.SC_L1_FULL
-                self.l1w = torch.as_tensor(
-                    np.ascontiguousarray(np.broadcast_to(np.moveaxis(w, 2, 0),
-                                                         (self.M, self.H, self.W))),
-                    device=S.device)
-        else:
-            self.l1_scalar = float(F32(np.asarray(w).ravel()[0]))
-        self.Dh = _dict_spectrum(Dm, self.H, self.W)
-        self.Sh = rfft2(S)
-
-    def elem(self, mode, X=None, Y=None, U=None, gY=None, gU=None, out=None):
-        p = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None  # noqa: E731
-        _lib.check(_lib.sc_adj_elem(mode, self.B, self.M, self.H, self.W, self.rho, self.alpha,
-                                    p(self.lam), self.l1_kind, self.l1_scalar, p(self.l1w),
-                                    p(X), p(Y), p(U), p(gY), p(gU), p(out), _stream()))
-
-    def freq(self, mode, io, Xh=None, gDh=None, gSh=None):
-        p = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None  # noqa: E731
-        _lib.check(_lib.sc_adj_freq(mode, self.B, self.M, self.H, self.W, self.rho,
-                                    p(self.Dh), p(self.Sh), p(io), p(Xh), p(gDh), p(gSh),
-                                    _stream()))
-
-    def step(self, Y, U, keep=False):
-        """One ADMM iteration in place on (Y, U); with keep, return (X, X^)."""
-        Z = torch.empty_like(Y)
-        self.elem(0, Y=Y, U=U, out=Z)
-        Zh = rfft2(Z)
-        self.freq(0, Zh)                      # Zh <- X^
-        X = irfft2(Zh, self.H, self.W)
-        self.elem(1, X=X, Y=Y, U=U)
-        return (X, Zh) if keep else None
+def _l1_weight(opt, M, H, W, device):
+    """L1Weight of the option dict as the solver's l1 argument."""
+    w = _opt_get(opt, "L1Weight")
+    if hasattr(w, "ndim") and np.asarray(w).size > 1:
+        w = np.asarray(w, dtype=F32)
+        if w.size == M:
+            return torch.as_tensor(w.ravel().copy(), device=device)
+        return torch.as_tensor(np.ascontiguousarray(
+            np.broadcast_to(np.moveaxis(w, 2, 0), (M, H, W))), device=device)
+    return float(F32(np.asarray(w if w is not None else 1.0).ravel()[0]))
 
 
 class _Unrolled(torch.autograd.Function):
@@ -123,55 +82,42 @@ class _Unrolled(torch.autograd.Function):
     def forward(ctx, D, S, lmbda, opt):
         Dm = D.detach().permute(2, 0, 1).contiguous().float()
         Sb = S.detach().float().contiguous()
-        c = _Ctx(Dm, Sb, lmbda, opt)
-        Y = torch.zeros((c.B, c.M, c.H, c.W), device=S.device)
-        U = torch.zeros_like(Y)
-        seg = max(1, int(math.ceil(math.sqrt(c.K))))
-        ckpt = []
-        # the fused solver, run segment by segment from each checkpoint
+        B, H, W = Sb.shape
+        M = Dm.shape[0]
+        lam0 = float(np.asarray(lmbda, dtype=F32).ravel()[0])
+        r = resolve_options(opt, lam0)
+        K = int(r["MaxMainIter"])
+        rho = _opt_get(opt, "rho")
+        rho = float(F32(5e1 * lam0 + 1.0)) if rho is None else float(F32(rho))
         fopt = dict(opt)
-        fopt.update({"RelStopTol": 0.0, "AbsStopTol": 0.0, "rho": c.rho,
+        fopt.update({"RelStopTol": 0.0, "AbsStopTol": 0.0, "rho": rho,
                      "AutoRho": {"Enabled": False}})
-        l1 = c.l1w if c.l1w is not None else c.l1_scalar
-        ds = prepare_device(Dm, Sb, lmbda, fopt, l1=l1, Y=Y, check_every=0)
-        ds.prob.U_out = U.data_ptr()
-        for k0 in range(0, c.K, seg):
-            ckpt.append((k0, Y.clone(), U.clone()))
-            ds.opts.max_iter = min(seg, c.K - k0)
-            ds.prob.U0 = U.data_ptr() if k0 > 0 else None
-            ds.run()
-        ctx.c, ctx.seg, ctx.ckpt = c, seg, ckpt
+        Y = torch.empty((B, M, H, W), device=S.device)
+        ds = prepare_device(Dm, Sb, lmbda, fopt, l1=_l1_weight(opt, M, H, W, S.device), Y=Y,
+                            check_every=0, workspace=False)
+        seg = max(1, int(math.ceil(math.sqrt(K))))
+        nbytes = _lib.sc_unrolled_workspace_size(C.byref(ds.prob), C.byref(ds.opts), seg)
+        if nbytes == 0:
+            _lib.check_last()
+        ws = torch.empty(nbytes, dtype=torch.uint8, device=S.device)
+        _lib.check(_lib.sc_unrolled_forward(C.byref(ds.prob), C.byref(ds.opts), seg,
+                                            C.c_void_p(ws.data_ptr()), nbytes, _stream()))
+        ctx.ds, ctx.ws, ctx.seg = ds, ws, seg
         ctx.dshape = D.shape
         return Y.permute(0, 2, 3, 1).contiguous()
 
     @staticmethod
     def backward(ctx, gX):
-        c = ctx.c
+        ds = ctx.ds
+        B, M, H, W = ds.prob.B, ds.prob.M, ds.prob.H, ds.prob.W
         gY = gX.detach().permute(0, 3, 1, 2).contiguous().float()
-        gU = torch.zeros_like(gY)
-        Wf = c.W // 2 + 1
-        gDh = torch.zeros((c.B, c.M, c.H, Wf), dtype=torch.complex64, device=gY.device)
-        gSh = torch.zeros((c.B, c.H, Wf), dtype=torch.complex64, device=gY.device)
-        gXs = torch.empty_like(gY)
-        for k0, Yc, Uc in reversed(ctx.ckpt):
-            k1 = min(c.K, k0 + ctx.seg)
-            Y, U = Yc.clone(), Uc.clone()
-            steps = []
-            for _ in range(k0, k1):
-                Yk, Uk = Y.clone(), U.clone()
-                X, Xh = c.step(Y, U, keep=True)
-                steps.append((Yk, Uk, X, Xh))
-            for Yk, Uk, X, Xh in reversed(steps):
-                c.elem(2, X=X, Y=Yk, U=Uk, gY=gY, gU=gU, out=gXs)
-                Gh = rfft2(gXs)
-                c.freq(1, Gh, Xh=Xh, gDh=gDh, gSh=gSh)   # Gh <- Q^
-                Q = irfft2(Gh, c.H, c.W)
-                c.elem(3, X=Q, gY=gY, gU=gU)
-            del steps
-        gS = irfft2(gSh, c.H, c.W)
-        gDfull = irfft2(torch.sum(gDh, dim=0), c.H, c.W)
-        gD = gDfull[:, :c.Kr, :c.Kc].permute(1, 2, 0).contiguous()
-        return gD.reshape(ctx.dshape), gS, None, None
+        gD = torch.empty((M, ds.prob.Kr, ds.prob.Kc), device=gY.device)
+        gS = torch.empty((B, H, W), device=gY.device)
+        _lib.check(_lib.sc_unrolled_backward(
+            C.byref(ds.prob), C.byref(ds.opts), ctx.seg, C.c_void_p(ctx.ws.data_ptr()),
+            ctx.ws.numel(), C.c_void_p(gY.data_ptr()), C.c_void_p(gD.data_ptr()),
+            C.c_void_p(gS.data_ptr()), _stream()))
+        return gD.permute(1, 2, 0).contiguous().reshape(ctx.dshape), gS, None, None
 
 
 def cbpdn_unrolled(D, S, lmbda, opt):

@@ -278,14 +278,16 @@ class DeviceSolve:
 
 
 def prepare_device(Dm, S, lmbda, opt, mu=0.0, grd=False, l1=1.0, gw=1.0, mask=None,
-                   rho0=None, Y=None, record_itstat=False, check_every=32, profile=False):
+                   rho0=None, Y=None, record_itstat=False, check_every=32, profile=False,
+                   workspace=True):
     """Prepare a device solve for a batch of equal-sized images.
 
     Dm: (M, Kr, Kc) float32 CUDA tensor; S: (B, H, W) float32 CUDA tensor;
     lmbda: float or (B,) tensor/array; l1: scalar, (M,) or broadcastable to
     (M, H, W); gw: scalar or (M,); mask: (B, H, W) int32 tensor (map 0 is
     then the AMS impulse) or None.  Returns a DeviceSolve whose ``run``
-    writes Y (B, M, H, W)."""
+    writes Y (B, M, H, W); with workspace=False it has no workspace (for
+    callers that size their own, e.g. the unrolled solve)."""
     import torch
     dev = S.device
     B, H, W = S.shape
@@ -346,6 +348,8 @@ def prepare_device(Dm, S, lmbda, opt, mu=0.0, grd=False, l1=1.0, gw=1.0, mask=No
     keep["Y"] = Y
     prob.Y = Y.data_ptr()
     o = _sc_options(r, record_itstat=record_itstat, check_every=check_every, profile=profile)
+    if not workspace:
+        return DeviceSolve(prob, o, None, keep)
     nbytes = _lib.sc_workspace_size(C.byref(prob), C.byref(o))
     if nbytes == 0:
         _lib.check_last()

@@ -91,6 +91,30 @@ def test_workspace_size_and_invalid_sizes():
     assert _lib.sc_last_status() == 2
 
 
+def test_unrolled_workspace_size_and_rejections():
+    p = _lib.ScProblem()
+    p.B, p.H, p.W, p.M, p.Kr, p.Kc = 2, 64, 64, 8, 8, 8
+    o = _lib.ScOptions()
+    o.max_iter = 10
+    base = _lib.sc_workspace_size(C.byref(p), C.byref(o))
+    R, Cs = 2 * 8 * 64 * 64, 2 * 8 * 64 * 36
+    n4 = _lib.sc_unrolled_workspace_size(C.byref(p), C.byref(o), 4)
+    # checkpoints for 3 segments (Y and U), 4 Y traces, 4 x^ traces, gV, Fb, gD^
+    assert n4 >= base + 4 * R * (2 * 3 + 4 + 1) + 8 * Cs * (4 + 2)
+    n10 = _lib.sc_unrolled_workspace_size(C.byref(p), C.byref(o), 10)
+    assert n10 > n4
+    for seg in (0, 11):
+        assert _lib.sc_unrolled_workspace_size(C.byref(p), C.byref(o), seg) == 0
+        assert _lib.sc_last_status() == 1
+    p.grd = 1
+    assert _lib.sc_unrolled_workspace_size(C.byref(p), C.byref(o), 4) == 0
+    assert _lib.sc_last_status() == 2
+    p.grd = 0
+    o.max_iter = 0
+    assert _lib.sc_unrolled_workspace_size(C.byref(p), C.byref(o), 1) == 0
+    assert _lib.sc_last_status() == 1
+
+
 def test_no_device_paths_fail_cleanly():
     assert sporco_cuda.util.device_count() >= 0
     if sporco_cuda.util.device_count() == 0:

@@ -98,11 +98,17 @@ def opt_for(cfg, variant):
     return opt
 
 
-def algorithmic_bytes(H, W, M):
-    """Per-iteration HBM bytes of the byte model (two-pass 2-D FFT)."""
+def algorithmic_bytes(H, W, M, variant="cbpdn"):
+    """Per-iteration HBM bytes of the byte model (two-pass 2-D FFT): the row
+    pass reads and writes the spectra F (2C) and Y, U (4R); the column pass
+    reads F and the dictionary spectra D (C_D = C per image) twice and
+    writes F (C + 2 C_D + C); with the gradient term (d varies with the
+    frequency) it also writes and re-reads the column spectra between its
+    two passes (2C)."""
     R = 4.0 * M * H * W
     Cs = 8.0 * M * H * (W // 2 + 1)
-    return 4 * R + 6 * Cs + 2 * Cs
+    col = 2 * Cs + 2 * Cs + (2 * Cs if variant in ("cbpdngrd", "cbpdngrdmsk") else 0)
+    return 4 * R + 2 * Cs + col
 
 
 def synth(cfg, seed, device):
@@ -344,7 +350,7 @@ def run_ours(args, cfg, rank, world, local_rank):
     bytes_it = 0.0
     for v in cfg["variants"]:
         M = cfg["M"] + (1 if v == "cbpdnmsk" else 0)
-        bytes_it += algorithmic_bytes(cfg["H"], cfg["W"], M) * cfg["iters"] * args.steps
+        bytes_it += algorithmic_bytes(cfg["H"], cfg["W"], M, v) * cfg["iters"] * args.steps
     achieved = bytes_it / (it_ms / 1e3) / 1e9 if it_ms > 0 else None
     kern = {k: {"ms_per_launch": a[0] / max(1, a[1]), "launches": a[1],
                 "share": a[0] / it_ms if it_ms else None} for k, a in prof_tot.items()}
@@ -371,7 +377,7 @@ def run_ours(args, cfg, rank, world, local_rank):
                          "unit": "GB/s", "frac": achieved / peak if achieved else None,
                          "traffic": None,
                          "algorithmic_bytes_per_iteration":
-                             algorithmic_bytes(cfg["H"], cfg["W"], cfg["M"]),
+                             bytes_it / (cfg["iters"] * args.steps * len(cfg["variants"])),
                          "iteration_ms": it_ms / max(1, n_it), "kernels": kern},
             "cpu_baseline": cpu,
             "gpu_launches": launches,
@@ -490,7 +496,7 @@ def run_batched(args, cfg, rank, world, local_rank):
     bytes_total = 0.0
     it_per_img = step()  # iteration counts per image (same data, same counts)
     for S, k in zip(imgs, it_per_img):
-        bytes_total += algorithmic_bytes(S.shape[0], S.shape[1], cfg["M"] + 1) * k
+        bytes_total += algorithmic_bytes(S.shape[0], S.shape[1], cfg["M"] + 1, "cbpdnmsk") * k
     achieved = bytes_total * args.steps / (ms / 1e3) / 1e9
     if rank != 0:
         return None

@@ -118,16 +118,20 @@ enum RowMode {
 // COL_SOLVE: all maps share d (cbpdn, or cbpdngrd with one GradWeight), so
 // sum_m |Df_m|^2 / d comes from the precomputed Psum; COL_SOLVE_W: per-map
 // d_m = mu w_m |G|^2 + rho, the sum is accumulated over the maps.
-// COL_SOLVE_X: COL_SOLVE that also writes x^ to ColParams::Xtr (the
+// COL_SOLVE_P: the solve with d = rho for every map and frequency (cbpdn,
+// cbpdnmsk), without the write-back of the column spectra between its two
+// passes.  COL_SOLVE_X: COL_SOLVE that also writes x^ to ColParams::Xtr (the
 // recomputation inside the adjoint).  COL_ADJ: adjoint of the plain cbpdn
 // solve (one d = rho): column FFT, Q^ = A^{-1} G^, gradient accumulation,
 // inverse column FFT.
 enum ColMode {
-  COL_SOLVE = 0, COL_FWD = 1, COL_INV = 2, COL_SOLVE_W = 3, COL_ADJ = 4, COL_SOLVE_X = 5
+  COL_SOLVE = 0, COL_FWD = 1, COL_INV = 2, COL_SOLVE_W = 3, COL_ADJ = 4, COL_SOLVE_X = 5,
+  COL_SOLVE_P = 6
 };
 // Modes that launch as a cluster over the maps of one column tile.
 __host__ __device__ constexpr bool col_clustered(int mode) {
-  return mode == COL_SOLVE || mode == COL_SOLVE_W || mode == COL_SOLVE_X || mode == COL_ADJ;
+  return mode == COL_SOLVE || mode == COL_SOLVE_W || mode == COL_SOLVE_X || mode == COL_ADJ ||
+         mode == COL_SOLVE_P;
 }
 
 __host__ __device__ inline size_t sc_align16(size_t x) { return (x + 15) & ~(size_t)15; }

@@ -479,6 +479,162 @@ col_kernel(ColParams P) {
       __syncthreads();
     }
     return;
+  } else if constexpr (MODE == COL_SOLVE_P) {
+    // Plain solve, d = rho for every map and frequency (cbpdn, cbpdnmsk).
+    // With P_m the row spectra of (Y - U)_m held in F, Z^_m = FFTcol(P_m) and
+    // x^_m = Z^_m + conj(Df_m) SC / rho, so the inverse column transform is
+    //   IFFTcol(x^_m) = H P_m + IFFTcol(conj(Df_m) SC) / rho
+    // (unnormalised transforms): pass 1 transforms P_m only to accumulate
+    // sum_m Df_m Z^_m and writes nothing back; pass 2 transforms the
+    // correction and adds H P_m, re-read from F.
+    float2* fbuf[2] = {stg, stg + TL};
+    float2* dbuf = stg + 2 * TL;
+    auto issue_tile = [&](const float2* base, float2* dst) {
+      for (int q = tid; q < 2 * H; q += NT) {
+        const int kr = q >> 1, h = q & 1;
+        cp_async16(dst + slot(kr) * T + 2 * h, base + (size_t)kr * Wp + c0 + 2 * h);
+      }
+    };
+    const size_t plane = (size_t)H * Wp;
+    const float2* Sh = P.Sh + (size_t)b * plane + c0;
+    const bool colok = c0 + cc < Wf;
+    const float irho = 1.f / rho;
+    // pass 1: acc = sum_m Df_m Z^_m
+    float2 num[EPT];
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) num[i] = make_float2(0.f, 0.f);
+    if (m0 < m1) {
+      issue_tile(Fi + (size_t)m0 * plane, fbuf[0]);
+      issue_tile(P.Dh + (size_t)m0 * plane, dbuf);
+    }
+    cp_async_commit();
+    int it = 0;
+    for (int m = m0; m < m1; ++m, ++it) {
+      float2* cur = fbuf[it & 1];
+      if (m + 1 < m1) issue_tile(Fi + (size_t)(m + 1) * plane, fbuf[(it + 1) & 1]);
+      cp_async_commit();
+      cp_async_wait<1>();  // F(m) and D(m)
+      __syncthreads();
+      fft_any<NH, T, RM>(cur + cc, P.ph, P.twH, t, g);
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        const int kr = t + i * g;
+        if (kr < H) {
+          const int sl = slot(kr) * T + cc;
+          const float2 Dv = dbuf[sl];
+          const float2 z = cur[sl];
+          num[i].x += Dv.x * z.x - Dv.y * z.y;
+          num[i].y += Dv.x * z.y + Dv.y * z.x;
+        }
+      }
+      __syncthreads();
+      if (m + 1 < m1) issue_tile(P.Dh + (size_t)(m + 1) * plane, dbuf);
+      cp_async_commit();
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    // the dictionary tile of pass 2's first map lands during the reduction
+    // (which uses [F1] only)
+    const int E = T * H;
+    float2* xn = fbuf[1];  // [E] complex, reduction scratch
+    // SC = S^ - cb,  cb = sum_m Df_m b_m / (rho + Psum) = (S^ Psum / rho + acc) / (1 + Psum / rho)
+    auto s_minus_cb = [&](int kr, int c, float2 acc) -> float2 {
+      const int k = c0 + c;
+      if (k >= Wf) return make_float2(0.f, 0.f);
+      const float2 Sv = __ldg(&Sh[(size_t)kr * Wp + c]);
+      const float sd = __ldg(&P.Psum[(size_t)kr * Wp + k]) * irho;
+      const float q = 1.f / (1.f + sd);
+      const float2 cb = make_float2((Sv.x * sd + acc.x) * q, (Sv.y * sd + acc.y) * q);
+      return make_float2(Sv.x - cb.x, Sv.y - cb.y);
+    };
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) {
+      const int kr = t + i * g;
+      if (kr < H) xn[kr * T + cc] = num[i];
+    }
+    if (m0 < m1) issue_tile(P.Dh + (size_t)m0 * plane, dbuf);
+    cp_async_commit();
+    if (P.G > 1) {
+      cg::cluster_group cluster = cg::this_cluster();
+      cluster.sync();
+      const int sl = (E + P.G - 1) / P.G;
+      const int e0 = rank * sl, e1 = min(E, e0 + sl);
+      for (int e = e0 + tid; e < e1; e += NT) {
+        float2 ns = make_float2(0.f, 0.f);
+        for (int r = 0; r < P.G; ++r) {
+          const float2 v = cluster.map_shared_rank(xn, r)[e];
+          ns.x += v.x;
+          ns.y += v.y;
+        }
+        xn[e] = s_minus_cb(e / T, e % T, ns);
+      }
+      cluster.sync();
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        const int kr = t + i * g;
+        if (kr < H) {
+          const int e = kr * T + cc;
+          const int owner = e / sl;
+          num[i] = owner == rank ? xn[e] : cluster.map_shared_rank(xn, owner)[e];
+        }
+      }
+      cluster.sync();
+    } else {
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        const int kr = t + i * g;
+        if (kr < H) num[i] = s_minus_cb(kr, cc, num[i]);
+      }
+      __syncthreads();
+    }
+    // num[i] = SC / rho; pass 2
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) num[i] = make_float2(num[i].x * irho, num[i].y * irho);
+    const float hs = (float)H;
+    float2* work = fbuf[0];
+    float2* ptile = fbuf[1];
+    for (int m = m0; m < m1; ++m) {
+      cp_async_wait<0>();  // D(m)
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        const int kr = t + i * g;
+        if (kr < H) {
+          const int sl = slot(kr) * T + cc;
+          float2 v = make_float2(0.f, 0.f);
+          if (colok) {
+            const float2 Dv = dbuf[sl];
+            const float2 sc = num[i];
+            // conj(conj(Df) SC / rho): the inverse via the forward FFT
+            v = make_float2(Dv.x * sc.x + Dv.y * sc.y, -(Dv.x * sc.y - Dv.y * sc.x));
+          }
+          work[sl] = v;
+        }
+      }
+      __syncthreads();
+      // P(m) lands during the transform, D(m+1) after it
+      issue_tile(Fi + (size_t)m * plane, ptile);
+      cp_async_commit();
+      if (m + 1 < m1) issue_tile(P.Dh + (size_t)(m + 1) * plane, dbuf);
+      cp_async_commit();
+      fft_any<NH, T, RM>(work + cc, P.ph, P.twH, t, g);
+      cp_async_wait<1>();  // P(m)
+      __syncthreads();
+      float2* dst = Fi + (size_t)m * plane + c0;
+      if (colok) {
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+          const int kr = t + i * g;
+          if (kr < H) {
+            const int sl = slot(kr) * T + cc;
+            const float2 v = work[sl], pv = ptile[sl];
+            dst[(size_t)kr * Wp + cc] = make_float2(v.x + hs * pv.x, hs * pv.y - v.y);
+          }
+        }
+      }
+    }
+    cp_async_wait<0>();
   } else if constexpr (MODE == COL_ADJ) {
     // Adjoint of the plain cbpdn solve, A = rho I + conj(Df) Df^T per
     // frequency (one d = rho for every map).  F holds the row spectra of

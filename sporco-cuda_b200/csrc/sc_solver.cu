@@ -134,7 +134,7 @@ struct Plan {
   int rowg_g;
   size_t rowg_smem;
   // hot column kernel (solve) and setup column kernels
-  int col_g, col_G, col_ntiles, col_NT, Hs;
+  int col_g, col_ntiles, col_NT, Hs;
   size_t col_smem;
   int colg_g, colg_NT;
   size_t colg_smem, colt_smem;
@@ -185,7 +185,6 @@ static int plan_geometry(int B, int M, int H, int W, Plan* pl) {
   pl->col_ntiles = (g.Wf + SC_COL_TILE - 1) / SC_COL_TILE;
   pl->col_g = scol ? ct_threads(H, col_radix(H)) : group_size(H);
   pl->col_NT = SC_COL_TILE * pl->col_g;
-  pl->col_G = std::min(8, M);
   pl->col_smem = col_smem_bytes(COL_SOLVE, scol ? ct_padded(H, col_radix(H)) : H);
   pl->colg_g = group_size(H);
   pl->colg_NT = SC_COL_TILE * pl->colg_g;
@@ -298,6 +297,61 @@ static int launch_row(const Plan& pl, RowParams rp, int B, cudaStream_t s, int n
   return SC_OK;
 }
 
+// Clusters of G CTAs of fn (NT threads, smem bytes each) the device keeps
+// resident at once; cached per (device, function, G, smem).
+static int resident_clusters(const void* fn, int NT, size_t smem, int G, int* out) {
+  struct Entry { int dev; const void* fn; int G; size_t smem; int n; };
+  static std::vector<Entry> cache;
+  int dev = 0;
+  CU_TRY(cudaGetDevice(&dev));
+  for (const Entry& e : cache)
+    if (e.dev == dev && e.fn == fn && e.G == G && e.smem == smem) {
+      *out = e.n;
+      return SC_OK;
+    }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(G, 1, 1);
+  cfg.blockDim = dim3(NT);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = G;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  CU_TRY(cudaOccupancyMaxActiveClusters(&n, fn, &cfg));
+  cache.push_back({dev, fn, G, smem, n});
+  *out = n;
+  return SC_OK;
+}
+
+// CTAs per cluster of a clustered column launch over `units` column tiles
+// (tiles x images).  Candidates 8, 4, 2 (at most M); the estimated time is
+// (maps per CTA) x (rounds of resident clusters over the units), ties go to
+// the larger cluster.  A cluster of 8 CTAs that each fill an SM leaves the
+// SMs of a GPC beyond a multiple of 8 idle; smaller clusters pack the GPCs
+// more tightly at the price of more maps per CTA.
+static int cluster_size(const void* fn, int NT, size_t smem, int M, long units, int* G_out) {
+  int best = std::min(8, M);
+  long best_cost = -1;
+  for (int G = 8; G >= 2; G /= 2) {
+    if (G > M) continue;
+    int nc = 0;
+    int st = resident_clusters(fn, NT, smem, G, &nc);
+    if (st) return st;
+    if (nc < 1) continue;
+    const long cost = (long)((M + G - 1) / G) * ((units + nc - 1) / nc);
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
+      best = G;
+    }
+  }
+  *G_out = std::max(1, best);
+  return SC_OK;
+}
+
 template <int MODE>
 static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s) {
   cp.Hs = pl.Hs;
@@ -305,16 +359,20 @@ static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s) {
     ColFn fn = col_fn<MODE>(cp.g.H);
     int st = prepare_fn((const void*)fn, true);
     if (st) return st;
+    int G = 1;
+    if ((st = cluster_size((const void*)fn, pl.col_NT, pl.col_smem, cp.g.M,
+                           (long)pl.col_ntiles * B, &G)))
+      return st;
     cp.gsz = pl.col_g;
-    cp.G = pl.col_G;
+    cp.G = G;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(pl.col_G, pl.col_ntiles, B);
+    cfg.gridDim = dim3(G, pl.col_ntiles, B);
     cfg.blockDim = dim3(pl.col_NT);
     cfg.dynamicSmemBytes = pl.col_smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = pl.col_G;
+    attr[0].val.clusterDim.x = G;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
@@ -517,7 +575,8 @@ struct Solve {
     for (int i = 0; i < n; ++i) {
       if ((st = timed(0, [&] {
              return per_map_d ? launch_col<COL_SOLVE_W>(pl, cp, B, s)
-                              : launch_col<COL_SOLVE>(pl, cp, B, s);
+                    : p->grd  ? launch_col<COL_SOLVE>(pl, cp, B, s)
+                              : launch_col<COL_SOLVE_P>(pl, cp, B, s);
            })))
         return st;
       if ((st = timed(1, [&] { return launch_row<ROW_ITER>(pl, rp, B, s); }))) return st;

@@ -372,17 +372,34 @@ __host__ __device__ constexpr int ct_threads(int n, int RM) {
   return g < 8 ? 8 : g;
 }
 
-// Shared-memory slot of element i of a compile-time transform: one pad slot
-// after every ct_pad elements (the first radix), which spreads the strided
-// stores of the first pass over all banks.
+// Shared-memory slot of element i of a compile-time transform.
+//  * One transform per slot run (ST == 1, the row pass), N a multiple of 16:
+//    an XOR swizzle inside every aligned block of 16 elements, slot =
+//    i ^ g(i >> 4) with g(x) = (x & 7) | (x & 4) << 1.  A half-warp of 8-byte
+//    accesses is conflict-free when it touches 16 contiguous aligned
+//    elements (every load, the stores of the later passes), the stride-8
+//    elements 8j + q (stores of the first radix-8 pass) or two runs of 8
+//    elements 64 apart (stores of the second radix-8 pass).  No padding.
+//  * Interleaved transforms (ST > 1, the column pass, ST columns of 8 bytes
+//    per slot): one pad slot after every ct_pad elements (the first radix),
+//    which spreads the strided stores of the first pass over all banks.
 __host__ __device__ constexpr int ct_pad(int n, int RM) { return ct_plan(n, RM).r[0]; }
-template <int N, int RM>
+__host__ __device__ constexpr bool ct_swizzled(int n, int ST) { return ST == 1 && n % 16 == 0; }
+template <int N, int RM, int ST>
 __device__ __forceinline__ int ct_phys(int i) {
-  constexpr int P = ct_pad(N, RM);
-  return i + i / P;
+  if constexpr (ct_swizzled(N, ST)) {
+    const int x = i >> 4;
+    return i ^ ((x & 7) | ((x & 4) << 1));
+  } else {
+    constexpr int P = ct_pad(N, RM);
+    return i + i / P;
+  }
 }
-// Padded length (elements) of a compile-time transform.
+// Shared-memory slots (elements) of one compile-time transform.
 __host__ __device__ constexpr int ct_padded(int n, int RM) { return n + n / ct_pad(n, RM); }
+__host__ __device__ constexpr int ct_len(int n, int RM, int ST) {
+  return ct_swizzled(n, ST) ? n : ct_padded(n, RM);
+}
 
 template <int N, int RM, int R, int NS, int G, int ST>
 __device__ __forceinline__ void ct_pass(float2* data, const float2* __restrict__ tw, int t) {
@@ -395,7 +412,7 @@ __device__ __forceinline__ void ct_pass(float2* data, const float2* __restrict__
     const int j = t + i * G;
     if ((B % G) == 0 || j < B) {
 #pragma unroll
-      for (int q = 0; q < R; ++q) v[i][q] = data[ct_phys<N, RM>(j + q * B) * ST];
+      for (int q = 0; q < R; ++q) v[i][q] = data[ct_phys<N, RM, ST>(j + q * B) * ST];
       if constexpr (NS > 1) twiddle_r<R>(v[i], tw, (j % NS) * STEP);
       dft_r<R>(v[i]);
     }
@@ -408,7 +425,7 @@ __device__ __forceinline__ void ct_pass(float2* data, const float2* __restrict__
       const int k = j % NS;
       const int base = (j - k) * R + k;
 #pragma unroll
-      for (int q = 0; q < R; ++q) data[ct_phys<N, RM>(base + q * NS) * ST] = v[i][q];
+      for (int q = 0; q < R; ++q) data[ct_phys<N, RM, ST>(base + q * NS) * ST] = v[i][q];
     }
   }
   __syncthreads();
@@ -437,9 +454,10 @@ __device__ __forceinline__ void fft_any(float2* data, const FftPlan& P,
   }
 }
 
-// Element index -> shared-memory slot for either path.
-template <int N, int RM>
+// Element index -> shared-memory slot for either path (ST: transforms
+// interleaved per slot, as passed to fft_any).
+template <int N, int RM, int ST>
 __device__ __forceinline__ int fft_slot(int i) {
   if constexpr (N == 0) return i;
-  else return ct_phys<N, RM>(i);
+  else return ct_phys<N, RM, ST>(i);
 }

@@ -130,10 +130,10 @@ row_kernel(RowParams P) {
   const int S = blockDim.x / g;
   const int s = threadIdx.x / g;
   const int t = threadIdx.x - s * g;
-  const int zlen = NW > 0 ? ct_padded(NW, RM) : W;
+  const int zlen = NW > 0 ? ct_len(NW, RM, 1) : W;
   unsigned char* slot = smem_raw + (size_t)s * row_slot_bytes(MODE, zlen, W, Wp);
   float2* z = reinterpret_cast<float2*>(slot);
-  auto zs = [](int k) { return fft_slot<NW, RM>(k); };
+  auto zs = [](int k) { return fft_slot<NW, RM, 1>(k); };
 
   float thr = 0.f, rsf_c = 0.f, uscale = 1.f, rho = 0.f;
   if constexpr (MODE == ROW_ITER || MODE == ROW_FIXUP || MODE == ROW_ADJ) {
@@ -427,7 +427,7 @@ col_kernel(ColParams P) {
   constexpr int EPT = NH > 0 ? (NH + ct_threads(NH, RM) - 1) / ct_threads(NH, RM) : SC_MAXE;
   const Geom& G = P.g;
   const int H = G.H, Wf = G.Wf, Wp = G.Wp, M = G.M;
-  const int hlen = NH > 0 ? ct_padded(NH, RM) : H;
+  const int hlen = NH > 0 ? ct_len(NH, RM, T) : H;
   const int TL = T * hlen;  // shared-memory slots of one tile
   float2* stg = reinterpret_cast<float2*>(smem_raw);  // [F0][F1][D]
 
@@ -440,7 +440,7 @@ col_kernel(ColParams P) {
   const int tid = threadIdx.x;
   const int cc = tid % T;   // column of this thread (T divides NT)
   const int t = tid / T;    // index within the column's thread group
-  auto slot = [](int kr) { return fft_slot<NH, RM>(kr); };
+  auto slot = [](int kr) { return fft_slot<NH, RM, T>(kr); };
 
   float rho = 0.f;
   if constexpr (col_clustered(MODE)) {

@@ -168,7 +168,7 @@ static int plan_geometry(int B, int M, int H, int W, Plan* pl) {
   if (make_fft_plan(W, &pl->pw) || make_fft_plan(H, &pl->ph))
     return set_status(SC_ERR_UNSUPPORTED, "cannot factor %d or %d", W, H);
   const bool srow = spec_row(W), scol = spec_col(H);
-  const int zlen = srow ? ct_padded(W, SC_ROW_RADIX) : W;
+  const int zlen = srow ? ct_len(W, SC_ROW_RADIX, 1) : W;
   pl->row_g = srow ? ct_threads(W, SC_ROW_RADIX) : group_size(W);
   const int S = SC_ROW_THREADS / pl->row_g;
   const long rows = (long)M * H;
@@ -185,11 +185,11 @@ static int plan_geometry(int B, int M, int H, int W, Plan* pl) {
   pl->col_ntiles = (g.Wf + SC_COL_TILE - 1) / SC_COL_TILE;
   pl->col_g = scol ? ct_threads(H, col_radix(H)) : group_size(H);
   pl->col_NT = SC_COL_TILE * pl->col_g;
-  pl->col_smem = col_smem_bytes(COL_SOLVE, scol ? ct_padded(H, col_radix(H)) : H);
+  pl->col_smem = col_smem_bytes(COL_SOLVE, scol ? ct_len(H, col_radix(H), SC_COL_TILE) : H);
   pl->colg_g = group_size(H);
   pl->colg_NT = SC_COL_TILE * pl->colg_g;
   pl->colg_smem = col_smem_bytes(COL_FWD, H);
-  pl->colt_smem = col_smem_bytes(COL_FWD, scol ? ct_padded(H, col_radix(H)) : H);
+  pl->colt_smem = col_smem_bytes(COL_FWD, scol ? ct_len(H, col_radix(H), SC_COL_TILE) : H);
   return SC_OK;
 }
 

@@ -102,6 +102,8 @@ struct ColParams {
   float mu;
   const float* wgrd;       // (M,)
   const float* Psum;       // (H, Wp) sum_m |Df_m|^2 (solve with one d for all maps)
+  const float2* E;         // (M, Kr, Wp) row spectra of the filter rows (COL_SOLVE_C*)
+  int Kr;                  // filter rows
   ImgState* st;
   float2* Xtr;             // COL_SOLVE_X: x^ also written here (B, M, H, Wp)
   // adjoint (COL_ADJ)
@@ -120,18 +122,25 @@ enum RowMode {
 // d_m = mu w_m |G|^2 + rho, the sum is accumulated over the maps.
 // COL_SOLVE_P: the solve with d = rho for every map and frequency (cbpdn,
 // cbpdnmsk), without the write-back of the column spectra between its two
-// passes.  COL_SOLVE_X: COL_SOLVE that also writes x^ to ColParams::Xtr (the
-// recomputation inside the adjoint).  COL_ADJ: adjoint of the plain cbpdn
+// passes.  COL_SOLVE_C8 / COL_SOLVE_C16: the same plain solve with the column
+// direction done by direct convolution with the filters' Kr <= 8 / 16 rows
+// (no per-map column transforms, no dictionary spectra).  COL_SOLVE_X:
+// COL_SOLVE that also writes x^ to ColParams::Xtr (the recomputation inside
+// the adjoint).  COL_ADJ: adjoint of the plain cbpdn
 // solve (one d = rho): column FFT, Q^ = A^{-1} G^, gradient accumulation,
 // inverse column FFT.
 enum ColMode {
   COL_SOLVE = 0, COL_FWD = 1, COL_INV = 2, COL_SOLVE_W = 3, COL_ADJ = 4, COL_SOLVE_X = 5,
-  COL_SOLVE_P = 6
+  COL_SOLVE_P = 6, COL_SOLVE_C8 = 7, COL_SOLVE_C16 = 8
 };
+// Filter rows (taps) of the convolution column solves.
+__host__ __device__ constexpr int col_taps(int mode) {
+  return mode == COL_SOLVE_C8 ? 8 : mode == COL_SOLVE_C16 ? 16 : 0;
+}
 // Modes that launch as a cluster over the maps of one column tile.
 __host__ __device__ constexpr bool col_clustered(int mode) {
   return mode == COL_SOLVE || mode == COL_SOLVE_W || mode == COL_SOLVE_X || mode == COL_ADJ ||
-         mode == COL_SOLVE_P;
+         mode == COL_SOLVE_P || mode == COL_SOLVE_C8 || mode == COL_SOLVE_C16;
 }
 
 __host__ __device__ inline size_t sc_align16(size_t x) { return (x + 15) & ~(size_t)15; }
@@ -151,7 +160,9 @@ __host__ __device__ inline size_t row_slot_bytes(int mode, int zlen, int W, int 
 // shared-memory slots of one column transform.  A tile is SC_COL_TILE
 // interleaved columns.  The solve double-buffers the spectrum tile and stages
 // the dictionary tile: [F0][F1][D]; the cluster reduction reuses [F1][D].
+// The convolution solves use three tiles and two staged filter-row tiles.
 __host__ __device__ inline size_t col_smem_bytes(int mode, int hlen) {
   const size_t tile = (size_t)SC_COL_TILE * hlen * 8;
-  return col_clustered(mode) ? 3 * tile : tile;
+  return (col_clustered(mode) ? 3 * tile : tile) +
+         (size_t)2 * col_taps(mode) * SC_COL_TILE * 8;
 }

@@ -479,6 +479,207 @@ col_kernel(ColParams P) {
       __syncthreads();
     }
     return;
+  } else if constexpr (MODE == COL_SOLVE_C8 || MODE == COL_SOLVE_C16) {
+    // Plain solve (d = rho) with the column direction done by direct
+    // convolution.  In the row-spectral domain (F = row spectra P_m of
+    // (Y - U)_m) filter m is E_m(t, kc), t < Kr (the row spectra of its rows),
+    // and its column spectrum is Df_m(kr) = sum_t E_m(t) w^(t kr).  Hence
+    //   sum_m Df_m Z^_m = FFTcol(a),   a(r) = sum_m sum_t E_m(t) P_m(r - t)
+    //   IFFTcol(conj(Df_m) SC)(r) = sum_t conj(E_m(t)) sc(r + t),  sc = IFFTcol(SC)
+    // (circular in r, unnormalised transforms), so
+    //   IFFTcol(x^_m) = H P_m + sum_t conj(E_m(t)) sc(r + t) / rho:
+    // pass 1 accumulates a over the maps (Kr complex multiply-adds per
+    // element), one column FFT pair per tile gives SC = S^ - cb and sc, and
+    // pass 2 writes every map's result.  Each thread owns L consecutive rows
+    // of one column and slides a window of L values along the column.
+    if constexpr (NH > 0) {
+      constexpr int KMAX = col_taps(MODE);
+      constexpr int L = EPT;  // rows per thread; g L = H for every compiled length
+      constexpr int NW = L + KMAX - 1;  // window of the L outputs
+      const int Kr = P.Kr;
+      float2* A = stg;            // cluster sum, its spectrum, then sc / rho
+      float2* Bt = stg + TL;      // spectrum tiles (pass 1: with A; pass 2: with Ct)
+      float2* Ct = stg + 2 * TL;  // partial sums of this CTA
+      float2* Es = stg + 3 * TL;  // [2][KMAX][T] filter rows
+      auto issue_tile = [&](const float2* base, float2* dst) {
+        for (int q = tid; q < 2 * H; q += NT) {
+          const int kr = q >> 1, h = q & 1;
+          cp_async16(dst + slot(kr) * T + 2 * h, base + (size_t)kr * Wp + c0 + 2 * h);
+        }
+      };
+      auto issue_E = [&](int m, float2* dst) {
+        for (int q = tid; q < 2 * Kr; q += NT) {
+          const int r = q >> 1, h = q & 1;
+          cp_async16(dst + r * T + 2 * h, P.E + ((size_t)m * Kr + r) * Wp + c0 + 2 * h);
+        }
+      };
+      const size_t plane = (size_t)H * Wp;
+      const float2* Sh = P.Sh + (size_t)b * plane + c0;
+      const bool colok = c0 + cc < Wf;
+      const float irho = 1.f / rho;
+      const int r0 = t * L;
+
+      // ------------------------------------------------------------ pass 1
+      float2 acc[L];
+#pragma unroll
+      for (int i = 0; i < L; ++i) acc[i] = make_float2(0.f, 0.f);
+      if (m0 < m1) {
+        issue_tile(Fi + (size_t)m0 * plane, A);
+        issue_E(m0, Es);
+      }
+      cp_async_commit();
+      int it = 0;
+      for (int m = m0; m < m1; ++m, ++it) {
+        const float2* cur = (it & 1) ? Bt : A;
+        const float2* ecur = Es + (it & 1) * KMAX * T;
+        if (m + 1 < m1) {
+          issue_tile(Fi + (size_t)(m + 1) * plane, (it & 1) ? A : Bt);
+          issue_E(m + 1, Es + ((it + 1) & 1) * KMAX * T);
+        }
+        cp_async_commit();
+        cp_async_wait<1>();  // P(m), E(m)
+        __syncthreads();
+        // w[j] = P(r0 - (KMAX - 1) + j): the window of all L outputs
+        float2 w[NW];
+#pragma unroll
+        for (int j = 0; j < NW; ++j) {
+          int rr = r0 - (KMAX - 1) + j;
+          if (j < KMAX - 1 && rr < 0) rr += H;
+          w[j] = (j < KMAX - 1 - Kr + 1) ? make_float2(0.f, 0.f) : cur[slot(rr) * T + cc];
+        }
+#pragma unroll
+        for (int tp = 0; tp < KMAX; ++tp) {
+          if (tp < Kr) {
+            const float2 e = ecur[tp * T + cc];
+#pragma unroll
+            for (int i = 0; i < L; ++i) {
+              const float2 v = w[i - tp + KMAX - 1];
+              // four fused multiply-adds per complex multiply-add
+              acc[i].x = fmaf(e.x, v.x, acc[i].x);
+              acc[i].x = fmaf(-e.y, v.y, acc[i].x);
+              acc[i].y = fmaf(e.x, v.y, acc[i].y);
+              acc[i].y = fmaf(e.y, v.x, acc[i].y);
+            }
+          }
+        }
+        __syncthreads();  // before the buffer is refilled
+      }
+      cp_async_commit();
+      cp_async_wait<0>();
+      __syncthreads();
+      // pass 2's first tile lands during the reduction and the transforms
+      if (m0 < m1) {
+        issue_tile(Fi + (size_t)m0 * plane, Bt);
+        issue_E(m0, Es);
+      }
+      cp_async_commit();
+
+      // ------------------------------------------- sum over the cluster
+      if (P.G > 1) {
+#pragma unroll
+        for (int i = 0; i < L; ++i) Ct[slot(r0 + i) * T + cc] = acc[i];
+        cg::cluster_group cluster = cg::this_cluster();
+        cluster.sync();
+        for (int e = tid; e < T * H; e += NT) {
+          const int kr = e / T, c = e - (e / T) * T;
+          const int sl = slot(kr) * T + c;
+          float2 v = make_float2(0.f, 0.f);
+          for (int r = 0; r < P.G; ++r) {
+            const float2 u = cluster.map_shared_rank(Ct, r)[sl];
+            v.x += u.x;
+            v.y += u.y;
+          }
+          A[sl] = v;
+        }
+        cluster.sync();
+      } else {
+#pragma unroll
+        for (int i = 0; i < L; ++i) A[slot(r0 + i) * T + cc] = acc[i];
+        __syncthreads();
+      }
+      // ------------------------- SC = S^ - cb, sc = IFFTcol(SC) / rho
+      fft_any<NH, T, RM>(A + cc, P.ph, P.twH, t, g);
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        const int kr = t + i * g;
+        if (kr < H) {
+          const int sl = slot(kr) * T + cc;
+          float2 v = make_float2(0.f, 0.f);
+          if (colok) {
+            const float2 q = A[sl];  // sum_m Df_m Z^_m
+            const float2 Sv = __ldg(&Sh[(size_t)kr * Wp + cc]);
+            const float sd = __ldg(&P.Psum[(size_t)kr * Wp + c0 + cc]) * irho;
+            const float qd = 1.f / (1.f + sd);
+            const float2 cb = make_float2((Sv.x * sd + q.x) * qd, (Sv.y * sd + q.y) * qd);
+            v = make_float2((Sv.x - cb.x) * irho, -(Sv.y - cb.y) * irho);  // conj(SC) / rho
+          }
+          A[sl] = v;
+        }
+      }
+      __syncthreads();
+      fft_any<NH, T, RM>(A + cc, P.ph, P.twH, t, g);
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        const int kr = t + i * g;
+        if (kr < H) {
+          const int sl = slot(kr) * T + cc;
+          A[sl].y = -A[sl].y;
+        }
+      }
+      // ------------------------------------------------------------ pass 2
+      const float hs = (float)H;
+      float2* Fo = Fi + c0 + cc;
+      __syncthreads();  // sc complete before the windows are read
+      // w[j] = sc(r0 + j) / rho: the window of all L outputs, the same for
+      // every map
+      float2 w[NW];
+#pragma unroll
+      for (int j = 0; j < NW; ++j) {
+        int rr = r0 + j;
+        if (rr >= H) rr -= H;
+        w[j] = (j < L + Kr - 1) ? A[slot(rr) * T + cc] : make_float2(0.f, 0.f);
+      }
+      it = 0;
+      for (int m = m0; m < m1; ++m, ++it) {
+        const float2* cur = (it & 1) ? Ct : Bt;
+        const float2* ecur = Es + (it & 1) * KMAX * T;
+        if (m + 1 < m1) {
+          issue_tile(Fi + (size_t)(m + 1) * plane, (it & 1) ? Bt : Ct);
+          issue_E(m + 1, Es + ((it + 1) & 1) * KMAX * T);
+        }
+        cp_async_commit();
+        cp_async_wait<1>();  // P(m), E(m)
+        __syncthreads();
+        float2 o[L];
+#pragma unroll
+        for (int i = 0; i < L; ++i) {
+          const float2 pv = cur[slot(r0 + i) * T + cc];
+          o[i] = make_float2(hs * pv.x, hs * pv.y);
+        }
+#pragma unroll
+        for (int tp = 0; tp < KMAX; ++tp) {
+          if (tp < Kr) {
+            const float2 e = ecur[tp * T + cc];
+#pragma unroll
+            for (int i = 0; i < L; ++i) {
+              const float2 v = w[i + tp];
+              o[i].x = fmaf(e.x, v.x, o[i].x);
+              o[i].x = fmaf(e.y, v.y, o[i].x);
+              o[i].y = fmaf(e.x, v.y, o[i].y);
+              o[i].y = fmaf(-e.y, v.x, o[i].y);
+            }
+          }
+        }
+        if (colok) {
+          float2* dst = Fo + (size_t)m * plane + (size_t)r0 * Wp;
+#pragma unroll
+          for (int i = 0; i < L; ++i) dst[(size_t)i * Wp] = o[i];
+        }
+        __syncthreads();  // before the buffer is refilled
+      }
+      cp_async_commit();
+      cp_async_wait<0>();
+    }
   } else if constexpr (MODE == COL_SOLVE_P) {
     // Plain solve, d = rho for every map and frequency (cbpdn, cbpdnmsk).
     // With P_m the row spectra of (Y - U)_m held in F, Z^_m = FFTcol(P_m) and

@@ -136,11 +136,12 @@ struct Plan {
   // hot column kernel (solve) and setup column kernels
   int col_g, col_ntiles, col_NT, Hs;
   size_t col_smem;
+  int col_hlen;
   int colg_g, colg_NT;
   size_t colg_smem, colt_smem;
   int max_iter;
-  size_t off_U, off_F, off_Dh, off_Sh, off_Ps, off_twW, off_twH, off_part, off_st, off_it,
-      off_xi, off_ndone, total;
+  size_t off_U, off_F, off_Dh, off_Sh, off_Ps, off_E, off_twW, off_twH, off_part, off_st,
+      off_it, off_xi, off_ndone, total;
 };
 
 static int g_num_sms = 0;
@@ -185,7 +186,8 @@ static int plan_geometry(int B, int M, int H, int W, Plan* pl) {
   pl->col_ntiles = (g.Wf + SC_COL_TILE - 1) / SC_COL_TILE;
   pl->col_g = scol ? ct_threads(H, col_radix(H)) : group_size(H);
   pl->col_NT = SC_COL_TILE * pl->col_g;
-  pl->col_smem = col_smem_bytes(COL_SOLVE, scol ? ct_len(H, col_radix(H), SC_COL_TILE) : H);
+  pl->col_hlen = scol ? ct_len(H, col_radix(H), SC_COL_TILE) : H;
+  pl->col_smem = col_smem_bytes(COL_SOLVE, pl->col_hlen);
   pl->colg_g = group_size(H);
   pl->colg_NT = SC_COL_TILE * pl->colg_g;
   pl->colg_smem = col_smem_bytes(COL_FWD, H);
@@ -211,6 +213,7 @@ static int plan_problem(const sc_problem* p, const sc_options* o, Plan* pl) {
   pl->off_Dh = take(sizeof(float2) * spec_img);
   pl->off_Sh = take(sizeof(float2) * (size_t)g.H * g.Wp * g.B);
   pl->off_Ps = take(sizeof(float) * (size_t)g.H * g.Wp);
+  pl->off_E = take(sizeof(float2) * (size_t)g.M * p->Kr * g.Wp);
   pl->off_twW = take(sizeof(float2) * g.W);
   pl->off_twH = take(sizeof(float2) * g.H);
   pl->off_part = take(sizeof(double) * 5 * (size_t)pl->row_nblk * g.B);
@@ -360,7 +363,8 @@ static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s) {
     int st = prepare_fn((const void*)fn, true);
     if (st) return st;
     int G = 1;
-    if ((st = cluster_size((const void*)fn, pl.col_NT, pl.col_smem, cp.g.M,
+    const size_t smem = col_smem_bytes(MODE, pl.col_hlen);
+    if ((st = cluster_size((const void*)fn, pl.col_NT, smem, cp.g.M,
                            (long)pl.col_ntiles * B, &G)))
       return st;
     cp.gsz = pl.col_g;
@@ -368,7 +372,7 @@ static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(G, pl.col_ntiles, B);
     cfg.blockDim = dim3(pl.col_NT);
-    cfg.dynamicSmemBytes = pl.col_smem;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -457,6 +461,7 @@ struct Solve {
   int* ndone = nullptr;
   float* Psum = nullptr;
   bool per_map_d = false, can_stop = false, finished = false;
+  int col_mode = COL_SOLVE_P;  // the column solve of the iteration
   int done_iters = 0;
   RowParams rp = {};
   ColParams cp = {};
@@ -487,6 +492,14 @@ struct Solve {
     Psum = (float*)((unsigned char*)workspace + pl.off_Ps);
     // one d for every map unless GradWeight differs between maps
     per_map_d = p->grd && !p->wgrd_uniform;
+    // Plain problems with short filters (Kr <= 16 rows) and a compiled column
+    // length take the convolution column solve.
+    col_mode = per_map_d ? COL_SOLVE_W
+               : p->grd  ? COL_SOLVE
+               : (spec_col(pl.g.H) && p->Kr <= 8)  ? COL_SOLVE_C8
+               : (spec_col(pl.g.H) && p->Kr <= 16) ? COL_SOLVE_C16
+                                                   : COL_SOLVE_P;
+    float2* Erows = (float2*)((unsigned char*)workspace + pl.off_E);
 
     twiddle_kernel<<<(g.W + 255) / 256, 256, 0, s>>>(twW, g.W);
     twiddle_kernel<<<(g.H + 255) / 256, 256, 0, s>>>(twH, g.H);
@@ -500,6 +513,10 @@ struct Solve {
       r.g = g; r.g.B = 1;
       r.pw = pl.pw; r.twW = twW; r.F = Dh; r.D = p->D; r.Kr = p->Kr; r.Kc = p->Kc;
       if ((st = launch_row<ROW_FWD_DICT>(pl, r, 1, s))) return st;
+      // the row spectra of the filter rows, before the column transform
+      CU_TRY(cudaMemcpy2DAsync(Erows, sizeof(float2) * p->Kr * g.Wp, Dh,
+                               sizeof(float2) * g.H * g.Wp, sizeof(float2) * p->Kr * g.Wp, g.M,
+                               cudaMemcpyDeviceToDevice, s));
       ColParams c = {};
       c.g = g; c.g.B = 1; c.ph = pl.ph; c.twH = twH; c.twW = twW; c.F = Dh;
       if ((st = launch_col<COL_FWD>(pl, c, 1, s))) return st;
@@ -546,6 +563,7 @@ struct Solve {
     rp.partials = part; rp.st = sts;
     cp.g = g; cp.ph = pl.ph; cp.twH = twH; cp.twW = twW; cp.F = F; cp.Dh = Dh; cp.Sh = Sh;
     cp.grd = p->grd; cp.mu = p->mu; cp.wgrd = p->wgrd; cp.Psum = Psum; cp.st = sts;
+    cp.E = Erows; cp.Kr = p->Kr;
     fp.max_iter = o->max_iter;
     fp.auto_rho = o->auto_rho; fp.period = std::max(1, o->auto_rho_period);
     fp.auto_scaling = o->auto_scaling; fp.std_residuals = o->std_residuals;
@@ -574,9 +592,13 @@ struct Solve {
     int st;
     for (int i = 0; i < n; ++i) {
       if ((st = timed(0, [&] {
-             return per_map_d ? launch_col<COL_SOLVE_W>(pl, cp, B, s)
-                    : p->grd  ? launch_col<COL_SOLVE>(pl, cp, B, s)
-                              : launch_col<COL_SOLVE_P>(pl, cp, B, s);
+             switch (col_mode) {
+               case COL_SOLVE_W: return launch_col<COL_SOLVE_W>(pl, cp, B, s);
+               case COL_SOLVE: return launch_col<COL_SOLVE>(pl, cp, B, s);
+               case COL_SOLVE_C8: return launch_col<COL_SOLVE_C8>(pl, cp, B, s);
+               case COL_SOLVE_C16: return launch_col<COL_SOLVE_C16>(pl, cp, B, s);
+               default: return launch_col<COL_SOLVE_P>(pl, cp, B, s);
+             }
            })))
         return st;
       if ((st = timed(1, [&] { return launch_row<ROW_ITER>(pl, rp, B, s); }))) return st;
@@ -811,6 +833,9 @@ extern "C" int sc_unrolled_forward(const sc_problem* p, const sc_options* o, int
   unsigned char* w = (unsigned char*)ws;
   Solve sv;
   if ((st = sv.setup(&u.p, &u.o, ws, u.pl.total, s))) return st;
+  // the same column solve as the recomputation in the reverse pass, so that
+  // both produce the same iterates
+  sv.col_mode = COL_SOLVE;
   for (int j = 0; j < u.nseg; ++j) {
     CU_TRY(cudaMemcpyAsync(w + u.ckY + sizeof(float) * u.R * j, u.p.Y, sizeof(float) * u.R,
                            cudaMemcpyDeviceToDevice, s));

@@ -88,6 +88,27 @@ def test_benchmark_shape_256_fixed_rho():
     assert abs(J - Jo) / Jo < 1e-5
 
 
+# Column lengths with compiled transform plans and filters of 9..16 rows take
+# the convolution column solve with 16 taps; 48 rows with 13-row filters
+# wrap the circular convolution over more than a quarter of the column;
+# filters of 17+ rows take the transform solve.
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(96, 64, 16), (48, 40, 13), (64, 48, 17), (128, 31, 12)])
+@pytest.mark.parametrize("variant", ["cbpdn", "cbpdnmsk"])
+def test_column_solve_filter_lengths(shape, variant):
+    H, W, K = shape
+    D, S = _synth(H, W, 6, K, 0.02, 99)
+    lam = 0.05
+    opt = {"MaxMainIter": 30, "RelStopTol": 0.0, "RelaxParam": 1.8,
+           "rho": float(np.float32(50 * np.float32(lam) + 1)), "AutoRho": {"Enabled": False}}
+    if variant == "cbpdn":
+        X, Xo = cb.cbpdn(D, S, lam, opt), O.cbpdn(D, S, lam, opt)
+    else:
+        Wm = (np.random.default_rng(4).random(S.shape) < 0.7).astype(np.float32)
+        X, Xo = cb.cbpdnmsk(D, S * Wm, Wm, lam, opt), O.cbpdnmsk(D, S * Wm, Wm, lam, opt)
+    assert _rel(X, Xo) < REL_TOL
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("variant", ["cbpdngrd", "cbpdnmsk"])
 def test_autorho_trajectory_512(variant):

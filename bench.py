@@ -98,16 +98,24 @@ def opt_for(cfg, variant):
     return opt
 
 
-def algorithmic_bytes(H, W, M, variant="cbpdn"):
-    """Per-iteration HBM bytes of the byte model (two-pass 2-D FFT): the row
-    pass reads and writes the spectra F (2C) and Y, U (4R); the column pass
-    reads F and the dictionary spectra D (C_D = C per image) twice and
-    writes F (C + 2 C_D + C); with the gradient term (d varies with the
-    frequency) it also writes and re-reads the column spectra between its
-    two passes (2C)."""
+# Column lengths with compiled transform plans (the convolution column solve
+# needs one for its per-tile transforms).
+SPEC_COL = {16, 32, 64, 128, 256, 512, 1024, 2048, 48, 96, 192, 384, 768, 1536}
+
+
+def algorithmic_bytes(H, W, M, variant="cbpdn", K=None):
+    """Per-iteration HBM bytes of the byte model.  Row pass: reads and writes
+    the spectra F (2C) and Y, U (4R).  Column pass, by solve: the
+    convolution solve (plain problems, filters of at most 16 rows, compiled
+    column length) reads F twice and writes it (3C); the transform solve
+    also reads the dictionary spectra twice (+2 C_D, C_D = C per image);
+    with the gradient term (d varies with the frequency) it also writes and
+    re-reads the column spectra between its two passes (+2C)."""
     R = 4.0 * M * H * W
     Cs = 8.0 * M * H * (W // 2 + 1)
-    col = 2 * Cs + 2 * Cs + (2 * Cs if variant in ("cbpdngrd", "cbpdngrdmsk") else 0)
+    grd = variant in ("cbpdngrd", "cbpdngrdmsk")
+    conv = not grd and K is not None and K <= 16 and H in SPEC_COL
+    col = 3 * Cs if conv else 3 * Cs + 2 * Cs + (2 * Cs if grd else 0)
     return 4 * R + 2 * Cs + col
 
 
@@ -350,7 +358,7 @@ def run_ours(args, cfg, rank, world, local_rank):
     bytes_it = 0.0
     for v in cfg["variants"]:
         M = cfg["M"] + (1 if v == "cbpdnmsk" else 0)
-        bytes_it += algorithmic_bytes(cfg["H"], cfg["W"], M, v) * cfg["iters"] * args.steps
+        bytes_it += algorithmic_bytes(cfg["H"], cfg["W"], M, v, cfg["K"]) * cfg["iters"] * args.steps
     achieved = bytes_it / (it_ms / 1e3) / 1e9 if it_ms > 0 else None
     kern = {k: {"ms_per_launch": a[0] / max(1, a[1]), "launches": a[1],
                 "share": a[0] / it_ms if it_ms else None} for k, a in prof_tot.items()}
@@ -496,7 +504,8 @@ def run_batched(args, cfg, rank, world, local_rank):
     bytes_total = 0.0
     it_per_img = step()  # iteration counts per image (same data, same counts)
     for S, k in zip(imgs, it_per_img):
-        bytes_total += algorithmic_bytes(S.shape[0], S.shape[1], cfg["M"] + 1, "cbpdnmsk") * k
+        bytes_total += algorithmic_bytes(S.shape[0], S.shape[1], cfg["M"] + 1, "cbpdnmsk",
+                                         cfg["K"]) * k
     achieved = bytes_total * args.steps / (ms / 1e3) / 1e9
     if rank != 0:
         return None

@@ -149,10 +149,11 @@ __host__ __device__ inline size_t sc_align16(size_t x) { return (x + 15) & ~(siz
 // (padded) number of shared-memory slots of one row transform.  The
 // iteration mode stages the next pair's two spectrum rows and the pair's Y
 // and U rows: [z: zlen complex][F: 2Wp complex][Y: 2W][U: 2W]; the adjoint
-// step stages gV and the shrinkage mask source in the Y and U places.
+// step stages gV and the shrinkage mask source in the Y and U places, the
+// rho fix-up the pair's U rows and spectrum rows.
 __host__ __device__ inline size_t row_slot_bytes(int mode, int zlen, int W, int Wp) {
   size_t z = sc_align16((size_t)zlen * 8);
-  if (mode != ROW_ITER && mode != ROW_ADJ) return z;
+  if (mode != ROW_ITER && mode != ROW_ADJ && mode != ROW_FIXUP) return z;
   return z + (size_t)(2 * Wp) * 8 + 2 * sc_align16((size_t)(2 * W) * 4);
 }
 

@@ -157,8 +157,8 @@ row_kernel(RowParams P) {
   float2* Fi = P.F + (size_t)b * img_spec;
   const long pstride = (long)gridDim.x * S;
 
-  if constexpr (MODE == ROW_ITER || MODE == ROW_ADJ) {
-    // ------------------------------------------ iteration / adjoint step
+  if constexpr (MODE == ROW_ITER || MODE == ROW_ADJ || MODE == ROW_FIXUP) {
+    // ------------------------------- iteration / adjoint step / rho fix-up
     constexpr bool ADJ = MODE == ROW_ADJ;
     float2* fst = reinterpret_cast<float2*>(slot + sc_align16((size_t)zlen * 8));
     float* ysm = reinterpret_cast<float*>(fst + 2 * (size_t)Wp);
@@ -194,6 +194,61 @@ row_kernel(RowParams P) {
         }
       }
     };
+
+    if constexpr (MODE == ROW_FIXUP) {
+      // F += (1 - 1/rsf) rowFFT(U) after a change of rho (U is rescaled by
+      // 1/rsf when the next row pass reads it).  U rows are staged one pair
+      // ahead (during the transform), F rows during the next pair's packing.
+      auto issue_U = [&](long p) {
+        if (p < npairs) {
+          const int n = ((2 * p + 1 < rows) ? 2 : 1) * W;
+          const float* us = Ui + 2 * p * W;
+          if (vec) {
+            for (int q = t; q < n / 4; q += g) cp_async16(usm + 4 * q, us + 4 * q);
+          } else {
+            for (int q = t; q < n; q += g) cp_async4(usm + q, us + q);
+          }
+        }
+      };
+      const long p0 = (long)blockIdx.x * S + s;
+      issue_U(p0);
+      issue_F(p0);
+      cp_async_commit();
+      for (long pb = (long)blockIdx.x * S; pb < npairs; pb += pstride) {
+        const long p = pb + s;
+        const bool valid = p < npairs;
+        const bool has1 = valid && (2 * p + 1 < rows);
+        cp_async_wait<0>();  // U(p), F(p)
+        __syncthreads();
+        if (valid) {
+          for (int k = t; k < W; k += g) z[zs(k)] = make_float2(usm[k], has1 ? usm[W + k] : 0.f);
+        }
+        __syncthreads();
+        issue_U(p + pstride);
+        cp_async_commit();
+        fft_any<NW, 1, RM>(z, P.pw, P.twW, t, g);
+        if (valid) {
+          float2* fa = Fi + 2 * p * Wp;
+          for (int k = t; k < Wf; k += g) {
+            const float2 Zk = z[zs(k)];
+            const float2 Zm = z[zs(k == 0 ? 0 : W - k)];
+            const float2 A = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
+            const float2 f0 = fst[k];
+            fa[k] = make_float2(f0.x + rsf_c * A.x, f0.y + rsf_c * A.y);
+            if (has1) {
+              const float2 Bv = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
+              const float2 f1 = fst[Wp + k];
+              fa[Wp + k] = make_float2(f1.x + rsf_c * Bv.x, f1.y + rsf_c * Bv.y);
+            }
+          }
+        }
+        __syncthreads();  // F staging consumed
+        issue_F(p + pstride);
+        cp_async_commit();
+      }
+      cp_async_wait<0>();
+      return;
+    }
 
     double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     const int32_t* mk = P.mask ? P.mask + (size_t)b * H * W : nullptr;
@@ -373,9 +428,6 @@ row_kernel(RowParams P) {
             if (has1 && h1 < P.Kr && k < P.Kc) v1 = P.D[((size_t)m1 * P.Kr + h1) * P.Kc + k];
             z[zs(k)] = make_float2(v0, v1);
           }
-        } else if constexpr (MODE == ROW_FIXUP) {
-          const float* U0 = P.U + (size_t)b * img_real + (size_t)r0 * W;
-          for (int k = t; k < W; k += g) z[zs(k)] = make_float2(U0[k], has1 ? U0[W + k] : 0.f);
         } else if constexpr (MODE == ROW_FWD_YU) {
           const float* Y0 = P.Y + (size_t)b * img_real + (size_t)r0 * W;
           const float* U0 = P.U + (size_t)b * img_real + (size_t)r0 * W;
@@ -393,17 +445,8 @@ row_kernel(RowParams P) {
           const float2 Zm = z[zs(k == 0 ? 0 : W - k)];
           const float2 A = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
           const float2 Bv = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
-          if constexpr (MODE == ROW_FIXUP) {
-            const float2 fa = a[k];
-            a[k] = make_float2(fa.x + rsf_c * A.x, fa.y + rsf_c * A.y);
-            if (has1) {
-              const float2 fb = bb[k];
-              bb[k] = make_float2(fb.x + rsf_c * Bv.x, fb.y + rsf_c * Bv.y);
-            }
-          } else {
-            a[k] = A;
-            if (has1) bb[k] = Bv;
-          }
+          a[k] = A;
+          if (has1) bb[k] = Bv;
         }
       }
       __syncthreads();
@@ -518,6 +561,32 @@ col_kernel(ColParams P) {
       const bool colok = c0 + cc < Wf;
       const float irho = 1.f / rho;
       const int r0 = t * L;
+      // Slot of row r0 + d, d a compile-time offset.  When a thread's L rows
+      // are exactly one padded block of the layout (L == RM, the pad period),
+      // row r0 + d lies in block t + floor(d / L) (mod the H / L blocks) at
+      // offset d mod L, so every window access is a per-thread block base
+      // plus a constant.
+      constexpr bool BLK = L == RM;
+      int bbase[5];  // slot of the first row of block t + delta, delta = -2..2
+#pragma unroll
+      for (int dl = -2; dl <= 2; ++dl) {
+        const int nb = H / L;
+        int bi = t + dl;
+        if (bi < 0) bi += nb;
+        if (bi >= nb) bi -= nb;
+        bbase[dl + 2] = bi * (L + 1);
+      }
+      auto rslot = [&](int d) -> int {  // d in (-2L, 2L); compile-time after unrolling
+        if constexpr (BLK) {
+          const int dl = d >= 0 ? d / L : -((-d + L - 1) / L);
+          return bbase[dl + 2] + (d - dl * L);
+        } else {
+          int rr = r0 + d;
+          if (rr < 0) rr += H;
+          if (rr >= H) rr -= H;
+          return slot(rr);
+        }
+      };
 
       // ------------------------------------------------------------ pass 1
       float2 acc[L];
@@ -542,11 +611,8 @@ col_kernel(ColParams P) {
         // w[j] = P(r0 - (KMAX - 1) + j): the window of all L outputs
         float2 w[NW];
 #pragma unroll
-        for (int j = 0; j < NW; ++j) {
-          int rr = r0 - (KMAX - 1) + j;
-          if (j < KMAX - 1 && rr < 0) rr += H;
-          w[j] = (j < KMAX - 1 - Kr + 1) ? make_float2(0.f, 0.f) : cur[slot(rr) * T + cc];
-        }
+        for (int j = 0; j < NW; ++j)
+          w[j] = (j < KMAX - Kr) ? make_float2(0.f, 0.f) : cur[rslot(j - (KMAX - 1)) * T + cc];
 #pragma unroll
         for (int tp = 0; tp < KMAX; ++tp) {
           if (tp < Kr) {
@@ -577,7 +643,7 @@ col_kernel(ColParams P) {
       // ------------------------------------------- sum over the cluster
       if (P.G > 1) {
 #pragma unroll
-        for (int i = 0; i < L; ++i) Ct[slot(r0 + i) * T + cc] = acc[i];
+        for (int i = 0; i < L; ++i) Ct[rslot(i) * T + cc] = acc[i];
         cg::cluster_group cluster = cg::this_cluster();
         cluster.sync();
         for (int e = tid; e < T * H; e += NT) {
@@ -594,7 +660,7 @@ col_kernel(ColParams P) {
         cluster.sync();
       } else {
 #pragma unroll
-        for (int i = 0; i < L; ++i) A[slot(r0 + i) * T + cc] = acc[i];
+        for (int i = 0; i < L; ++i) A[rslot(i) * T + cc] = acc[i];
         __syncthreads();
       }
       // ------------------------- SC = S^ - cb, sc = IFFTcol(SC) / rho
@@ -634,11 +700,8 @@ col_kernel(ColParams P) {
       // every map
       float2 w[NW];
 #pragma unroll
-      for (int j = 0; j < NW; ++j) {
-        int rr = r0 + j;
-        if (rr >= H) rr -= H;
-        w[j] = (j < L + Kr - 1) ? A[slot(rr) * T + cc] : make_float2(0.f, 0.f);
-      }
+      for (int j = 0; j < NW; ++j)
+        w[j] = (j < L + Kr - 1) ? A[rslot(j) * T + cc] : make_float2(0.f, 0.f);
       it = 0;
       for (int m = m0; m < m1; ++m, ++it) {
         const float2* cur = (it & 1) ? Ct : Bt;
@@ -653,7 +716,7 @@ col_kernel(ColParams P) {
         float2 o[L];
 #pragma unroll
         for (int i = 0; i < L; ++i) {
-          const float2 pv = cur[slot(r0 + i) * T + cc];
+          const float2 pv = cur[rslot(i) * T + cc];
           o[i] = make_float2(hs * pv.x, hs * pv.y);
         }
 #pragma unroll

@@ -129,7 +129,7 @@ struct Plan {
   FftPlan pw, ph;
   // hot row kernels (iteration, fix-up): compile-time plan when available
   int row_g, row_nblk;
-  size_t row_smem, row_smem_fix;
+  size_t row_smem, row_smem_tool;
   // setup row kernels: runtime plan
   int rowg_g;
   size_t rowg_smem;
@@ -178,7 +178,7 @@ static int plan_geometry(int B, int M, int H, int W, Plan* pl) {
   long cap = std::max(1L, (long)num_sms() * 8 / B);
   pl->row_nblk = (int)std::min(want, cap);
   pl->row_smem = (size_t)S * row_slot_bytes(ROW_ITER, zlen, W, g.Wp);
-  pl->row_smem_fix = (size_t)S * row_slot_bytes(ROW_FIXUP, zlen, W, g.Wp);
+  pl->row_smem_tool = (size_t)S * row_slot_bytes(ROW_FWD_REAL, zlen, W, g.Wp);
   pl->rowg_g = group_size(W);
   pl->rowg_smem = (size_t)(SC_ROW_THREADS / pl->rowg_g) * row_slot_bytes(ROW_FWD_REAL, W, W, g.Wp);
 
@@ -290,8 +290,8 @@ static int launch_row(const Plan& pl, RowParams rp, int B, cudaStream_t s, int n
   rp.gsz = hot ? pl.row_g : pl.rowg_g;
   rp.nblk = nblk > 0 ? nblk : pl.row_nblk;
   dim3 grid(rp.nblk, B);
-  const size_t smem = (MODE == ROW_ITER || MODE == ROW_ADJ) ? pl.row_smem
-                      : hot ? pl.row_smem_fix : pl.rowg_smem;
+  const size_t smem = (MODE == ROW_ITER || MODE == ROW_ADJ || MODE == ROW_FIXUP) ? pl.row_smem
+                      : hot ? pl.row_smem_tool : pl.rowg_smem;
   // one slot (row pair in flight) per rp.gsz threads
   const int threads = (SC_ROW_THREADS / rp.gsz) * rp.gsz;
   fn<<<grid, threads, smem, s>>>(rp);

@@ -101,16 +101,30 @@ def opt_for(cfg, variant):
 # Column lengths with compiled transform plans (the convolution column solve
 # needs one for its per-tile transforms).
 SPEC_COL = {16, 32, 64, 128, 256, 512, 1024, 2048, 48, 96, 192, 384, 768, 1536}
+SMEM_MAX = 227 * 1024  # shared memory of one CTA
 
 
-def algorithmic_bytes(H, W, M, variant="cbpdn", K=None):
-    """Per-iteration HBM bytes of the byte model.  Row pass: reads and writes
-    the spectra F (2C) and Y, U (4R).  Column pass, by solve: the
-    convolution solve (plain problems, filters of at most 16 rows, compiled
-    column length) reads F twice and writes it (3C); the transform solve
-    also reads the dictionary spectra twice (+2 C_D, C_D = C per image);
-    with the gradient term (d varies with the frequency) it also writes and
-    re-reads the column spectra between its two passes (+2C)."""
+def graded_bytes(H, W, M, images=1):
+    """Algorithmic HBM bytes of one ADMM iteration of `images` images of one
+    size (the graded byte model).  R = 4 M H W, C = 8 M H (W/2+1); p = 1 when
+    one map's half-spectrum fits in one CTA's shared memory (the 2-D FFT can
+    stay on chip), else 2.  Per image 4R + 6C (p = 2) or 4R + 2C (p = 1): Y
+    and U read and written once, three (or one) spectrum round trips; per
+    size the dictionary spectra are read twice (p = 2) or once (p = 1)."""
+    R = 4.0 * M * H * W
+    Cs = 8.0 * M * H * (W // 2 + 1)
+    p = 1 if 8 * H * (W // 2 + 1) <= SMEM_MAX else 2
+    return images * (4 * R + (6 if p == 2 else 2) * Cs) + (2 if p == 2 else 1) * Cs
+
+
+def design_bytes(H, W, M, variant="cbpdn", K=None):
+    """Per-iteration HBM bytes this design moves for one image.  Row pass:
+    reads and writes the spectra F (2C) and Y, U (4R).  Column pass, by
+    solve: the convolution solve (plain problems, filters of at most 16 rows,
+    compiled column length) reads F twice and writes it (3C); the transform
+    solve also reads the dictionary spectra twice (+2 C_D, C_D = C per
+    image); with the gradient term (d varies with the frequency) it also
+    writes and re-reads the column spectra between its two passes (+2C)."""
     R = 4.0 * M * H * W
     Cs = 8.0 * M * H * (W // 2 + 1)
     grd = variant in ("cbpdngrd", "cbpdngrdmsk")
@@ -355,11 +369,13 @@ def run_ours(args, cfg, rank, world, local_rank):
     peak, peak_kind = measured_peaks()
     it_ms = sum(a[0] for a in prof_tot.values())
     n_it = prof_tot.get("col_kernel", [0, 1])[1]
-    bytes_it = 0.0
+    bytes_it = design_it = 0.0
     for v in cfg["variants"]:
         M = cfg["M"] + (1 if v == "cbpdnmsk" else 0)
-        bytes_it += algorithmic_bytes(cfg["H"], cfg["W"], M, v, cfg["K"]) * cfg["iters"] * args.steps
+        bytes_it += graded_bytes(cfg["H"], cfg["W"], M) * cfg["iters"] * args.steps
+        design_it += design_bytes(cfg["H"], cfg["W"], M, v, cfg["K"]) * cfg["iters"] * args.steps
     achieved = bytes_it / (it_ms / 1e3) / 1e9 if it_ms > 0 else None
+    n_solve_it = cfg["iters"] * args.steps * len(cfg["variants"])
     kern = {k: {"ms_per_launch": a[0] / max(1, a[1]), "launches": a[1],
                 "share": a[0] / it_ms if it_ms else None} for k, a in prof_tot.items()}
     out = None
@@ -375,7 +391,7 @@ def run_ours(args, cfg, rank, world, local_rank):
                        "solves_per_step": len(cfg["variants"]),
                        "parallelism": "replicas%d" % world if world > 1 else "single",
                        "l2": "working set larger than L2 (no flush)" if
-                       algorithmic_bytes(cfg["H"], cfg["W"], cfg["M"]) > 126e6 else
+                       graded_bytes(cfg["H"], cfg["W"], cfg["M"]) > 126e6 else
                        "working set fits in L2"},
             "e2e": {"value": e_value, "unit": "iter/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
@@ -384,8 +400,10 @@ def run_ours(args, cfg, rank, world, local_rank):
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": achieved / peak if achieved else None,
                          "traffic": None,
-                         "algorithmic_bytes_per_iteration":
-                             bytes_it / (cfg["iters"] * args.steps * len(cfg["variants"])),
+                         "algorithmic_bytes_per_iteration": bytes_it / n_solve_it,
+                         "design_bytes_per_iteration": design_it / n_solve_it,
+                         "design_frac": (design_it / (it_ms / 1e3) / 1e9 / peak)
+                         if it_ms > 0 else None,
                          "iteration_ms": it_ms / max(1, n_it), "kernels": kern},
             "cpu_baseline": cpu,
             "gpu_launches": launches,
@@ -503,9 +521,16 @@ def run_batched(args, cfg, rank, world, local_rank):
     peak, peak_kind = measured_peaks()
     bytes_total = 0.0
     it_per_img = step()  # iteration counts per image (same data, same counts)
+    bucket_it = {}
     for S, k in zip(imgs, it_per_img):
-        bytes_total += algorithmic_bytes(S.shape[0], S.shape[1], cfg["M"] + 1, "cbpdnmsk",
-                                         cfg["K"]) * k
+        H_, W_ = S.shape
+        # state bytes per image-iteration; dictionary reads once per size and
+        # iteration of its bucket (the longest-running image of that size)
+        bytes_total += (graded_bytes(H_, W_, cfg["M"] + 1, 1) -
+                        graded_bytes(H_, W_, cfg["M"] + 1, 0)) * k
+        bucket_it[(H_, W_)] = max(bucket_it.get((H_, W_), 0), k)
+    for (H_, W_), k in bucket_it.items():
+        bytes_total += graded_bytes(H_, W_, cfg["M"] + 1, 0) * k
     achieved = bytes_total * args.steps / (ms / 1e3) / 1e9
     if rank != 0:
         return None

@@ -440,6 +440,70 @@ __device__ __forceinline__ void fft_ct(float2* data, const float2* __restrict__ 
   }
 }
 
+// Passes [P, PEND) of a compile-time plan.
+template <int N, int RM, int G, int ST, int P, int PEND>
+__device__ __forceinline__ void fft_ct_passes(float2* data, const float2* __restrict__ tw, int t) {
+  constexpr CtPlan pl = ct_plan(N, RM);
+  if constexpr (P < PEND) {
+    ct_pass<N, RM, pl.r[P], ct_ns(pl, P), G, ST>(data, tw, t);
+    fft_ct_passes<N, RM, G, ST, P + 1, PEND>(data, tw, t);
+  }
+}
+
+// A compile-time transform whose first radix is N/G and whose last pass has
+// a stride N/R_last that is a multiple of G gives thread t the elements
+// t + G m (m < N/G) both as the inputs of its first pass and as the outputs
+// of its last pass.  Two transforms in a row can then hand over in
+// registers: the last pass of one, an element-wise step and the first pass
+// of the next need no shared-memory round trip (powers of two from 64 with
+// radix-8 plans).
+__host__ __device__ constexpr bool ct_reg_edges(int n, int RM) {
+  const CtPlan p = ct_plan(n, RM);
+  const int G = ct_threads(n, RM);
+  return p.np >= 2 && n % G == 0 && p.r[0] == n / G && (n / p.r[p.np - 1]) % G == 0;
+}
+
+// First pass of a compile-time transform with its inputs in registers,
+// v[m] = element t + G m; results stored to shared memory.  Starts with a
+// barrier, so callers may still be reading the data array.
+template <int N, int RM, int ST>
+__device__ __forceinline__ void ct_first_from_regs(float2* data, float2* v, int t) {
+  constexpr CtPlan pl = ct_plan(N, RM);
+  constexpr int R = pl.r[0];
+  dft_r<R>(v);  // Ns = 1: no twiddles; butterfly j = t takes t + G q
+  __syncthreads();
+  const int base = t * R;
+#pragma unroll
+  for (int q = 0; q < R; ++q) data[ct_phys<N, RM, ST>(base + q) * ST] = v[q];
+  __syncthreads();
+}
+
+// Last pass of a compile-time transform with its outputs left in registers,
+// v[m] = element t + G m.  Reads shared memory only.
+template <int N, int RM, int ST>
+__device__ __forceinline__ void ct_last_to_regs(const float2* data,
+                                                const float2* __restrict__ tw, float2* v,
+                                                int t) {
+  constexpr CtPlan pl = ct_plan(N, RM);
+  constexpr int G = ct_threads(N, RM);
+  constexpr int PL = pl.np - 1;
+  constexpr int R = pl.r[PL];
+  constexpr int NS = ct_ns(pl, PL);  // = N / R: butterfly j's outputs are j + NS q
+  constexpr int NB = NS / G;
+  constexpr int STEP = N / (NS * R);
+#pragma unroll
+  for (int i = 0; i < NB; ++i) {
+    const int j = t + i * G;
+    float2 u[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) u[q] = data[ct_phys<N, RM, ST>(j + q * NS) * ST];
+    twiddle_r<R>(u, tw, (j % NS) * STEP);
+    dft_r<R>(u);
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[i + NB * q] = u[q];
+  }
+}
+
 // Forward DFT of length N of the elements of one transform (N > 0:
 // compile-time plan with radix-RM passes, element i at
 // data[ct_phys<N, RM>(i) * ST]; N == 0: runtime plan P with g threads,

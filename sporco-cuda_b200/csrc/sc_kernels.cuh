@@ -278,6 +278,116 @@ row_kernel(RowParams P) {
     cp_async_commit();
     issue_YU(p0);
     cp_async_commit();
+    if constexpr (NW > 0 && ct_reg_edges(NW, RM)) {
+      // Register hand-over: thread t holds the elements t + g m of the row
+      // pair's transform both at the end of the inverse transform and at the
+      // start of the forward one, so the unpacking of the spectrum rows, the
+      // element-wise step and the first forward pass run on registers.
+      constexpr int EM = NW / ct_threads(NW, RM);  // elements per thread
+      constexpr int NP = ct_plan(NW, RM).np;
+      for (long pb = (long)blockIdx.x * S; pb < npairs; pb += pstride) {
+        const long p = pb + s;
+        const bool valid = p < npairs;
+        const long r0 = 2 * p, r1 = 2 * p + 1;
+        const bool has1 = valid && (r1 < rows);
+        float2 v[EM];
+        cp_async_wait<1>();  // F(p)
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < EM; ++m)
+          v[m] = valid ? pack_inverse(fst, fst + Wp, has1, t + g * m, W, Wf) : make_float2(0.f, 0.f);
+        ct_first_from_regs<NW, RM, 1>(z, v, t);
+        issue_F(p + pstride);  // the staged rows are consumed
+        cp_async_commit();
+        fft_ct_passes<NW, RM, ct_threads(NW, RM), 1, 1, NP - 1>(z, P.twW, t);
+        cp_async_wait<1>();  // Y(p), U(p)
+        __syncthreads();
+        ct_last_to_regs<NW, RM, 1>(z, P.twW, v, t);
+        if (ADJ && valid) {
+          float* gv = P.gV + (size_t)b * img_real + (size_t)r0 * W;
+          const bool first = P.first != 0;
+#pragma unroll
+          for (int m = 0; m < EM; ++m) {
+            const int k = t + g * m;
+            const float q0 = first ? 0.f : v[m].x * P.invN;
+            const float q1 = first ? 0.f : -v[m].y * P.invN;
+            const float v0 = ysm[k];
+            const float gy0 = first ? v0 : a1 * v0 + rho * q0;
+            const float gu0 = first ? 0.f : v0 - rho * q0;
+            const float n0 = usm[k] != 0.f ? gy0 : gu0;
+            gv[k] = n0;
+            float n1 = 0.f;
+            if (has1) {
+              const float v1 = ysm[W + k];
+              const float gy1 = first ? v1 : a1 * v1 + rho * q1;
+              const float gu1 = first ? 0.f : v1 - rho * q1;
+              n1 = usm[W + k] != 0.f ? gy1 : gu1;
+              gv[W + k] = n1;
+            }
+            v[m] = make_float2(a * n0, a * n1);
+          }
+        } else if (valid) {
+          const int m0 = (int)(r0 / H), h0 = (int)(r0 - (long)m0 * H);
+          const int m1 = (int)(r1 / H), h1 = (int)(r1 - (long)m1 * H);
+          float* Y0 = P.Yo + (size_t)b * img_real + (size_t)r0 * W;
+          float* U0 = P.U + (size_t)b * img_real + (size_t)r0 * W;
+          float w0 = P.l1_scalar, w1 = P.l1_scalar;
+          if (P.l1_kind == 1) { w0 = P.l1w[m0]; w1 = has1 ? P.l1w[m1] : 0.f; }
+          const float* wr0 = P.l1_kind == 2 ? P.l1w + ((size_t)m0 * H + h0) * W : nullptr;
+          const float* wr1 = (P.l1_kind == 2 && has1) ? P.l1w + ((size_t)m1 * H + h1) * W : nullptr;
+          const bool ams0 = mk && m0 == 0, ams1 = mk && m1 == 0;
+          const float t0 = thr * w0, t1 = thr * w1;
+          const bool fast = !ams0 && !ams1 && !wr0 && !wr1 && has1;
+          float f[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+          for (int m = 0; m < EM; ++m) {
+            const int k = t + g * m;
+            float y, u, yu1 = 0.f;
+            if (fast) {
+              const float yu0 =
+                  elem(v[m].x * P.invN, ysm[k], usm[k] * uscale, false, 0, t0, &y, &u, f);
+              Y0[k] = y;
+              U0[k] = u;
+              yu1 = elem(-v[m].y * P.invN, ysm[W + k], usm[W + k] * uscale, false, 0, t1, &y, &u, f);
+              Y0[W + k] = y;
+              U0[W + k] = u;
+              v[m] = make_float2(yu0, yu1);
+            } else {
+              const float yu0 = elem(v[m].x * P.invN, ysm[k], usm[k] * uscale, ams0,
+                                     ams0 ? mk[h0 * W + k] : 0, thr * (wr0 ? wr0[k] : w0), &y, &u, f);
+              Y0[k] = y;
+              U0[k] = u;
+              if (has1) {
+                yu1 = elem(-v[m].y * P.invN, ysm[W + k], usm[W + k] * uscale, ams1,
+                           ams1 ? mk[h1 * W + k] : 0, thr * (wr1 ? wr1[k] : w1), &y, &u, f);
+                Y0[W + k] = y;
+                U0[W + k] = u;
+              }
+              v[m] = make_float2(yu0, yu1);
+            }
+          }
+#pragma unroll
+          for (int i = 0; i < 5; ++i) acc[i] += (double)f[i];
+        } else {
+#pragma unroll
+          for (int m = 0; m < EM; ++m) v[m] = make_float2(0.f, 0.f);
+        }
+        ct_first_from_regs<NW, RM, 1>(z, v, t);
+        issue_YU(p + pstride);  // Y/U staging is free again
+        cp_async_commit();
+        fft_ct_passes<NW, RM, ct_threads(NW, RM), 1, 1, NP>(z, P.twW, t);
+        if (valid) {
+          float2* fa = Fi + r0 * Wp;
+          for (int k = t; k < Wf; k += g) {
+            const float2 Zk = z[zs(k)];
+            const float2 Zm = z[zs(k == 0 ? 0 : W - k)];
+            fa[k] = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
+            if (has1) fa[Wp + k] = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
+          }
+        }
+        __syncthreads();
+      }
+    } else
     for (long pb = (long)blockIdx.x * S; pb < npairs; pb += pstride) {
       const long p = pb + s;
       const bool valid = p < npairs;

@@ -262,7 +262,7 @@ def cpu_sample(cfg, D, S, mask, budget_s=15.0):
 def run_ours(args, cfg, rank, world, local_rank):
     import torch
     import sporco_cuda.cbpdn as cb
-    from sporco_cuda import _lib
+    from sporco_cuda import _lib, replicas
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     D, S, mask = synth(cfg, 12345 + args.config, dev)
@@ -318,12 +318,9 @@ def run_ours(args, cfg, rank, world, local_rank):
         barrier()
     ms = ev0.elapsed_time(ev1)
     launches = _lib.sc_launch_count() - n_launch0
-    if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
     iters_per_step = cfg["iters"] * len(cfg["variants"])
-    value = world * iters_per_step * args.steps / (ms / 1e3)
+    value = replicas.job_rate(iters_per_step * args.steps, ms)
+    ms = replicas.max_over_ranks(ms)
 
     # end-to-end through the reference-facing API (numpy host buffers)
     Dn = np.ascontiguousarray(D.permute(1, 2, 0).cpu().numpy())
@@ -350,11 +347,7 @@ def run_ours(args, cfg, rank, world, local_rank):
         e_ms = (time.perf_counter() - t0) * 1e3
     else:
         e_ms = float("nan")
-    if world > 1:
-        t = torch.tensor([e_ms], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e_ms = float(t.item())
-    e_value = world * iters_per_step * e_steps / (e_ms / 1e3)
+    e_value = replicas.job_rate(iters_per_step * e_steps, e_ms)
     h2d = d2h = 0
     for v in cfg["variants"]:
         M = cfg["M"] + (1 if v == "cbpdnmsk" else 0)
@@ -452,7 +445,7 @@ def run_batched(args, cfg, rank, world, local_rank):
     single solves over the same images."""
     import torch
     import sporco_cuda.cbpdn as cb
-    from sporco_cuda import _lib
+    from sporco_cuda import _lib, replicas
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     D, imgs, masks, lam = synth_images(cfg, 12345 + args.config + rank, dev)
@@ -485,14 +478,8 @@ def run_batched(args, cfg, rank, world, local_rank):
         barrier()
     ms = ev0.elapsed_time(ev1)
     launches = _lib.sc_launch_count() - n0
-    if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-        t = torch.tensor([total_it], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t)
-        total_it = int(t.item())
-    value = total_it / (ms / 1e3)
+    value = replicas.job_rate(total_it, ms)
+    ms = replicas.max_over_ranks(ms)
     # loop of single solves over the same images (device inputs)
     Di = torch.cat((torch.zeros((1, cfg["K"], cfg["K"]), device=dev), D), 0)
     Di[0, 0, 0] = 1.0  # the AMS impulse filter, as cbpdnmsk prepends it
@@ -564,7 +551,7 @@ def run_adjoint(args, cfg, rank, world, local_rank):
     import torch
     import sporco_cuda.adjoint as adj
     import sporco_cuda.cbpdn as cb
-    from sporco_cuda import _lib
+    from sporco_cuda import _lib, replicas
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     B = cfg["nimg"]
@@ -616,7 +603,10 @@ def run_adjoint(args, cfg, rank, world, local_rank):
             b_ms += b_
     launches = _lib.sc_launch_count() - n0
     ms = f_ms + b_ms
-    value = world * B * cfg["iters"] * args.steps / (ms / 1e3)
+    value = replicas.job_rate(B * cfg["iters"] * args.steps, ms)
+    f_ms = replicas.max_over_ranks(f_ms)
+    b_ms = replicas.max_over_ranks(b_ms)
+    ms = f_ms + b_ms
     # the fused solver on the same batch, for reference
     ds = cb.prepare_device(D, S, cfg["lmbda"], opt)
     ds.run()

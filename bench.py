@@ -117,6 +117,24 @@ def graded_bytes(H, W, M, images=1):
     return images * (4 * R + (6 if p == 2 else 2) * Cs) + (2 if p == 2 else 1) * Cs
 
 
+def graded_kernel_bytes(H, W, M):
+    """The graded bytes of one image's iteration split by pass: the row pass
+    reads and writes Y, U and the spectra (4R + 2C); the column pass takes
+    the remaining spectrum round trips and the dictionary reads (4C + 2C_D
+    when p = 2, C_D when p = 1)."""
+    R = 4.0 * M * H * W
+    Cs = 8.0 * M * H * (W // 2 + 1)
+    p = 1 if 8 * H * (W // 2 + 1) <= SMEM_MAX else 2
+    return {"row_kernel": 4 * R + 2 * Cs, "col_kernel": (6 * Cs) if p == 2 else Cs}
+
+
+# DRAM bytes per launch and map measured by ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum) for kernels whose traffic grows in proportion to the
+# maps; from the 2048x2048, M=24 capture summarised in
+# profiles/launch_list_2048x2048_m24.md.
+MEASURED_TRAFFIC_PER_MAP = {(2048, 2048): {"row_kernel": (1211e6 + 1149e6) / 24}}
+
+
 def design_bytes(H, W, M, variant="cbpdn", K=None):
     """Per-iteration HBM bytes this design moves for one image.  Row pass:
     reads and writes the spectra F (2C) and Y, U (4R).  Column pass, by
@@ -371,6 +389,24 @@ def run_ours(args, cfg, rank, world, local_rank):
     n_solve_it = cfg["iters"] * args.steps * len(cfg["variants"])
     kern = {k: {"ms_per_launch": a[0] / max(1, a[1]), "launches": a[1],
                 "share": a[0] / it_ms if it_ms else None} for k, a in prof_tot.items()}
+    # the dominant kernel: graded bytes per launch over its mean launch time
+    dom = None
+    if kern:
+        name = max(kern, key=lambda k: kern[k]["ms_per_launch"] * kern[k]["launches"])
+        gb = 0.0
+        for v in cfg["variants"]:
+            M = cfg["M"] + (1 if v == "cbpdnmsk" else 0)
+            gb += graded_kernel_bytes(cfg["H"], cfg["W"], M).get(name, 0.0)
+        gb /= len(cfg["variants"])
+        t = kern[name]["ms_per_launch"]
+        tr = MEASURED_TRAFFIC_PER_MAP.get((cfg["H"], cfg["W"]), {}).get(name)
+        dom = {"name": name, "share": kern[name]["share"],
+               "algorithmic_bytes_per_launch": gb,
+               "achieved": gb / (t / 1e3) / 1e9 if t > 0 and gb > 0 else None,
+               "frac": gb / (t / 1e3) / 1e9 / peak if t > 0 and gb > 0 else None,
+               "traffic": tr * cfg["M"] if tr else None,
+               "traffic_source": "ncu capture at 2048x2048, M=24, scaled by the maps"
+               if tr else None}
     out = None
     if rank == 0:
         cpu = cpu_sample(cfg, D.cpu().numpy(), Sn, Wn) if world == 1 and not args.no_cpu else None
@@ -397,7 +433,8 @@ def run_ours(args, cfg, rank, world, local_rank):
                          "design_bytes_per_iteration": design_it / n_solve_it,
                          "design_frac": (design_it / (it_ms / 1e3) / 1e9 / peak)
                          if it_ms > 0 else None,
-                         "iteration_ms": it_ms / max(1, n_it), "kernels": kern},
+                         "iteration_ms": it_ms / max(1, n_it), "kernels": kern,
+                         "dominant_kernel": dom},
             "cpu_baseline": cpu,
             "gpu_launches": launches,
             "clocks": clk.summary(),

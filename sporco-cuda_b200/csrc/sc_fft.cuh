@@ -401,6 +401,24 @@ __host__ __device__ constexpr int ct_len(int n, int RM, int ST) {
   return ct_swizzled(n, ST) ? n : ct_padded(n, RM);
 }
 
+// Slot of element i0 + q * STRIDE (q < Q, compile-time) from the slot of i0.
+// In the swizzled layout the XOR pattern of an aligned 16-block depends on
+// bits 4..6 of the index only, so a stride that is a multiple of 128 keeps
+// it (slot = slot(i0) + q STRIDE), and a run of Q <= 16 elements inside one
+// aligned 16-block from an i0 that is a multiple of Q keeps it too
+// (slot = slot(i0) ^ q).  Otherwise the slot is computed per element.
+template <int N, int RM, int ST, int STRIDE, int Q>
+struct CtRun {
+  static constexpr bool add = ct_swizzled(N, ST) ? (STRIDE % 128 == 0) : false;
+  static constexpr bool xr = ct_swizzled(N, ST) && STRIDE == 1 && Q <= 16 && 16 % Q == 0;
+  __device__ __forceinline__ static int base(int i0) { return ct_phys<N, RM, ST>(i0); }
+  __device__ __forceinline__ static int at(int s0, int i0, int q) {
+    if constexpr (add) return s0 + q * STRIDE;
+    else if constexpr (xr) return s0 ^ q;
+    else return ct_phys<N, RM, ST>(i0 + q * STRIDE);
+  }
+};
+
 template <int N, int RM, int R, int NS, int G, int ST>
 __device__ __forceinline__ void ct_pass(float2* data, const float2* __restrict__ tw, int t) {
   constexpr int B = N / R;
@@ -411,8 +429,10 @@ __device__ __forceinline__ void ct_pass(float2* data, const float2* __restrict__
   for (int i = 0; i < NB; ++i) {
     const int j = t + i * G;
     if ((B % G) == 0 || j < B) {
+      using LD = CtRun<N, RM, ST, B, R>;
+      const int s0 = LD::base(j);
 #pragma unroll
-      for (int q = 0; q < R; ++q) v[i][q] = data[ct_phys<N, RM, ST>(j + q * B) * ST];
+      for (int q = 0; q < R; ++q) v[i][q] = data[LD::at(s0, j, q) * ST];
       if constexpr (NS > 1) twiddle_r<R>(v[i], tw, (j % NS) * STEP);
       dft_r<R>(v[i]);
     }
@@ -424,8 +444,10 @@ __device__ __forceinline__ void ct_pass(float2* data, const float2* __restrict__
     if ((B % G) == 0 || j < B) {
       const int k = j % NS;
       const int base = (j - k) * R + k;
+      using SD = CtRun<N, RM, ST, NS, R>;
+      const int s0 = SD::base(base);
 #pragma unroll
-      for (int q = 0; q < R; ++q) data[ct_phys<N, RM, ST>(base + q * NS) * ST] = v[i][q];
+      for (int q = 0; q < R; ++q) data[SD::at(s0, base, q) * ST] = v[i][q];
     }
   }
   __syncthreads();
@@ -473,8 +495,10 @@ __device__ __forceinline__ void ct_first_from_regs(float2* data, float2* v, int 
   dft_r<R>(v);  // Ns = 1: no twiddles; butterfly j = t takes t + G q
   __syncthreads();
   const int base = t * R;
+  using SD = CtRun<N, RM, ST, 1, R>;
+  const int s0 = SD::base(base);
 #pragma unroll
-  for (int q = 0; q < R; ++q) data[ct_phys<N, RM, ST>(base + q) * ST] = v[q];
+  for (int q = 0; q < R; ++q) data[SD::at(s0, base, q) * ST] = v[q];
   __syncthreads();
 }
 
@@ -495,8 +519,10 @@ __device__ __forceinline__ void ct_last_to_regs(const float2* data,
   for (int i = 0; i < NB; ++i) {
     const int j = t + i * G;
     float2 u[R];
+    using LD = CtRun<N, RM, ST, NS, R>;
+    const int s0 = LD::base(j);
 #pragma unroll
-    for (int q = 0; q < R; ++q) u[q] = data[ct_phys<N, RM, ST>(j + q * NS) * ST];
+    for (int q = 0; q < R; ++q) u[q] = data[LD::at(s0, j, q) * ST];
     twiddle_r<R>(u, tw, (j % NS) * STEP);
     dft_r<R>(u);
 #pragma unroll

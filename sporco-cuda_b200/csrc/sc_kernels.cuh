@@ -723,8 +723,9 @@ col_kernel(ColParams P) {
 #pragma unroll
         for (int j = 0; j < NW; ++j)
           w[j] = (j < KMAX - Kr) ? make_float2(0.f, 0.f) : cur[rslot(j - (KMAX - 1)) * T + cc];
+        // last tap first: it uses the window values that were loaded first
 #pragma unroll
-        for (int tp = 0; tp < KMAX; ++tp) {
+        for (int tp = KMAX - 1; tp >= 0; --tp) {
           if (tp < Kr) {
             const float2 e = ecur[tp * T + cc];
 #pragma unroll

@@ -24,7 +24,8 @@ __host__ __device__ constexpr int col_radix(int H) { return H >= 512 ? 16 : 8; }
 
 // Per-image ADMM scalar state, kept on the device for the whole solve.
 struct ImgState {
-  double rho;    // rho used by the next iteration
+  double rho;      // rho used by the next iteration
+  double rho_prev; // rho of the last iteration (its Y: shrinkage of V at lambda / rho_prev)
   double rsf;    // scale factor chosen by the last adaptive-rho step (1: none)
   double uscale; // the next row pass reads U scaled by this (1 / rsf)
   double r, s;   // last residuals (normalised unless StdResiduals)
@@ -64,7 +65,8 @@ struct RowParams {
   int nblk;                // CTAs per image (grid.x)
   float2* F;               // (B, M, H, Wp) spectra
   float* Y;                // (B, M, H, W)
-  float* U;                // (B, M, H, W)
+  float* U;                // (B, M, H, W): U, or V = Y + U for ROW_ITER
+  int vstate;              // ROW_FIXUP: P.U holds V (1) or U (0)
   float* Yo;               // ROW_ITER writes Y here (== Y unless a trace is kept)
   // epilogue
   const float* lam;        // (B,)
@@ -115,7 +117,9 @@ struct ColParams {
 enum RowMode {
   ROW_ITER = 0, ROW_FWD_REAL = 1, ROW_FWD_DICT = 2, ROW_INV_REAL = 3, ROW_FIXUP = 4,
   ROW_FWD_YU = 5, // row spectra of Y - U (start from given iterates)
-  ROW_ADJ = 6     // adjoint step: Q = row IFFT, gV update, row FFT of relax * gV
+  ROW_ADJ = 6,    // adjoint step: Q = row IFFT, gV update, row FFT of relax * gV
+  ROW_ITER_YU = 7 // ROW_ITER with Y and U stored separately (warm starts, the
+                  // adjoint's recomputation, which keeps Y of every step)
 };
 // COL_SOLVE: all maps share d (cbpdn, or cbpdngrd with one GradWeight), so
 // sum_m |Df_m|^2 / d comes from the precomputed Psum; COL_SOLVE_W: per-map
@@ -153,7 +157,7 @@ __host__ __device__ inline size_t sc_align16(size_t x) { return (x + 15) & ~(siz
 // rho fix-up the pair's U rows and spectrum rows.
 __host__ __device__ inline size_t row_slot_bytes(int mode, int zlen, int W, int Wp) {
   size_t z = sc_align16((size_t)zlen * 8);
-  if (mode != ROW_ITER && mode != ROW_ADJ && mode != ROW_FIXUP) return z;
+  if (mode != ROW_ITER && mode != ROW_ITER_YU && mode != ROW_ADJ && mode != ROW_FIXUP) return z;
   return z + (size_t)(2 * Wp) * 8 + 2 * sc_align16((size_t)(2 * W) * 4);
 }
 

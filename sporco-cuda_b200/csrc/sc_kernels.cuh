@@ -113,6 +113,67 @@ __device__ __forceinline__ float2 pack_inverse(const float2* a, const float2* bb
   return make_float2(A.x + Bv.y, -(Bv.x - A.y));
 }
 
+// Threshold weight of one image row: scalar w, or the row wr of a full
+// weight array; mrow: the AMS mask row when the row belongs to map 0 of a
+// masked problem.
+struct RowW {
+  float w;
+  const float* wr;
+  const int32_t* mrow;
+};
+
+// Y of the shrinkage step at element k of a row: the AMS step (1 - mask) v
+// on map 0 of masked problems, else the soft threshold at th times the
+// row's weight (cbpdn_kernels.cu:129-311, 1137-1155).
+__device__ __forceinline__ float shrink_y(float v, float th, const RowW& r, int k) {
+  return r.mrow ? (float)(1 - r.mrow[k]) * v : soft_threshold(v, th * (r.wr ? r.wr[k] : r.w));
+}
+
+// Per-launch constants of the iteration's element-wise step.
+struct IterC {
+  float a, a1;   // RelaxParam, 1 - RelaxParam
+  bool relax;    // RelaxParam != 1
+  float uscale;  // the stored U is read scaled by this (1/rsf after a rho change)
+};
+
+// One element of the iteration's element-wise step: over-relaxation,
+// shrinkage, dual update, residual partial sums (single precision within a
+// row pair).  VS: the stored state is V = Y + U of the previous iteration
+// (s0), whose Y is recomputed as its shrinkage at the previous threshold
+// tq; else s0, s1 are Y and U.  FAST: scalar thresholds tc, tq (weights
+// applied), no AMS row.  Writes V (VS) or Y and U; returns y - u.
+template <bool VS, bool FAST>
+__device__ __forceinline__ float iter_elem(float x, float s0, float s1, const RowW& r, int k,
+                                           float tc, float tq, const IterC& c, float* f,
+                                           float* o0, float* o1) {
+  float yo, uo;
+  if constexpr (VS) {
+    // before the first iteration V = 0 and tq = 0, so yo = uo = 0
+    yo = FAST ? soft_threshold(s0, tq) : shrink_y(s0, tq, r, k);
+    uo = (s0 - yo) * c.uscale;
+  } else {
+    yo = s0;
+    uo = s1 * c.uscale;
+  }
+  const float xr = c.relax ? c.a * x + c.a1 * yo : x;
+  const float v = xr + uo;
+  const float y = FAST ? soft_threshold(v, tc) : shrink_y(v, tc, r, k);
+  const float u = v - y;
+  if constexpr (VS) {
+    *o0 = v;
+  } else {
+    *o0 = y;
+    *o1 = u;
+  }
+  const float dxy = x - y, dyy = yo - y;
+  f[0] += x * x;
+  f[1] += y * y;
+  f[2] += u * u;
+  f[3] += dxy * dxy;
+  f[4] += dyy * dyy;
+  return y - u;
+}
+
 // ============================================================== row pass ==
 // NW > 0: row length W known at compile time (specialised FFT plan);
 // NW == 0: any W (runtime FFT plan).
@@ -135,18 +196,24 @@ row_kernel(RowParams P) {
   float2* z = reinterpret_cast<float2*>(slot);
   auto zs = [](int k) { return fft_slot<NW, RM, 1>(k); };
 
-  float thr = 0.f, rsf_c = 0.f, uscale = 1.f, rho = 0.f;
-  if constexpr (MODE == ROW_ITER || MODE == ROW_FIXUP || MODE == ROW_ADJ) {
+  // thr: lambda / rho of this iteration; thr_prev: of the iteration that
+  // produced the stored state (the same float value that iteration used)
+  float thr = 0.f, thr_prev = 0.f, rsf_c = 0.f, uscale = 1.f, rho = 0.f;
+  if constexpr (MODE == ROW_ITER || MODE == ROW_ITER_YU || MODE == ROW_FIXUP ||
+                MODE == ROW_ADJ) {
     const ImgState& st = P.st[b];
     if (st.done) return;
-    if constexpr (MODE == ROW_ITER) {
+    if constexpr (MODE == ROW_ITER || MODE == ROW_ITER_YU) {
       thr = (float)((double)P.lam[b] / st.rho);
+      // no iteration yet: V = 0 and a zero threshold give Y = U = 0
+      thr_prev = st.k == 0 ? 0.f : (float)((double)P.lam[b] / st.rho_prev);
       uscale = (float)st.uscale;
     } else if constexpr (MODE == ROW_ADJ) {
       rho = (float)st.rho;
     } else {
       if (st.rsf == 1.0) return;
       rsf_c = (float)(1.0 - 1.0 / st.rsf);
+      thr_prev = (float)((double)P.lam[b] / st.rho_prev);
     }
   }
 
@@ -157,16 +224,33 @@ row_kernel(RowParams P) {
   float2* Fi = P.F + (size_t)b * img_spec;
   const long pstride = (long)gridDim.x * S;
 
-  if constexpr (MODE == ROW_ITER || MODE == ROW_ADJ || MODE == ROW_FIXUP) {
+  if constexpr (MODE == ROW_ITER || MODE == ROW_ITER_YU || MODE == ROW_ADJ ||
+                MODE == ROW_FIXUP) {
     // ------------------------------- iteration / adjoint step / rho fix-up
     constexpr bool ADJ = MODE == ROW_ADJ;
+    // ROW_ITER keeps the ADMM state as V = Y + U (one array, P.U): Y of an
+    // iteration is the shrinkage of V, U = V - Y.  ROW_ITER_YU keeps Y and U.
+    constexpr bool VS = MODE == ROW_ITER;
+    constexpr bool TWO = MODE == ROW_ITER_YU || ADJ;  // two staged real arrays
     float2* fst = reinterpret_cast<float2*>(slot + sc_align16((size_t)zlen * 8));
     float* ysm = reinterpret_cast<float*>(fst + 2 * (size_t)Wp);
     float* usm = ysm + sc_align16((size_t)(2 * W) * 4) / 4;
-    // staged per row pair: Y and U (iteration), gV and the mask source (adjoint)
-    const float* Yi = (ADJ ? P.gV : P.Y) + (size_t)b * img_real;
+    // staged per row pair: V (iteration), Y and U (iteration from Y, U), gV
+    // and the mask source (adjoint), the state array (fix-up, into usm)
+    const float* Yi = (ADJ ? P.gV : VS ? P.U : P.Y) + (size_t)b * img_real;
     const float* Ui = (ADJ ? P.Ymask : P.U) + (size_t)b * img_real;
     const bool vec = (W & 3) == 0;
+    const int32_t* mk = P.mask ? P.mask + (size_t)b * H * W : nullptr;
+    // threshold weights and AMS mask row of image row r of this image
+    auto roww = [&](long r, bool ok) -> RowW {
+      RowW o{P.l1_scalar, nullptr, nullptr};
+      if (!ok) return o;
+      const int m = (int)(r / H), h = (int)(r - (long)m * H);
+      if (P.l1_kind == 1) o.w = P.l1w[m];
+      if (P.l1_kind == 2) o.wr = P.l1w + ((size_t)m * H + h) * W;
+      if (mk && m == 0) o.mrow = mk + (size_t)h * W;
+      return o;
+    };
 
     auto issue_F = [&](long p) {
       if (p < npairs) {
@@ -184,12 +268,12 @@ row_kernel(RowParams P) {
         if (vec) {
           for (int q = t; q < n / 4; q += g) {
             cp_async16(ysm + 4 * q, ys + 4 * q);
-            cp_async16(usm + 4 * q, us + 4 * q);
+            if constexpr (TWO) cp_async16(usm + 4 * q, us + 4 * q);
           }
         } else {
           for (int q = t; q < n; q += g) {
             cp_async4(ysm + q, ys + q);
-            cp_async4(usm + q, us + q);
+            if constexpr (TWO) cp_async4(usm + q, us + q);
           }
         }
       }
@@ -197,8 +281,10 @@ row_kernel(RowParams P) {
 
     if constexpr (MODE == ROW_FIXUP) {
       // F += (1 - 1/rsf) rowFFT(U) after a change of rho (U is rescaled by
-      // 1/rsf when the next row pass reads it).  U rows are staged one pair
-      // ahead (during the transform), F rows during the next pair's packing.
+      // 1/rsf when the next row pass reads it).  The state rows (U, or V with
+      // U = V - Y) are staged one pair ahead (during the transform), F rows
+      // during the next pair's packing.
+      const bool vstate = P.vstate != 0;
       auto issue_U = [&](long p) {
         if (p < npairs) {
           const int n = ((2 * p + 1 < rows) ? 2 : 1) * W;
@@ -221,7 +307,25 @@ row_kernel(RowParams P) {
         cp_async_wait<0>();  // U(p), F(p)
         __syncthreads();
         if (valid) {
-          for (int k = t; k < W; k += g) z[zs(k)] = make_float2(usm[k], has1 ? usm[W + k] : 0.f);
+          if (vstate) {
+            const RowW w0 = roww(2 * p, true), w1 = roww(2 * p + 1, has1);
+            if (!w0.mrow && !w1.mrow && !w0.wr && !w1.wr) {
+              const float t0 = thr_prev * w0.w, t1 = thr_prev * w1.w;
+              for (int k = t; k < W; k += g) {
+                const float v0 = usm[k], v1 = has1 ? usm[W + k] : 0.f;
+                z[zs(k)] = make_float2(v0 - soft_threshold(v0, t0), v1 - soft_threshold(v1, t1));
+              }
+            } else {
+              for (int k = t; k < W; k += g) {
+                const float v0 = usm[k], v1 = has1 ? usm[W + k] : 0.f;
+                z[zs(k)] = make_float2(v0 - shrink_y(v0, thr_prev, w0, k),
+                                       has1 ? v1 - shrink_y(v1, thr_prev, w1, k) : 0.f);
+              }
+            }
+          } else {
+            for (int k = t; k < W; k += g)
+              z[zs(k)] = make_float2(usm[k], has1 ? usm[W + k] : 0.f);
+          }
         }
         __syncthreads();
         issue_U(p + pstride);
@@ -251,26 +355,38 @@ row_kernel(RowParams P) {
     }
 
     double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    const int32_t* mk = P.mask ? P.mask + (size_t)b * H * W : nullptr;
-    const float a = P.relax, a1 = 1.f - P.relax;
-    const bool relax = P.relax != 1.f;
-    // one element of the epilogue: returns y - u, accumulates the residual
-    // partial sums in f[] (single precision within a row pair)
-    auto elem = [&](float x, float yo, float uo, bool ams, int mval, float tw, float* y_out,
-                    float* u_out, float* f) -> float {
-      const float xr = relax ? a * x + a1 * yo : x;
-      const float v = xr + uo;
-      const float y = ams ? (float)(1 - mval) * v : soft_threshold(v, tw);
-      const float u = v - y;
-      *y_out = y;
-      *u_out = u;
-      const float dxy = x - y, dyy = yo - y;
-      f[0] += x * x;
-      f[1] += y * y;
-      f[2] += u * u;
-      f[3] += dxy * dxy;
-      f[4] += dyy * dyy;
-      return y - u;
+    IterC ic;
+    ic.a = P.relax;
+    ic.a1 = 1.f - P.relax;
+    ic.relax = P.relax != 1.f;
+    ic.uscale = uscale;
+    // State rows of the pair (V, or Y and U) are written here.
+    auto out0 = [&](long r0) -> float* {
+      return (VS ? P.U : P.Yo) + (size_t)b * img_real + (size_t)r0 * W;
+    };
+    auto outu = [&](long r0) -> float* { return P.U + (size_t)b * img_real + (size_t)r0 * W; };
+    // The element-wise step of the iteration on the pair element k (both
+    // rows): x from the inverse transform zz; returns the packed y - u.
+    // fast: both rows present, scalar thresholds, no AMS row.
+    // fast: both rows present, scalar thresholds (tc*, tq*), no AMS row
+    auto elem_fast = [&](float tc0, float tc1, float tq0, float tq1, int k, float2 zz,
+                         float* O0, float* Q0, float* f) -> float2 {
+      const RowW w{};
+      const float yu0 = iter_elem<VS, true>(zz.x * P.invN, ysm[k], TWO ? usm[k] : 0.f, w, k,
+                                            tc0, tq0, ic, f, O0 + k, Q0 + k);
+      const float yu1 = iter_elem<VS, true>(-zz.y * P.invN, ysm[W + k], TWO ? usm[W + k] : 0.f,
+                                            w, k, tc1, tq1, ic, f, O0 + W + k, Q0 + W + k);
+      return make_float2(yu0, yu1);
+    };
+    auto elem_gen = [&](const RowW& w0, const RowW& w1, bool has1, int k, float2 zz, float* O0,
+                        float* Q0, float* f) -> float2 {
+      float yu1 = 0.f;
+      const float yu0 = iter_elem<VS, false>(zz.x * P.invN, ysm[k], TWO ? usm[k] : 0.f, w0, k,
+                                             thr, thr_prev, ic, f, O0 + k, Q0 + k);
+      if (has1)
+        yu1 = iter_elem<VS, false>(-zz.y * P.invN, ysm[W + k], TWO ? usm[W + k] : 0.f, w1, k,
+                                   thr, thr_prev, ic, f, O0 + W + k, Q0 + W + k);
+      return make_float2(yu0, yu1);
     };
 
     long p0 = (long)blockIdx.x * S + s;
@@ -300,71 +416,47 @@ row_kernel(RowParams P) {
         issue_F(p + pstride);  // the staged rows are consumed
         cp_async_commit();
         fft_ct_passes<NW, RM, ct_threads(NW, RM), 1, 1, NP - 1>(z, P.twW, t);
-        cp_async_wait<1>();  // Y(p), U(p)
+        cp_async_wait<1>();  // the pair's state rows
         __syncthreads();
         ct_last_to_regs<NW, RM, 1>(z, P.twW, v, t);
         if (ADJ && valid) {
           float* gv = P.gV + (size_t)b * img_real + (size_t)r0 * W;
-          const bool first = P.first != 0;
+          const bool firstq = P.first != 0;
 #pragma unroll
           for (int m = 0; m < EM; ++m) {
             const int k = t + g * m;
-            const float q0 = first ? 0.f : v[m].x * P.invN;
-            const float q1 = first ? 0.f : -v[m].y * P.invN;
+            const float q0 = firstq ? 0.f : v[m].x * P.invN;
+            const float q1 = firstq ? 0.f : -v[m].y * P.invN;
             const float v0 = ysm[k];
-            const float gy0 = first ? v0 : a1 * v0 + rho * q0;
-            const float gu0 = first ? 0.f : v0 - rho * q0;
+            const float gy0 = firstq ? v0 : ic.a1 * v0 + rho * q0;
+            const float gu0 = firstq ? 0.f : v0 - rho * q0;
             const float n0 = usm[k] != 0.f ? gy0 : gu0;
             gv[k] = n0;
             float n1 = 0.f;
             if (has1) {
               const float v1 = ysm[W + k];
-              const float gy1 = first ? v1 : a1 * v1 + rho * q1;
-              const float gu1 = first ? 0.f : v1 - rho * q1;
+              const float gy1 = firstq ? v1 : ic.a1 * v1 + rho * q1;
+              const float gu1 = firstq ? 0.f : v1 - rho * q1;
               n1 = usm[W + k] != 0.f ? gy1 : gu1;
               gv[W + k] = n1;
             }
-            v[m] = make_float2(a * n0, a * n1);
+            v[m] = make_float2(ic.a * n0, ic.a * n1);
           }
-        } else if (valid) {
-          const int m0 = (int)(r0 / H), h0 = (int)(r0 - (long)m0 * H);
-          const int m1 = (int)(r1 / H), h1 = (int)(r1 - (long)m1 * H);
-          float* Y0 = P.Yo + (size_t)b * img_real + (size_t)r0 * W;
-          float* U0 = P.U + (size_t)b * img_real + (size_t)r0 * W;
-          float w0 = P.l1_scalar, w1 = P.l1_scalar;
-          if (P.l1_kind == 1) { w0 = P.l1w[m0]; w1 = has1 ? P.l1w[m1] : 0.f; }
-          const float* wr0 = P.l1_kind == 2 ? P.l1w + ((size_t)m0 * H + h0) * W : nullptr;
-          const float* wr1 = (P.l1_kind == 2 && has1) ? P.l1w + ((size_t)m1 * H + h1) * W : nullptr;
-          const bool ams0 = mk && m0 == 0, ams1 = mk && m1 == 0;
-          const float t0 = thr * w0, t1 = thr * w1;
-          const bool fast = !ams0 && !ams1 && !wr0 && !wr1 && has1;
+        } else if (!ADJ && valid) {
+          const RowW w0 = roww(r0, true), w1 = roww(r1, has1);
+          const bool fast = has1 && !w0.mrow && !w1.mrow && !w0.wr && !w1.wr;
+          const float tc0 = thr * w0.w, tc1 = thr * w1.w;
+          const float tq0 = thr_prev * w0.w, tq1 = thr_prev * w1.w;
+          float* O0 = out0(r0);
+          float* Q0 = outu(r0);
           float f[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+          if (fast) {
 #pragma unroll
-          for (int m = 0; m < EM; ++m) {
-            const int k = t + g * m;
-            float y, u, yu1 = 0.f;
-            if (fast) {
-              const float yu0 =
-                  elem(v[m].x * P.invN, ysm[k], usm[k] * uscale, false, 0, t0, &y, &u, f);
-              Y0[k] = y;
-              U0[k] = u;
-              yu1 = elem(-v[m].y * P.invN, ysm[W + k], usm[W + k] * uscale, false, 0, t1, &y, &u, f);
-              Y0[W + k] = y;
-              U0[W + k] = u;
-              v[m] = make_float2(yu0, yu1);
-            } else {
-              const float yu0 = elem(v[m].x * P.invN, ysm[k], usm[k] * uscale, ams0,
-                                     ams0 ? mk[h0 * W + k] : 0, thr * (wr0 ? wr0[k] : w0), &y, &u, f);
-              Y0[k] = y;
-              U0[k] = u;
-              if (has1) {
-                yu1 = elem(-v[m].y * P.invN, ysm[W + k], usm[W + k] * uscale, ams1,
-                           ams1 ? mk[h1 * W + k] : 0, thr * (wr1 ? wr1[k] : w1), &y, &u, f);
-                Y0[W + k] = y;
-                U0[W + k] = u;
-              }
-              v[m] = make_float2(yu0, yu1);
-            }
+            for (int m = 0; m < EM; ++m)
+              v[m] = elem_fast(tc0, tc1, tq0, tq1, t + g * m, v[m], O0, Q0, f);
+          } else {
+#pragma unroll
+            for (int m = 0; m < EM; ++m) v[m] = elem_gen(w0, w1, has1, t + g * m, v[m], O0, Q0, f);
           }
 #pragma unroll
           for (int i = 0; i < 5; ++i) acc[i] += (double)f[i];
@@ -373,7 +465,7 @@ row_kernel(RowParams P) {
           for (int m = 0; m < EM; ++m) v[m] = make_float2(0.f, 0.f);
         }
         ct_first_from_regs<NW, RM, 1>(z, v, t);
-        issue_YU(p + pstride);  // Y/U staging is free again
+        issue_YU(p + pstride);  // the state staging is free again
         cp_async_commit();
         fft_ct_passes<NW, RM, ct_threads(NW, RM), 1, 1, NP>(z, P.twW, t);
         if (valid) {
@@ -387,109 +479,81 @@ row_kernel(RowParams P) {
         }
         __syncthreads();
       }
-    } else
-    for (long pb = (long)blockIdx.x * S; pb < npairs; pb += pstride) {
-      const long p = pb + s;
-      const bool valid = p < npairs;
-      const long r0 = 2 * p, r1 = 2 * p + 1;
-      const bool has1 = valid && (r1 < rows);
-      cp_async_wait<1>();  // F(p)
-      __syncthreads();
-      if (valid) {
-        for (int k = t; k < W; k += g) z[zs(k)] = pack_inverse(fst, fst + Wp, has1, k, W, Wf);
-      }
-      __syncthreads();
-      issue_F(p + pstride);  // lands during this pair's transforms
-      cp_async_commit();
-      fft_any<NW, 1, RM>(z, P.pw, P.twW, t, g);
-      cp_async_wait<1>();  // Y(p), U(p)
-      __syncthreads();
-      if (ADJ && valid) {
-        // Q = IFFT(Q^) (zero before the first step); gradients w.r.t. Y and U
-        // of this step, gY = (1 - a) gV + rho Q, gU = gV - rho Q; gV of the
-        // step before: gY where its shrinkage was active (Y != 0), else gU.
-        float* gv = P.gV + (size_t)b * img_real + (size_t)r0 * W;
-        const bool first = P.first != 0;
-        for (int k = t; k < W; k += g) {
-          const float2 zz = z[zs(k)];
-          const float q0 = first ? 0.f : zz.x * P.invN;
-          const float q1 = first ? 0.f : -zz.y * P.invN;
-          const float v0 = ysm[k];
-          const float gy0 = first ? v0 : a1 * v0 + rho * q0;
-          const float gu0 = first ? 0.f : v0 - rho * q0;
-          const float n0 = usm[k] != 0.f ? gy0 : gu0;
-          gv[k] = n0;
-          float n1 = 0.f;
-          if (has1) {
-            const float v1 = ysm[W + k];
-            const float gy1 = first ? v1 : a1 * v1 + rho * q1;
-            const float gu1 = first ? 0.f : v1 - rho * q1;
-            n1 = usm[W + k] != 0.f ? gy1 : gu1;
-            gv[W + k] = n1;
-          }
-          z[zs(k)] = make_float2(a * n0, a * n1);
+    } else {
+      for (long pb = (long)blockIdx.x * S; pb < npairs; pb += pstride) {
+        const long p = pb + s;
+        const bool valid = p < npairs;
+        const long r0 = 2 * p, r1 = 2 * p + 1;
+        const bool has1 = valid && (r1 < rows);
+        cp_async_wait<1>();  // F(p)
+        __syncthreads();
+        if (valid) {
+          for (int k = t; k < W; k += g) z[zs(k)] = pack_inverse(fst, fst + Wp, has1, k, W, Wf);
         }
-      } else if (valid) {
-        const int m0 = (int)(r0 / H), h0 = (int)(r0 - (long)m0 * H);
-        const int m1 = (int)(r1 / H), h1 = (int)(r1 - (long)m1 * H);
-        float* Y0 = P.Yo + (size_t)b * img_real + (size_t)r0 * W;
-        float* U0 = P.U + (size_t)b * img_real + (size_t)r0 * W;
-        float w0 = P.l1_scalar, w1 = P.l1_scalar;
-        if (P.l1_kind == 1) { w0 = P.l1w[m0]; w1 = has1 ? P.l1w[m1] : 0.f; }
-        const float* wr0 = P.l1_kind == 2 ? P.l1w + ((size_t)m0 * H + h0) * W : nullptr;
-        const float* wr1 = (P.l1_kind == 2 && has1) ? P.l1w + ((size_t)m1 * H + h1) * W : nullptr;
-        const bool ams0 = mk && m0 == 0, ams1 = mk && m1 == 0;
-        const float t0 = thr * w0, t1 = thr * w1;
-        float f[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-        if (!ams0 && !ams1 && !wr0 && !wr1 && has1) {
-          // common case: two rows, scalar thresholds
+        __syncthreads();
+        issue_F(p + pstride);  // lands during this pair's transforms
+        cp_async_commit();
+        fft_any<NW, 1, RM>(z, P.pw, P.twW, t, g);
+        cp_async_wait<1>();  // the pair's state rows
+        __syncthreads();
+        if (ADJ && valid) {
+          // Q = IFFT(Q^) (zero before the first step); gradients w.r.t. Y and U
+          // of this step, gY = (1 - a) gV + rho Q, gU = gV - rho Q; gV of the
+          // step before: gY where its shrinkage was active (Y != 0), else gU.
+          float* gv = P.gV + (size_t)b * img_real + (size_t)r0 * W;
+          const bool firstq = P.first != 0;
           for (int k = t; k < W; k += g) {
             const float2 zz = z[zs(k)];
-            float y, u;
-            const float yu0 = elem(zz.x * P.invN, ysm[k], usm[k] * uscale, false, 0, t0, &y, &u, f);
-            Y0[k] = y;
-            U0[k] = u;
-            const float yu1 =
-                elem(-zz.y * P.invN, ysm[W + k], usm[W + k] * uscale, false, 0, t1, &y, &u, f);
-            Y0[W + k] = y;
-            U0[W + k] = u;
-            z[zs(k)] = make_float2(yu0, yu1);
-          }
-        } else {
-          for (int k = t; k < W; k += g) {
-            const float2 zz = z[zs(k)];
-            float y, u, yu1 = 0.f;
-            const float yu0 = elem(zz.x * P.invN, ysm[k], usm[k] * uscale, ams0,
-                                   ams0 ? mk[h0 * W + k] : 0, thr * (wr0 ? wr0[k] : w0), &y, &u, f);
-            Y0[k] = y;
-            U0[k] = u;
+            const float q0 = firstq ? 0.f : zz.x * P.invN;
+            const float q1 = firstq ? 0.f : -zz.y * P.invN;
+            const float v0 = ysm[k];
+            const float gy0 = firstq ? v0 : ic.a1 * v0 + rho * q0;
+            const float gu0 = firstq ? 0.f : v0 - rho * q0;
+            const float n0 = usm[k] != 0.f ? gy0 : gu0;
+            gv[k] = n0;
+            float n1 = 0.f;
             if (has1) {
-              yu1 = elem(-zz.y * P.invN, ysm[W + k], usm[W + k] * uscale, ams1,
-                         ams1 ? mk[h1 * W + k] : 0, thr * (wr1 ? wr1[k] : w1), &y, &u, f);
-              Y0[W + k] = y;
-              U0[W + k] = u;
+              const float v1 = ysm[W + k];
+              const float gy1 = firstq ? v1 : ic.a1 * v1 + rho * q1;
+              const float gu1 = firstq ? 0.f : v1 - rho * q1;
+              n1 = usm[W + k] != 0.f ? gy1 : gu1;
+              gv[W + k] = n1;
             }
-            z[zs(k)] = make_float2(yu0, yu1);
+            z[zs(k)] = make_float2(ic.a * n0, ic.a * n1);
+          }
+        } else if (!ADJ && valid) {
+          const RowW w0 = roww(r0, true), w1 = roww(r1, has1);
+          const bool fast = has1 && !w0.mrow && !w1.mrow && !w0.wr && !w1.wr;
+          const float tc0 = thr * w0.w, tc1 = thr * w1.w;
+          const float tq0 = thr_prev * w0.w, tq1 = thr_prev * w1.w;
+          float* O0 = out0(r0);
+          float* Q0 = outu(r0);
+          float f[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+          if (fast) {
+            for (int k = t; k < W; k += g)
+              z[zs(k)] = elem_fast(tc0, tc1, tq0, tq1, k, z[zs(k)], O0, Q0, f);
+          } else {
+            for (int k = t; k < W; k += g) z[zs(k)] = elem_gen(w0, w1, has1, k, z[zs(k)], O0, Q0, f);
+          }
+#pragma unroll
+          for (int i = 0; i < 5; ++i) acc[i] += (double)f[i];
+        }
+        __syncthreads();
+        issue_YU(p + pstride);  // the state staging is free again
+        cp_async_commit();
+        fft_any<NW, 1, RM>(z, P.pw, P.twW, t, g);
+        if (valid) {
+          float2* fa = Fi + r0 * Wp;
+          for (int k = t; k < Wf; k += g) {
+            const float2 Zk = z[zs(k)];
+            const float2 Zm = z[zs(k == 0 ? 0 : W - k)];
+            // A = (Z_k + conj Z_{-k}) / 2 ;  B = (Z_k - conj Z_{-k}) / (2i)
+            fa[k] = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
+            if (has1) fa[Wp + k] = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
           }
         }
-#pragma unroll
-        for (int i = 0; i < 5; ++i) acc[i] += (double)f[i];
+        __syncthreads();
       }
-      __syncthreads();
-      issue_YU(p + pstride);  // Y/U staging is free again
-      cp_async_commit();
-      fft_any<NW, 1, RM>(z, P.pw, P.twW, t, g);
-      if (valid) {
-        float2* fa = Fi + r0 * Wp;
-        for (int k = t; k < Wf; k += g) {
-          const float2 Zk = z[zs(k)];
-          const float2 Zm = z[zs(k == 0 ? 0 : W - k)];
-          // A = (Z_k + conj Z_{-k}) / 2 ;  B = (Z_k - conj Z_{-k}) / (2i)
-          fa[k] = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
-          if (has1) fa[Wp + k] = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
-        }
-      }
-      __syncthreads();
     }
     cp_async_wait<0>();
     if constexpr (ADJ) return;
@@ -501,7 +565,7 @@ row_kernel(RowParams P) {
     }
     return;
   } else {
-    // ------------------------------------- setup, tool and fix-up modes
+    // ---------------------------------------------- setup and tool modes
     for (long pb = (long)blockIdx.x * S; pb < npairs; pb += pstride) {
       const long p = pb + s;
       const bool valid = p < npairs;
@@ -1474,6 +1538,7 @@ __global__ void finalize_kernel(const double* __restrict__ partials, int nblk,
   }
   S.nX = nX; S.nY = nY; S.nU = nU;
   S.r = r; S.s = s; S.epri = epri; S.edua = edua;
+  S.rho_prev = rho;
   S.rho = rsf * rho;
   S.rsf = rsf;
   // U as stored is the U of this iteration; the next row pass reads it scaled
@@ -1497,6 +1562,7 @@ __global__ void init_state_kernel(ImgState* st, const float* rho0, int B, int* n
   if (b >= B) return;
   ImgState s;
   s.rho = (double)rho0[b];
+  s.rho_prev = s.rho;
   s.rsf = 1.0;
   s.uscale = 1.0;
   s.r = s.s = s.epri = s.edua = 0.0;
@@ -1518,6 +1584,42 @@ __global__ void twiddle_kernel(float2* tw, int n) {
 }
 
 // out = U scaled to the value the next iteration would read (U * uscale).
+// Y and U from the state V = Y + U (row_kernel<ROW_ITER>), at the end of a
+// solve or at a checkpoint: Y = shrinkage of V at lambda / rho_prev (what the
+// last iteration computed), U = (V - Y) scaled by uscale; both zero before
+// the first iteration.  Grid (blocks, B); U may be NULL.
+__global__ void state_yu_kernel(const float* __restrict__ V, float* __restrict__ Y,
+                                float* __restrict__ U, const ImgState* __restrict__ st,
+                                const float* __restrict__ lam, int M, int H, int W, int l1_kind,
+                                float l1_scalar, const float* __restrict__ l1w,
+                                const int32_t* __restrict__ mask) {
+  const int b = blockIdx.y;
+  const ImgState& S = st[b];
+  const bool first = S.k == 0;
+  const float thr = (float)((double)lam[b] / S.rho_prev);
+  const float us = (float)S.uscale;
+  const size_t plane = (size_t)H * W, n = (size_t)M * plane;
+  const size_t off = (size_t)b * n;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int m = (int)(i / plane);
+    const size_t hw = i - (size_t)m * plane;
+    const float v = V[off + i];
+    float y = 0.f, u = 0.f;
+    if (!first) {
+      if (mask && m == 0) {
+        y = (float)(1 - mask[(size_t)b * plane + hw]) * v;
+      } else {
+        const float w = l1_kind == 1 ? l1w[m] : l1_kind == 2 ? l1w[i] : l1_scalar;
+        y = soft_threshold(v, thr * w);
+      }
+      u = (v - y) * us;
+    }
+    Y[off + i] = y;
+    if (U) U[off + i] = u;
+  }
+}
+
 __global__ void export_u_kernel(const float* __restrict__ U, float* __restrict__ out,
                                 const ImgState* __restrict__ st, size_t per_img, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;

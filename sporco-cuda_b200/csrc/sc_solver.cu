@@ -240,7 +240,8 @@ typedef void (*ColFn)(ColParams);
 // plan.
 template <int MODE>
 constexpr bool row_specialised() {
-  return MODE == ROW_ITER || MODE == ROW_FIXUP || MODE == ROW_FWD_REAL || MODE == ROW_INV_REAL ||
+  return MODE == ROW_ITER || MODE == ROW_ITER_YU || MODE == ROW_FIXUP || MODE == ROW_FWD_REAL ||
+         MODE == ROW_INV_REAL ||
          MODE == ROW_ADJ;
 }
 
@@ -290,7 +291,8 @@ static int launch_row(const Plan& pl, RowParams rp, int B, cudaStream_t s, int n
   rp.gsz = hot ? pl.row_g : pl.rowg_g;
   rp.nblk = nblk > 0 ? nblk : pl.row_nblk;
   dim3 grid(rp.nblk, B);
-  const size_t smem = (MODE == ROW_ITER || MODE == ROW_ADJ || MODE == ROW_FIXUP) ? pl.row_smem
+  const size_t smem = (MODE == ROW_ITER || MODE == ROW_ITER_YU || MODE == ROW_ADJ ||
+                       MODE == ROW_FIXUP) ? pl.row_smem
                       : hot ? pl.row_smem_tool : pl.rowg_smem;
   // one slot (row pair in flight) per rp.gsz threads
   const int threads = (SC_ROW_THREADS / rp.gsz) * rp.gsz;
@@ -461,6 +463,9 @@ struct Solve {
   int* ndone = nullptr;
   float* Psum = nullptr;
   bool per_map_d = false, can_stop = false, finished = false;
+  // State V = Y + U in the U array (row_kernel<ROW_ITER>), Y written by
+  // result(); with a warm start Y and U are kept apart (ROW_ITER_YU).
+  bool vstate = true;
   int col_mode = COL_SOLVE_P;  // the column solve of the iteration
   int done_iters = 0;
   RowParams rp = {};
@@ -492,6 +497,7 @@ struct Solve {
     Psum = (float*)((unsigned char*)workspace + pl.off_Ps);
     // one d for every map unless GradWeight differs between maps
     per_map_d = p->grd && !p->wgrd_uniform;
+    vstate = p->U0 == nullptr;
     // Plain problems with short filters (Kr <= 16 rows) and a compiled column
     // length take the convolution column solve.
     col_mode = per_map_d ? COL_SOLVE_W
@@ -560,7 +566,7 @@ struct Solve {
     rp.g = g; rp.pw = pl.pw; rp.twW = twW; rp.F = F; rp.Y = p->Y; rp.Yo = p->Y; rp.U = U;
     rp.lam = p->lmbda; rp.l1_kind = p->l1_kind; rp.l1_scalar = p->l1_scalar; rp.l1w = p->l1w;
     rp.mask = p->mask; rp.relax = o->relax; rp.invN = (float)(1.0 / ((double)g.H * g.W));
-    rp.partials = part; rp.st = sts;
+    rp.partials = part; rp.st = sts; rp.vstate = vstate ? 1 : 0;
     cp.g = g; cp.ph = pl.ph; cp.twH = twH; cp.twW = twW; cp.F = F; cp.Dh = Dh; cp.Sh = Sh;
     cp.grd = p->grd; cp.mu = p->mu; cp.wgrd = p->wgrd; cp.Psum = Psum; cp.st = sts;
     cp.E = Erows; cp.Kr = p->Kr;
@@ -601,7 +607,11 @@ struct Solve {
              }
            })))
         return st;
-      if ((st = timed(1, [&] { return launch_row<ROW_ITER>(pl, rp, B, s); }))) return st;
+      if ((st = timed(1, [&] {
+             return vstate ? launch_row<ROW_ITER>(pl, rp, B, s)
+                           : launch_row<ROW_ITER_YU>(pl, rp, B, s);
+           })))
+        return st;
       if ((st = timed(2, [&]() -> int {
              finalize_kernel<<<B, 256, 0, s>>>(part, pl.row_nblk, sts, fp);
              CU_TRY(cudaGetLastError());
@@ -628,7 +638,20 @@ struct Solve {
     return SC_OK;
   }
 
+  // Y and U from the state V into y and u (u may be NULL).
+  int state_yu(float* y, float* u) {
+    const Geom& g = pl.g;
+    const size_t n = (size_t)g.M * g.H * g.W;
+    dim3 grid((unsigned)std::min<size_t>((n + 255) / 256, 1024), g.B);
+    state_yu_kernel<<<grid, 256, 0, s>>>(U, y, u, sts, p->lmbda, g.M, g.H, g.W, p->l1_kind,
+                                         p->l1_scalar, p->l1w, p->mask);
+    CU_TRY(cudaGetLastError());
+    ++g_launches;
+    return SC_OK;
+  }
+
   int export_u() {
+    if (vstate) return state_yu(p->Y, p->U_out);
     if (!p->U_out) return SC_OK;
     const size_t per = (size_t)pl.g.M * pl.g.H * pl.g.W, n = per * pl.g.B;
     export_u_kernel<<<(unsigned)std::min<size_t>((n + 255) / 256, 4096), 256, 0, s>>>(
@@ -837,10 +860,10 @@ extern "C" int sc_unrolled_forward(const sc_problem* p, const sc_options* o, int
   // both produce the same iterates
   sv.col_mode = COL_SOLVE;
   for (int j = 0; j < u.nseg; ++j) {
-    CU_TRY(cudaMemcpyAsync(w + u.ckY + sizeof(float) * u.R * j, u.p.Y, sizeof(float) * u.R,
-                           cudaMemcpyDeviceToDevice, s));
-    CU_TRY(cudaMemcpyAsync(w + u.ckU + sizeof(float) * u.R * j, sv.U, sizeof(float) * u.R,
-                           cudaMemcpyDeviceToDevice, s));
+    // (Y, U) of the state at the segment's start
+    if ((st = sv.state_yu((float*)(w + u.ckY + sizeof(float) * u.R * j),
+                          (float*)(w + u.ckU + sizeof(float) * u.R * j))))
+      return st;
     if ((st = sv.launch(std::min(u.seg, u.K - j * u.seg), untimed))) return st;
   }
   sc_result res;
@@ -930,7 +953,7 @@ extern "C" int sc_unrolled_backward(const sc_problem* p, const sc_options* o, in
       RowParams rr = sv.rp;
       rr.Y = Yat(i);
       rr.Yo = Yat(i + 1);
-      if ((st = launch_row<ROW_ITER>(pl, rr, B, s))) return st;
+      if ((st = launch_row<ROW_ITER_YU>(pl, rr, B, s))) return st;
     }
     // reverse it
     ra.Ymask = Yat(n);

@@ -69,6 +69,12 @@ CONFIGS = {
                      "iterations, loss ||D*X - S_clean||^2 + 0.01||X||_1, backward to D and S",
             H=256, W=256, M=32, K=11, density=0.01, lmbda=0.05, mu=0.0, nimg=16,
             variants=["cbpdn"], iters=200, autorho=False, mask_p=None),
+    # 1024x1024 with the maps of the 2048x2048 problem: the column pass's
+    # per-CTA work of that problem at a quarter of its memory (3 GB), for
+    # kernel profiles
+    10: dict(workload="cbpdn 1024x1024 M=256 16x16, 20 iterations, AutoRho (profiling case)",
+             H=1024, W=1024, M=256, K=16, density=0.01, lmbda=0.02, mu=0.0,
+             variants=["cbpdn"], iters=20, autorho=True, mask_p=None),
     # small 2048x2048 case for kernel profiles (2 GB on the device)
     9: dict(workload="cbpdn 2048x2048 M=24 16x16, 20 iterations, AutoRho (profiling case)",
             H=2048, W=2048, M=24, K=16, density=0.01, lmbda=0.02, mu=0.0,

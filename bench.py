@@ -302,18 +302,25 @@ def run_ours(args, cfg, rank, world, local_rank):
             Di[1:] = D
             l1 = np.ones(M1, np.float32)
             l1[0] = 0.0
-            ds = cb.prepare_device(Di, (S * mask)[None], lam, opt, l1=l1,
-                                   mask=mask.to(torch.int32)[None], profile=True)
+            pair = [cb.prepare_device(Di, (S * mask)[None], lam, opt, l1=l1,
+                                      mask=mask.to(torch.int32)[None], profile=pf)
+                    for pf in (False, True)]
         else:
-            ds = cb.prepare_device(D, S[None], lam, opt, mu=cfg["mu"],
-                                   grd=(v == "cbpdngrd"), profile=True)
-        solves.append((v, ds))
+            pair = [cb.prepare_device(D, S[None], lam, opt, mu=cfg["mu"],
+                                      grd=(v == "cbpdngrd"), profile=pf)
+                    for pf in (False, True)]
+        solves.append((v, pair[0], pair[1]))
 
-    def step():
+    def step(profiled=False):
+        """One pass of every solve; with profiled, CUDA events around every
+        kernel launch (the per-kernel split of the roofline)."""
         prof = {}
-        for v, ds in solves:
-            ds.run()
-            for k, (ms, n) in ds.profile().items():
+        for v, ds, dsp in solves:
+            if not profiled:
+                ds.run()
+                continue
+            dsp.run()
+            for k, (ms, n) in dsp.profile().items():
                 a = prof.setdefault(k, [0.0, 0])
                 a[0] += ms
                 a[1] += n
@@ -326,22 +333,27 @@ def run_ours(args, cfg, rank, world, local_rank):
 
     for _ in range(args.warmup):
         step()
+    step(profiled=True)
     barrier()
     n_launch0 = _lib.sc_launch_count()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    prof_tot = {}
     with ClockSampler(local_rank) as clk:
         ev0.record()
         for _ in range(args.steps):
-            p = step()
-            for k, (ms, n) in p.items():
-                a = prof_tot.setdefault(k, [0.0, 0])
-                a[0] += ms
-                a[1] += n
+            step()
         ev1.record()
         barrier()
     ms = ev0.elapsed_time(ev1)
     launches = _lib.sc_launch_count() - n_launch0
+    # the same steps again with an event pair around every kernel launch (on
+    # the solver's stream): the per-kernel split and the roofline
+    prof_tot = {}
+    for _ in range(args.steps):
+        for k, (pms, n) in step(profiled=True).items():
+            a = prof_tot.setdefault(k, [0.0, 0])
+            a[0] += pms
+            a[1] += n
+    barrier()
     iters_per_step = cfg["iters"] * len(cfg["variants"])
     value = replicas.job_rate(iters_per_step * args.steps, ms)
     ms = replicas.max_over_ranks(ms)

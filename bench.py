@@ -143,7 +143,7 @@ MEASURED_TRAFFIC_PER_MAP = {(2048, 2048): {"row_kernel": (1211e6 + 1149e6) / 24}
 
 def design_bytes(H, W, M, variant="cbpdn", K=None):
     """Per-iteration HBM bytes this design moves for one image.  Row pass:
-    reads and writes the spectra F (2C) and Y, U (4R).  Column pass, by
+    reads and writes the spectra F (2C) and the state V = Y + U (2R).  Column pass, by
     solve: the convolution solve (plain problems, filters of at most 16 rows,
     compiled column length) reads F twice and writes it (3C); the transform
     solve also reads the dictionary spectra twice (+2 C_D, C_D = C per
@@ -154,7 +154,7 @@ def design_bytes(H, W, M, variant="cbpdn", K=None):
     grd = variant in ("cbpdngrd", "cbpdngrdmsk")
     conv = not grd and K is not None and K <= 16 and H in SPEC_COL
     col = 3 * Cs if conv else 3 * Cs + 2 * Cs + (2 * Cs if grd else 0)
-    return 4 * R + 2 * Cs + col
+    return 2 * R + 2 * Cs + col
 
 
 def synth(cfg, seed, device):

@@ -357,17 +357,48 @@ static int cluster_size(const void* fn, int NT, size_t smem, int M, long units, 
   return SC_OK;
 }
 
+// Cluster sizes measured by the autotuner, per (device, kernel, image size,
+// maps); they replace the occupancy model's choice for that shape whatever
+// the number of images, so that a batch and a single solve of one size use
+// the same cluster size (the map reduction's summation order depends on it).
+struct TunedG {
+  int dev;
+  const void* fn;
+  int H, W, M;
+  int G;
+};
+static std::vector<TunedG> g_tuned;
+
+// The autotuner runs unless SPORCO_B200_AUTOTUNE is set to 0.
+static bool autotune_enabled() {
+  const char* e = getenv("SPORCO_B200_AUTOTUNE");
+  return !(e && e[0] == '0');
+}
+
+static bool tuned_size(const void* fn, const Geom& g, int* G) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  for (const TunedG& e : g_tuned)
+    if (e.dev == dev && e.fn == fn && e.H == g.H && e.W == g.W && e.M == g.M) {
+      *G = e.G;
+      return true;
+    }
+  return false;
+}
+
+// force_G > 0: launch with that cluster size (the autotuner's trials).
 template <int MODE>
-static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s) {
+static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s, int force_G = 0) {
   cp.Hs = pl.Hs;
   if (col_clustered(MODE)) {
     ColFn fn = col_fn<MODE>(cp.g.H);
     int st = prepare_fn((const void*)fn, true);
     if (st) return st;
-    int G = 1;
+    int G = force_G;
     const size_t smem = col_smem_bytes(MODE, pl.col_hlen);
-    if ((st = cluster_size((const void*)fn, pl.col_NT, smem, cp.g.M,
-                           (long)pl.col_ntiles * B, &G)))
+    const long units = (long)pl.col_ntiles * B;
+    if (G <= 0 && !tuned_size((const void*)fn, cp.g, &G) &&
+        (st = cluster_size((const void*)fn, pl.col_NT, smem, cp.g.M, units, &G)))
       return st;
     cp.gsz = pl.col_g;
     cp.G = G;
@@ -467,6 +498,7 @@ struct Solve {
   // result(); with a warm start Y and U are kept apart (ROW_ITER_YU).
   bool vstate = true;
   int col_mode = COL_SOLVE_P;  // the column solve of the iteration
+  bool tune = true;            // run the column-pass autotuner at set-up
   int done_iters = 0;
   RowParams rp = {};
   ColParams cp = {};
@@ -544,19 +576,7 @@ struct Solve {
       c.g = g; c.g.M = 1; c.ph = pl.ph; c.twH = twH; c.twW = twW; c.F = Sh;
       if ((st = launch_col<COL_FWD>(pl, c, g.B, s))) return st;
     }
-    const size_t real_all = (size_t)g.B * g.M * g.H * g.W;
-    if (p->U0) {
-      // start from the given iterates: U from U0, Y as given, F = rowFFT(Y - U)
-      CU_TRY(cudaMemcpyAsync(U, p->U0, sizeof(float) * real_all, cudaMemcpyDeviceToDevice, s));
-      CU_TRY(cudaMemsetAsync(F, 0, sizeof(float2) * (size_t)g.B * g.M * g.H * g.Wp, s));
-      RowParams r = {};
-      r.g = g; r.pw = pl.pw; r.twW = twW; r.F = F; r.Y = p->Y; r.U = U;
-      if ((st = launch_row<ROW_FWD_YU>(pl, r, g.B, s))) return st;
-    } else {
-      CU_TRY(cudaMemsetAsync(p->Y, 0, sizeof(float) * real_all, s));
-      CU_TRY(cudaMemsetAsync(U, 0, sizeof(float) * real_all, s));
-      CU_TRY(cudaMemsetAsync(F, 0, sizeof(float2) * (size_t)g.B * g.M * g.H * g.Wp, s));
-    }
+    if ((st = init_iterates())) return st;
     init_state_kernel<<<(g.B + 127) / 128, 128, 0, s>>>(sts, p->rho0, g.B, ndone);
     xi_kernel<<<(g.B + 127) / 128, 128, 0, s>>>(xi, p->lmbda, g.B, o->rsdl_target,
                                                  o->std_residuals);
@@ -581,7 +601,99 @@ struct Solve {
     // solve early; the host then never waits on the device mid-solve.
     can_stop = o->rel_tol > 0.f || o->abs_tol > 0.f;
     finished = o->max_iter <= 0;
+    if (tune && autotune_enabled() && o->max_iter > 0) {
+      if ((st = tune_col())) return st;
+    }
     return SC_OK;
+  }
+
+  // The starting iterates and their row spectra.
+  int init_iterates() {
+    const Geom& g = pl.g;
+    const size_t real_all = (size_t)g.B * g.M * g.H * g.W;
+    if (p->U0) {
+      // start from the given iterates: U from U0, Y as given, F = rowFFT(Y - U)
+      CU_TRY(cudaMemcpyAsync(U, p->U0, sizeof(float) * real_all, cudaMemcpyDeviceToDevice, s));
+      CU_TRY(cudaMemsetAsync(F, 0, sizeof(float2) * (size_t)g.B * g.M * g.H * g.Wp, s));
+      RowParams r = {};
+      r.g = g; r.pw = pl.pw; r.twW = twW; r.F = F; r.Y = p->Y; r.U = U;
+      int st = launch_row<ROW_FWD_YU>(pl, r, g.B, s);
+      if (st) return st;
+    } else {
+      CU_TRY(cudaMemsetAsync(p->Y, 0, sizeof(float) * real_all, s));
+      CU_TRY(cudaMemsetAsync(U, 0, sizeof(float) * real_all, s));
+      CU_TRY(cudaMemsetAsync(F, 0, sizeof(float2) * (size_t)g.B * g.M * g.H * g.Wp, s));
+    }
+    return SC_OK;
+  }
+
+  // The column pass of the iteration at cluster size G (0: tuned or model).
+  int launch_iter_col(int G) {
+    const int B = pl.g.B;
+    switch (col_mode) {
+      case COL_SOLVE_W: return launch_col<COL_SOLVE_W>(pl, cp, B, s, G);
+      case COL_SOLVE: return launch_col<COL_SOLVE>(pl, cp, B, s, G);
+      case COL_SOLVE_C8: return launch_col<COL_SOLVE_C8>(pl, cp, B, s, G);
+      case COL_SOLVE_C16: return launch_col<COL_SOLVE_C16>(pl, cp, B, s, G);
+      default: return launch_col<COL_SOLVE_P>(pl, cp, B, s, G);
+    }
+  }
+  const void* iter_col_fn() const {
+    switch (col_mode) {
+      case COL_SOLVE_W: return (const void*)col_fn<COL_SOLVE_W>(pl.g.H);
+      case COL_SOLVE: return (const void*)col_fn<COL_SOLVE>(pl.g.H);
+      case COL_SOLVE_C8: return (const void*)col_fn<COL_SOLVE_C8>(pl.g.H);
+      case COL_SOLVE_C16: return (const void*)col_fn<COL_SOLVE_C16>(pl.g.H);
+      default: return (const void*)col_fn<COL_SOLVE_P>(pl.g.H);
+    }
+  }
+
+  // Autotuner of the column pass: the first solve of a shape in a process
+  // times the iteration's column pass at every cluster size the device can
+  // hold (8, 4, 2 CTAs, at most M; two rounds, the faster time of each kept)
+  // on the freshly initialised state, keeps the fastest for later launches
+  // of that shape and initialises the iterates again (the trials overwrite
+  // the spectra).  It waits for the device once, at that first set-up.
+  int tune_col() {
+    const Geom& g = pl.g;
+    const void* fn = iter_col_fn();
+    int G0 = 0;
+    if (tuned_size(fn, g, &G0)) return SC_OK;
+    int st = prepare_fn(fn, true);
+    if (st) return st;
+    const size_t smem = col_smem_bytes(col_mode, pl.col_hlen);
+    int cand[3], nc = 0;
+    for (int G = 8; G >= 2; G /= 2) {
+      int n = 0;
+      if (G > g.M) continue;
+      if ((st = resident_clusters(fn, pl.col_NT, smem, G, &n))) return st;
+      if (n >= 1) cand[nc++] = G;
+    }
+    if (nc < 2) return SC_OK;  // nothing to choose
+    cudaEvent_t e0, e1;
+    CU_TRY(cudaEventCreate(&e0));
+    CU_TRY(cudaEventCreate(&e1));
+    float best_ms[3] = {1e30f, 1e30f, 1e30f};
+    for (int round = 0; round < 2 && !st; ++round) {
+      for (int i = 0; i < nc && !st; ++i) {
+        float ms = 0.f;
+        if (cudaEventRecord(e0, s) != cudaSuccess) { st = SC_ERR_CUDA; break; }
+        st = launch_iter_col(cand[i]);
+        if (!st && cudaEventRecord(e1, s) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
+            cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+          best_ms[i] = std::min(best_ms[i], ms);
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st) return st;
+    int bi = 0;
+    for (int i = 1; i < nc; ++i)
+      if (best_ms[i] < best_ms[bi]) bi = i;
+    int dev = 0;
+    CU_TRY(cudaGetDevice(&dev));
+    g_tuned.push_back({dev, fn, g.H, g.W, g.M, cand[bi]});
+    return init_iterates();
   }
 
   // Iterations to launch before the next poll.
@@ -598,13 +710,7 @@ struct Solve {
     int st;
     for (int i = 0; i < n; ++i) {
       if ((st = timed(0, [&] {
-             switch (col_mode) {
-               case COL_SOLVE_W: return launch_col<COL_SOLVE_W>(pl, cp, B, s);
-               case COL_SOLVE: return launch_col<COL_SOLVE>(pl, cp, B, s);
-               case COL_SOLVE_C8: return launch_col<COL_SOLVE_C8>(pl, cp, B, s);
-               case COL_SOLVE_C16: return launch_col<COL_SOLVE_C16>(pl, cp, B, s);
-               default: return launch_col<COL_SOLVE_P>(pl, cp, B, s);
-             }
+             return launch_iter_col(0);
            })))
         return st;
       if ((st = timed(1, [&] {
@@ -855,6 +961,7 @@ extern "C" int sc_unrolled_forward(const sc_problem* p, const sc_options* o, int
   cudaStream_t s = (cudaStream_t)stream;
   unsigned char* w = (unsigned char*)ws;
   Solve sv;
+  sv.tune = false;  // forward and recomputation must use the same cluster sizes
   if ((st = sv.setup(&u.p, &u.o, ws, u.pl.total, s))) return st;
   // the same column solve as the recomputation in the reverse pass, so that
   // both produce the same iterates
@@ -926,6 +1033,7 @@ extern "C" int sc_unrolled_backward(const sc_problem* p, const sc_options* o, in
   // the caller's result
   u.p.Y = Ytr;
   Solve sv;
+  sv.tune = false;
   if ((st = sv.setup(&u.p, &u.o, ws, pl.total, s))) return st;
   CU_TRY(cudaMemsetAsync(gDh, 0, sizeof(float2) * u.C, s));
   CU_TRY(cudaMemsetAsync(gSh, 0, sizeof(float2) * (size_t)B * g.H * g.Wp, s));

@@ -121,7 +121,7 @@ typedef struct sc_options {
   float rsdl_target;    /* AutoRho.RsdlTarget, <= 0: derive from lambda */
   int auto_scaling;     /* AutoRho.AutoScaling */
   int std_residuals;    /* AutoRho.StdResiduals */
-  int record_itstat;    /* keep per-iteration r, s, rho on the device */
+  int record_itstat;    /* keep per-iteration statistics on the device (see sc_read_state) */
   int check_every;      /* host polls the stop flag every this many iterations (0: never) */
   int profile;          /* time every iteration kernel with CUDA events (sc_last_profile) */
 } sc_options;
@@ -176,8 +176,17 @@ int sc_cbpdn_solve_batch(const sc_problem *probs, int nprob, const sc_options *o
                          void *const *workspaces, const size_t *workspace_bytes,
                          sc_result *res, void *const *streams);
 
+/* Values per image and iteration in the statistics (sc_read_state). */
+#define SC_ITSTAT_FIELDS 8
+
 /* Per-image iteration counts / final rho / itstat after a solve, copied from
- * the workspace of that solve (host pointers; itstat may be NULL). */
+ * the workspace of that solve (host pointers; itstat may be NULL).  itstat is
+ * (B, max_iter, 8) doubles per iteration: r, s, rho, eps_pri, eps_dua, then
+ * the functional at Y, its data fidelity 0.5 ||sum_m d_m * y_m - s||^2 and
+ * its L1 sum ||w y||_1 (the reference's Verbose columns, cbpdn.cu:438-517;
+ * the functional adds lambda times the L1 sum and, with the gradient term,
+ * mu/2 sum_m w_m ||grad y_m||^2; masked problems count the impulse map as a
+ * filter, as the reference does).  Kept only with options.record_itstat. */
 int sc_read_state(const sc_problem *p, const sc_options *o, const void *workspace,
                   int *iterations, double *rho, double *itstat, void *stream);
 

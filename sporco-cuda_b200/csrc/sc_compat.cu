@@ -135,14 +135,18 @@ int record(int st, const char* msg) { return sc_set_status_external(st, msg); }
   } while (0)
 
 void print_itstat(const std::vector<double>& it, int iters, int grd) {
-  // The reference prints Itn / functional / r / s / rho per iteration
-  // (cbpdn.cu:309-312, 438-517); here r, s and rho recorded on the device.
-  const char* sep = "----------------------------------------";
-  printf("Itn   r         s         %s\n%s\n", "\xcf\x81", sep);
-  for (int k = 0; k < iters; ++k)
-    printf("%4d %9.2e %9.2e %9.2e\n", k, it[k * 5 + 0], it[k * 5 + 1], it[k * 5 + 2]);
+  // The reference's Verbose table (cbpdn.cu:309-312, 438-517): iteration,
+  // functional, data fidelity, L1 term, r, s, rho; here all recorded on the
+  // device during the solve (the functional at Y).
+  const char* sep =
+      "-------------------------------------------------------------------";
+  printf("Itn   Fnc       DFid      Regl1     r         s         %s\n%s\n",
+         grd ? "rho (grd) " : "rho", sep);
+  for (int k = 0; k < iters; ++k) {
+    const double* v = &it[(size_t)k * SC_ITSTAT_FIELDS];
+    printf("%4d %9.2e %9.2e %9.2e %9.2e %9.2e %9.2e\n", k, v[5], v[6], v[7], v[0], v[1], v[2]);
+  }
   printf("%s\n", sep);
-  (void)grd;
 }
 
 void run_compat(float* D, float* S, float lambda, float mu, void* vopt, float* Yout, int grd) {
@@ -258,7 +262,7 @@ void run_compat(float* D, float* S, float lambda, float mu, void* vopt, float* Y
   if (st != SC_OK) return;
   COMPAT_TRY(cudaMemcpyAsync(Yout, p.Y, sz_Y, cudaMemcpyDeviceToHost, s));
   if (opt->Verbose == 1) {
-    std::vector<double> it(5 * (size_t)std::max(1, o.max_iter));
+    std::vector<double> it(SC_ITSTAT_FIELDS * (size_t)std::max(1, o.max_iter));
     int iters = 0;
     double rho = 0;
     sc_read_state(&p, &o, base + off_ws, &iters, &rho, it.data(), s);

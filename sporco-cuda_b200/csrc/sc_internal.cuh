@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "../../include/sporco_b200.h"
 #include "sc_fft.cuh"
 
 // Elements one thread holds during an FFT pass (see sc_fft.cuh).
@@ -44,7 +45,7 @@ struct FinParams {
   double rho_scaling, rsdl_ratio, abs_tol, rel_tol;
   double nelem;          // coefficients per image (M H W)
   const double* xi;      // (B,) residual ratio target per image
-  double* itstat;        // (B, max_iter, 5) or NULL
+  double* itstat;        // (B, max_iter, SC_ITSTAT_FIELDS) or NULL
   int* ndone;            // images finished
 };
 

@@ -1519,7 +1519,7 @@ __global__ void finalize_kernel(const double* __restrict__ partials, int nblk,
   }
   const int k = S.k + 1;
   if (F.itstat) {
-    double* it = F.itstat + ((size_t)b * F.max_iter + (k - 1)) * 5;
+    double* it = F.itstat + ((size_t)b * F.max_iter + (k - 1)) * SC_ITSTAT_FIELDS;
     it[0] = r; it[1] = s; it[2] = rho; it[3] = epri; it[4] = edua;
   }
   double rsf = 1.0;
@@ -1618,6 +1618,95 @@ __global__ void state_yu_kernel(const float* __restrict__ V, float* __restrict__
     Y[off + i] = y;
     if (U) U[off + i] = u;
   }
+}
+
+// ============================================================= functional ==
+// The functional at Y (Verbose statistics, cbpdn.cu:438-517): data fidelity
+// 0.5 ||sum_m d_m * y_m - s||^2 and, with the gradient term,
+// mu/2 sum_m w_m ||grad y_m||^2, both by Parseval over the half spectrum
+// (columns 0 and W/2 once, the others twice; divided by H W), from the
+// spectra Yh (B, M, H, Wp), Dh (M, H, Wp) and Sh (B, H, Wp).  Grid (nblk,
+// B); part (B, nblk, 2): fidelity and gradient sums.
+__global__ void objective_spec_kernel(const float2* __restrict__ Yh,
+                                      const float2* __restrict__ Dh,
+                                      const float2* __restrict__ Sh, Geom g, int grd,
+                                      const float* __restrict__ wgrd,
+                                      const float2* __restrict__ twH,
+                                      const float2* __restrict__ twW, double* part) {
+  __shared__ double scratch[(256 / 32) * 2];
+  const int b = blockIdx.y;
+  const size_t plane = (size_t)g.H * g.Wp;
+  const float2* Yb = Yh + (size_t)b * g.M * plane;
+  double v[2] = {0.0, 0.0};
+  const size_t nf = (size_t)g.H * g.Wf;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nf;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int kr = (int)(i / g.Wf), kc = (int)(i - (size_t)kr * g.Wf);
+    const size_t f = (size_t)kr * g.Wp + kc;
+    const double w = (kc == 0 || 2 * kc == g.W) ? 1.0 : 2.0;
+    double rx = -(double)Sh[(size_t)b * plane + f].x, ry = -(double)Sh[(size_t)b * plane + f].y;
+    double gs = 0.0;
+    for (int m = 0; m < g.M; ++m) {
+      const float2 d = Dh[(size_t)m * plane + f], y = Yb[(size_t)m * plane + f];
+      rx += (double)d.x * y.x - (double)d.y * y.y;
+      ry += (double)d.x * y.y + (double)d.y * y.x;
+      if (grd) gs += (double)wgrd[m] * ((double)y.x * y.x + (double)y.y * y.y);
+    }
+    v[0] += w * (rx * rx + ry * ry);
+    if (grd) {
+      const double gk = (2.0 - 2.0 * (double)twW[kc].x) + (2.0 - 2.0 * (double)twH[kr].x);
+      v[1] += w * gk * gs;
+    }
+  }
+  block_sum<2>(v, scratch);
+  if (threadIdx.x == 0) {
+    double* o = part + ((size_t)b * gridDim.x + blockIdx.x) * 2;
+    o[0] = v[0];
+    o[1] = v[1];
+  }
+}
+
+// sum |w y| per (image, block): the L1 term at Y.  Grid (nblk, B);
+// part (B, nblk).
+__global__ void objective_l1_kernel(const float* __restrict__ Y, Geom g, int l1_kind,
+                                    float l1_scalar, const float* __restrict__ l1w,
+                                    double* part) {
+  __shared__ double scratch[256 / 32];
+  const int b = blockIdx.y;
+  const size_t plane = (size_t)g.H * g.W, n = (size_t)g.M * plane;
+  const float* Yb = Y + (size_t)b * n;
+  double v[1] = {0.0};
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const float w = l1_kind == 1 ? l1w[i / plane] : l1_kind == 2 ? l1w[i] : l1_scalar;
+    v[0] += fabs((double)w * (double)Yb[i]);
+  }
+  block_sum<1>(v, scratch);
+  if (threadIdx.x == 0) part[(size_t)b * gridDim.x + blockIdx.x] = v[0];
+}
+
+// Functional, fidelity and L1 terms into the statistics row of the iteration
+// just completed (ImgState::k).  One thread per image.
+__global__ void objective_final_kernel(const double* __restrict__ pspec,
+                                       const double* __restrict__ pl1, int nblk,
+                                       const ImgState* __restrict__ st,
+                                       const float* __restrict__ lam, double invN, float mu,
+                                       double* itstat, int max_iter, int B) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  const int k = st[b].k;
+  if (k < 1 || k > max_iter) return;
+  double df = 0.0, gr = 0.0, l1 = 0.0;
+  for (int i = 0; i < nblk; ++i) {
+    df += pspec[((size_t)b * nblk + i) * 2];
+    gr += pspec[((size_t)b * nblk + i) * 2 + 1];
+    l1 += pl1[(size_t)b * nblk + i];
+  }
+  df *= 0.5 * invN;
+  double* it = itstat + ((size_t)b * max_iter + (k - 1)) * SC_ITSTAT_FIELDS;
+  it[5] = df + (double)lam[b] * l1 + 0.5 * (double)mu * gr * invN;
+  it[6] = df;
+  it[7] = l1;
 }
 
 __global__ void export_u_kernel(const float* __restrict__ U, float* __restrict__ out,

@@ -124,6 +124,9 @@ static bool spec_col(int n) {
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// CTAs per image of the functional's reduction kernels (statistics only).
+#define SC_OBJ_BLOCKS 128
+
 struct Plan {
   Geom g;
   FftPlan pw, ph;
@@ -141,7 +144,7 @@ struct Plan {
   size_t colg_smem, colt_smem;
   int max_iter;
   size_t off_U, off_F, off_Dh, off_Sh, off_Ps, off_E, off_twW, off_twH, off_part, off_st,
-      off_it, off_xi, off_ndone, total;
+      off_it, off_xi, off_ndone, off_objspec, off_objpart, total;
 };
 
 static int g_num_sms = 0;
@@ -218,7 +221,12 @@ static int plan_problem(const sc_problem* p, const sc_options* o, Plan* pl) {
   pl->off_twH = take(sizeof(float2) * g.H);
   pl->off_part = take(sizeof(double) * 5 * (size_t)pl->row_nblk * g.B);
   pl->off_st = take(sizeof(ImgState) * g.B);
-  pl->off_it = take(o->record_itstat ? sizeof(double) * 5 * (size_t)std::max(1, o->max_iter) * g.B : 0);
+  pl->off_it = take(o->record_itstat ? sizeof(double) * SC_ITSTAT_FIELDS *
+                                          (size_t)std::max(1, o->max_iter) * g.B
+                                    : 0);
+  // the functional at Y (statistics only): Y's spectra, partial sums
+  pl->off_objspec = take(o->record_itstat ? sizeof(float2) * spec_img * g.B : 0);
+  pl->off_objpart = take(o->record_itstat ? sizeof(double) * 3 * SC_OBJ_BLOCKS * g.B : 0);
   pl->off_xi = take(sizeof(double) * g.B);
   pl->off_ndone = take(sizeof(int));
   pl->total = off;
@@ -493,6 +501,7 @@ struct Solve {
   ImgState* sts = nullptr;
   int* ndone = nullptr;
   float* Psum = nullptr;
+  void* wsbase = nullptr;
   bool per_map_d = false, can_stop = false, finished = false;
   // State V = Y + U in the U array (row_kernel<ROW_ITER>), Y written by
   // result(); with a warm start Y and U are kept apart (ROW_ITER_YU).
@@ -524,6 +533,7 @@ struct Solve {
     if ((p->W % 4) == 0 && (((uintptr_t)p->Y) & 15))
       return set_status(SC_ERR_INVALID, "Y must be 16-byte aligned");
     const Geom& g = pl.g;
+    wsbase = workspace;
     carve(pl, (unsigned char*)workspace, &U, &F, &Dh, &Sh, &twW, &twH, &part, &sts, &it, &xi,
           &ndone);
     Psum = (float*)((unsigned char*)workspace + pl.off_Ps);
@@ -722,7 +732,7 @@ struct Solve {
              finalize_kernel<<<B, 256, 0, s>>>(part, pl.row_nblk, sts, fp);
              CU_TRY(cudaGetLastError());
              ++g_launches;
-             return SC_OK;
+             return o->record_itstat ? objective() : SC_OK;
            })))
         return st;
       if (o->auto_rho) {
@@ -741,6 +751,34 @@ struct Solve {
     CU_TRY(cudaMemcpyAsync(&nd, ndone, sizeof(int), cudaMemcpyDeviceToHost, s));
     CU_TRY(cudaStreamSynchronize(s));
     if (nd >= pl.g.B) finished = true;
+    return SC_OK;
+  }
+
+  // The functional at Y of the iteration just completed into the statistics
+  // (record_itstat): Y from the state, its 2-D spectrum, then the fidelity,
+  // gradient and L1 sums (cbpdn.cu:438-517).
+  int objective() {
+    const Geom& g = pl.g;
+    unsigned char* ws = (unsigned char*)wsbase;
+    float2* Yh = (float2*)(ws + pl.off_objspec);
+    double* pspec = (double*)(ws + pl.off_objpart);
+    double* pl1 = pspec + 2 * SC_OBJ_BLOCKS * g.B;
+    int st;
+    if (vstate && (st = state_yu(p->Y, nullptr))) return st;
+    RowParams r = {};
+    r.g = g; r.pw = pl.pw; r.twW = twW; r.F = Yh; r.src = p->Y;
+    if ((st = launch_row<ROW_FWD_REAL>(pl, r, g.B, s))) return st;
+    ColParams c = {};
+    c.g = g; c.ph = pl.ph; c.twH = twH; c.twW = twW; c.F = Yh;
+    if ((st = launch_col<COL_FWD>(pl, c, g.B, s))) return st;
+    const dim3 grid(SC_OBJ_BLOCKS, g.B);
+    objective_spec_kernel<<<grid, 256, 0, s>>>(Yh, Dh, Sh, g, p->grd, p->wgrd, twH, twW, pspec);
+    objective_l1_kernel<<<grid, 256, 0, s>>>(p->Y, g, p->l1_kind, p->l1_scalar, p->l1w, pl1);
+    objective_final_kernel<<<(g.B + 127) / 128, 128, 0, s>>>(
+        pspec, pl1, SC_OBJ_BLOCKS, sts, p->lmbda, 1.0 / ((double)g.H * g.W),
+        p->grd ? p->mu : 0.f, it, o->max_iter, g.B);
+    CU_TRY(cudaGetLastError());
+    g_launches += 3;
     return SC_OK;
   }
 
@@ -1118,7 +1156,8 @@ extern "C" int sc_read_state(const sc_problem* p, const sc_options* o, const voi
                          cudaMemcpyDeviceToHost, s));
   if (itstat && o->record_itstat)
     CU_TRY(cudaMemcpyAsync(itstat, ws + pl.off_it,
-                           sizeof(double) * 5 * (size_t)std::max(1, o->max_iter) * pl.g.B,
+                           sizeof(double) * SC_ITSTAT_FIELDS * (size_t)std::max(1, o->max_iter) *
+                               pl.g.B,
                            cudaMemcpyDeviceToHost, s));
   CU_TRY(cudaStreamSynchronize(s));
   for (int b = 0; b < pl.g.B; ++b) {

@@ -229,6 +229,12 @@ def _sc_options(r, record_itstat=False, check_every=32, profile=False):
     return o
 
 
+# Per-iteration statistics (sc_read_state): r, s, rho, eps_pri, eps_dua,
+# functional at Y, its data fidelity term, its L1 sum.
+ITSTAT_FIELDS = 8
+ITSTAT_NAMES = ("r", "s", "rho", "epri", "edua", "fnc", "dfid", "regl1")
+
+
 class DeviceSolve:
     """A prepared device solve: problem struct, options and workspace.
 
@@ -260,7 +266,7 @@ class DeviceSolve:
         rho = (C.c_double * B)()
         it = None
         if self.opts.record_itstat:
-            it = np.zeros((B, max(1, self.opts.max_iter), 5), dtype=np.float64)
+            it = np.zeros((B, max(1, self.opts.max_iter), ITSTAT_FIELDS), dtype=np.float64)
         st = _lib.sc_read_state(C.byref(self.prob), C.byref(self.opts),
                                 C.c_void_p(self.ws.data_ptr()), iters, rho,
                                 it.ctypes.data_as(C.POINTER(C.c_double)) if it is not None else None,

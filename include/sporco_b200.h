@@ -215,6 +215,14 @@ typedef struct sc_profile {
 } sc_profile;
 int sc_last_profile(sc_profile *out);
 
+/* Cancel every solve in progress in this process (any host thread): each
+ * stops launching iterations at its next check (every options.check_every
+ * iterations; without a stopping test it keeps at most two such chunks
+ * queued), writes the iterates it reached and returns SC_ERR_CANCELLED.
+ * Solves started after the call are not affected.  No counterpart in the
+ * reference (which can only be stopped with its process). */
+void sc_cancel(void);
+
 /* Number of kernels this library has launched since it was loaded. */
 unsigned long long sc_launch_count(void);
 

@@ -55,6 +55,9 @@ static int set_status(int st, const char* fmt, ...) {
 int sc_set_status_external(int st, const char* msg) { return set_status(st, msg && *msg ? "%s" : nullptr, msg); }
 
 static std::atomic<unsigned long long> g_launches{0};
+// Bumped by sc_cancel; a solve that sees it change stops launching.
+static std::atomic<unsigned> g_cancel_gen{0};
+extern "C" void sc_cancel(void) { g_cancel_gen.fetch_add(1); }
 static thread_local sc_profile g_profile = {};
 
 extern "C" unsigned long long sc_launch_count(void) { return g_launches.load(); }
@@ -508,6 +511,10 @@ struct Solve {
   bool vstate = true;
   int col_mode = COL_SOLVE_P;  // the column solve of the iteration
   bool tune = true;            // run the column-pass autotuner at set-up
+  unsigned gen0 = 0;           // cancellation generation at set-up
+  bool cancelled = false;
+  cudaEvent_t pace[2] = {nullptr, nullptr};
+  int nchunk = 0;
   int done_iters = 0;
   RowParams rp = {};
   ColParams cp = {};
@@ -518,6 +525,7 @@ struct Solve {
     p = p_;
     o = o_;
     s = stream;
+    gen0 = g_cancel_gen.load();
     if (!p || !o) return set_status(SC_ERR_INVALID, "null problem or options");
     int st = plan_problem(p, o, &pl);
     if (st) return st;
@@ -709,7 +717,7 @@ struct Solve {
   // Iterations to launch before the next poll.
   int chunk() const {
     int c = o->max_iter - done_iters;
-    if (o->check_every > 0 && can_stop) c = std::min(c, o->check_every);
+    if (o->check_every > 0) c = std::min(c, o->check_every);
     return c;
   }
 
@@ -745,13 +753,37 @@ struct Solve {
   }
 
   // Wait for the launched iterations and stop when every image is finished.
+  // Between chunks: with a stopping test, wait for the chunk and read the
+  // "finished" counter; without one, wait only for the chunk before (one
+  // chunk stays queued, the device never idles).  Either way a cancellation
+  // (sc_cancel) seen here stops the launches.
   int poll() {
     if (finished) return SC_OK;
-    int nd = 0;
-    CU_TRY(cudaMemcpyAsync(&nd, ndone, sizeof(int), cudaMemcpyDeviceToHost, s));
-    CU_TRY(cudaStreamSynchronize(s));
-    if (nd >= pl.g.B) finished = true;
+    if (can_stop) {
+      int nd = 0;
+      CU_TRY(cudaMemcpyAsync(&nd, ndone, sizeof(int), cudaMemcpyDeviceToHost, s));
+      CU_TRY(cudaStreamSynchronize(s));
+      if (nd >= pl.g.B) finished = true;
+    } else {
+      for (int i = 0; i < 2; ++i)
+        if (!pace[i]) CU_TRY(cudaEventCreateWithFlags(&pace[i], cudaEventDisableTiming));
+      CU_TRY(cudaEventRecord(pace[nchunk & 1], s));
+      if (nchunk > 0) CU_TRY(cudaEventSynchronize(pace[(nchunk - 1) & 1]));
+      ++nchunk;
+    }
+    if (g_cancel_gen.load() != gen0) {
+      cancelled = true;
+      finished = true;
+    }
     return SC_OK;
+  }
+
+  Solve() = default;
+  Solve(const Solve&) = delete;  // owns its pacing events
+  Solve& operator=(const Solve&) = delete;
+  ~Solve() {
+    for (int i = 0; i < 2; ++i)
+      if (pace[i]) cudaEventDestroy(pace[i]);
   }
 
   // The functional at Y of the iteration just completed into the statistics
@@ -808,6 +840,11 @@ struct Solve {
   int result(sc_result* res) {
     int st = export_u();
     if (st) return st;
+    if (cancelled) {
+      CU_TRY(cudaStreamSynchronize(s));
+      return set_status(SC_ERR_CANCELLED, "solve cancelled (sc_cancel) after %d iterations",
+                        done_iters);
+    }
     if (!res) return SC_OK;
     const int B = pl.g.B;
     ImgState h0;

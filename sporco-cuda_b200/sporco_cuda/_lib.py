@@ -156,6 +156,7 @@ sc_unrolled_forward = _proto("sc_unrolled_forward", C.c_int,
 sc_unrolled_backward = _proto("sc_unrolled_backward", C.c_int,
                               [PP, PO, C.c_int, VP, C.c_size_t, VP, VP, VP, VP])
 sc_last_profile = _proto("sc_last_profile", C.c_int, [C.POINTER(ScProfile)])
+sc_cancel = _proto("sc_cancel", None, [])
 sc_launch_count = _proto("sc_launch_count", C.c_ulonglong, [])
 sc_last_status = _proto("sc_last_status", C.c_int, [])
 sc_last_error = _proto("sc_last_error", C.c_char_p, [])
@@ -168,7 +169,7 @@ EXPORTED = [
     "get_memory_info", "get_device_name", "sc_workspace_size", "sc_options_from_algopt",
     "sc_cbpdn_solve", "sc_cbpdn_solve_batch", "sc_read_state", "sc_rfft2", "sc_irfft2",
     "sc_rfft2_noalloc", "sc_unrolled_workspace_size", "sc_unrolled_forward",
-    "sc_unrolled_backward", "sc_last_profile", "sc_launch_count",
+    "sc_unrolled_backward", "sc_cancel", "sc_last_profile", "sc_launch_count",
     "sc_last_status", "sc_last_error", "sc_version",
 ]
 

@@ -262,3 +262,41 @@ def test_verbose_table(capfd):
     assert len(rows) == 7
     fnc = [float(r.split()[1]) for r in rows]
     assert all(np.isfinite(fnc)) and fnc[-1] > 0
+
+
+@pytest.mark.gpu
+def test_cancel_stops_a_running_solve():
+    """sc_cancel from another thread stops a long fixed-iteration solve at its
+    next chunk: SolverError with SC_ERR_CANCELLED, well before the end; a solve
+    started afterwards runs normally."""
+    import threading
+    import time
+    from sporco_cuda import _lib
+    D, S = _synth(512, 512, 32, 8, 0.01, 3)
+    opt = {"MaxMainIter": 20000, "RelStopTol": 0.0, "AutoRho": {"Enabled": False}}
+    Dm = torch.tensor(np.moveaxis(D, 2, 0).copy(), device="cuda")
+    St = torch.tensor(S, device="cuda")[None]
+    ds = cb.prepare_device(Dm, St, 0.05, opt, check_every=16)
+    ds.run()  # set-up and autotuning out of the way (the run is the full solve)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ds.run()
+    torch.cuda.synchronize()
+    full = time.perf_counter() - t0
+    err = {}
+
+    def work():
+        try:
+            ds.run()
+        except _lib.SolverError as e:
+            err["e"] = e
+    th = threading.Thread(target=work)
+    t0 = time.perf_counter()
+    th.start()
+    time.sleep(0.1 * full)
+    _lib.sc_cancel()
+    th.join()
+    took = time.perf_counter() - t0
+    assert "e" in err and err["e"].status == 7, err
+    assert took < 0.6 * full, (took, full)
+    ds.run()  # a new solve is not cancelled

@@ -138,7 +138,7 @@ def graded_kernel_bytes(H, W, M):
 # dram__bytes_write.sum) for kernels whose traffic grows in proportion to the
 # maps; from the 2048x2048, M=24 capture summarised in
 # profiles/launch_list_2048x2048_m24.md.
-MEASURED_TRAFFIC_PER_MAP = {(2048, 2048): {"row_kernel": (1211e6 + 1149e6) / 24}}
+MEASURED_TRAFFIC_PER_MAP = {(2048, 2048): {"row_kernel": (807e6 + 744e6) / 24}}
 
 
 def design_bytes(H, W, M, variant="cbpdn", K=None):

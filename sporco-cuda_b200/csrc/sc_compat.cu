@@ -10,6 +10,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "../../include/sporco_b200.h"
@@ -149,6 +151,57 @@ void print_itstat(const std::vector<double>& it, int iters, int grd) {
   printf("%s\n", sep);
 }
 
+// Device-to-host copy into a pageable buffer (the caller's numpy array).
+// A plain cudaMemcpy to pageable memory goes through the driver's staging at
+// a few GB/s, and a fresh array also pays one page fault per 4 KB on first
+// touch.  Here the data comes over in chunks by DMA into two page-locked
+// staging buffers (allocated once per process, 2 x 64 MB) while host
+// threads copy the previous chunk into the destination in parallel, taking
+// its page faults in parallel too.
+constexpr size_t kStageBytes = (size_t)64 << 20;
+std::mutex g_stage_mu;
+void* g_stage[2] = {nullptr, nullptr};
+
+cudaError_t d2h_pageable(void* dst, const void* src, size_t n, cudaStream_t s) {
+  if (n < ((size_t)8 << 20)) return cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, s);
+  std::lock_guard<std::mutex> lock(g_stage_mu);
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < 2 && e == cudaSuccess; ++i)
+    if (!g_stage[i]) e = cudaHostAlloc(&g_stage[i], kStageBytes, cudaHostAllocDefault);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    return cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, s);
+  }
+  cudaEvent_t ev[2];
+  for (int i = 0; i < 2; ++i)
+    if ((e = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming)) != cudaSuccess) return e;
+  const size_t nch = (n + kStageBytes - 1) / kStageBytes;
+  const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  auto issue = [&](size_t k) -> cudaError_t {
+    const size_t off = k * kStageBytes, len = std::min(kStageBytes, n - off);
+    cudaError_t r = cudaMemcpyAsync(g_stage[k & 1], (const char*)src + off, len,
+                                    cudaMemcpyDeviceToHost, s);
+    return r == cudaSuccess ? cudaEventRecord(ev[k & 1], s) : r;
+  };
+  e = issue(0);
+  for (size_t k = 0; k < nch && e == cudaSuccess; ++k) {
+    if (k + 1 < nch && (e = issue(k + 1)) != cudaSuccess) break;
+    if ((e = cudaEventSynchronize(ev[k & 1])) != cudaSuccess) break;
+    const size_t off = k * kStageBytes, len = std::min(kStageBytes, n - off);
+    const size_t part = (len + hw - 1) / hw;
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < hw; ++t) {
+      const size_t a0 = t * part;
+      if (a0 >= len) break;
+      const size_t l = std::min(part, len - a0);
+      th.emplace_back([=] { memcpy((char*)dst + off + a0, (const char*)g_stage[k & 1] + a0, l); });
+    }
+    for (auto& x : th) x.join();
+  }
+  for (int i = 0; i < 2; ++i) cudaEventDestroy(ev[i]);
+  return e;
+}
+
 void run_compat(float* D, float* S, float lambda, float mu, void* vopt, float* Yout, int grd) {
   AlgOpt* opt = (AlgOpt*)vopt;
   record(SC_OK, "");
@@ -260,7 +313,7 @@ void run_compat(float* D, float* S, float lambda, float mu, void* vopt, float* Y
   sc_result res;
   int st = sc_cbpdn_solve(&p, &o, base + off_ws, ws, &res, s);
   if (st != SC_OK) return;
-  COMPAT_TRY(cudaMemcpyAsync(Yout, p.Y, sz_Y, cudaMemcpyDeviceToHost, s));
+  COMPAT_TRY(d2h_pageable(Yout, p.Y, sz_Y, s));
   if (opt->Verbose == 1) {
     std::vector<double> it(SC_ITSTAT_FIELDS * (size_t)std::max(1, o.max_iter));
     int iters = 0;

@@ -76,9 +76,10 @@ int check_cuda_req(int device) {
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return -1;
   if (device < 0 || device >= n) return -1;
-  cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return -1;
-  if (prop.major < 10) return -1;  // this build carries sm_100a code only
+  int major = 0;  // (one attribute: the full property query is slow per call)
+  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess)
+    return -1;
+  if (major < 10) return -1;  // this build carries sm_100a code only
   return device;
 }
 

@@ -375,21 +375,29 @@ __host__ __device__ constexpr int ct_threads(int n, int RM) {
 // Shared-memory slot of element i of a compile-time transform.
 //  * One transform per slot run (ST == 1, the row pass), N a multiple of 16:
 //    an XOR swizzle inside every aligned block of 16 elements, slot =
-//    i ^ g(i >> 4) with g(x) = (x & 7) | (x & 4) << 1.  A half-warp of 8-byte
-//    accesses is conflict-free when it touches 16 contiguous aligned
-//    elements (every load, the stores of the later passes), the stride-8
-//    elements 8j + q (stores of the first radix-8 pass) or two runs of 8
-//    elements 64 apart (stores of the second radix-8 pass).  No padding.
+//    i ^ g(i >> 4), with g(x) = (x & 7) | (x & 4) << 1 for radix-8 plans
+//    and g(x) = x & 15 for radix-16 plans.  A half-warp of 8-byte accesses
+//    is conflict-free when it touches 16 contiguous aligned elements (every
+//    load, the stores of the later passes) or the stores of the first pass
+//    (elements R j + q of 16 consecutive butterflies j); with radix 8 also
+//    two runs of 8 elements 64 apart (stores of the second pass).  No
+//    padding.
 //  * Interleaved transforms (ST > 1, the column pass, ST columns of 8 bytes
 //    per slot): one pad slot after every ct_pad elements (the first radix),
 //    which spreads the strided stores of the first pass over all banks.
 __host__ __device__ constexpr int ct_pad(int n, int RM) { return ct_plan(n, RM).r[0]; }
 __host__ __device__ constexpr bool ct_swizzled(int n, int ST) { return ST == 1 && n % 16 == 0; }
+// g of the swizzled layout; linear over GF(2): g(a ^ b) = g(a) ^ g(b).
+template <int RM>
+__host__ __device__ constexpr int ct_swz(int x) {
+  return RM == 16 ? (x & 15) : ((x & 7) | ((x & 4) << 1));
+}
+// Index period of the swizzle pattern (g reads bits 4..7 or 4..6 of i).
+__host__ __device__ constexpr int ct_swz_period(int RM) { return RM == 16 ? 256 : 128; }
 template <int N, int RM, int ST>
 __device__ __forceinline__ int ct_phys(int i) {
   if constexpr (ct_swizzled(N, ST)) {
-    const int x = i >> 4;
-    return i ^ ((x & 7) | ((x & 4) << 1));
+    return i ^ ct_swz<RM>(i >> 4);
   } else {
     constexpr int P = ct_pad(N, RM);
     return i + i / P;
@@ -402,20 +410,31 @@ __host__ __device__ constexpr int ct_len(int n, int RM, int ST) {
 }
 
 // Slot of element i0 + q * STRIDE (q < Q, compile-time) from the slot of i0.
-// In the swizzled layout the XOR pattern of an aligned 16-block depends on
-// bits 4..6 of the index only, so a stride that is a multiple of 128 keeps
-// it (slot = slot(i0) + q STRIDE), and a run of Q <= 16 elements inside one
-// aligned 16-block from an i0 that is a multiple of Q keeps it too
-// (slot = slot(i0) ^ q).  Otherwise the slot is computed per element.
+// In the swizzled layout:
+//  * a stride that is a multiple of the swizzle period keeps the pattern:
+//    slot = slot(i0) + q STRIDE;
+//  * STRIDE and Q powers of two and i0 sharing no bit with q STRIDE (the
+//    callers' butterflies: loads j + q B with j < B, stores base + q NS with
+//    base = (j - j % NS) R + j % NS, first-pass stores R t + q): i0 + q
+//    STRIDE = i0 | q STRIDE and g is linear, so slot = slot(i0) ^ q STRIDE ^
+//    g(q STRIDE >> 4), a compile-time constant per q (an add folded into the
+//    address when STRIDE >= 16).
+// Otherwise the slot is computed per element.
 template <int N, int RM, int ST, int STRIDE, int Q>
 struct CtRun {
-  static constexpr bool add = ct_swizzled(N, ST) ? (STRIDE % 128 == 0) : false;
-  static constexpr bool xr = ct_swizzled(N, ST) && STRIDE == 1 && Q <= 16 && 16 % Q == 0;
+  static constexpr bool pow2(int x) { return x > 0 && (x & (x - 1)) == 0; }
+  static constexpr bool add = ct_swizzled(N, ST) && STRIDE % ct_swz_period(RM) == 0;
+  static constexpr bool lin = ct_swizzled(N, ST) && pow2(STRIDE) && pow2(Q);
   __device__ __forceinline__ static int base(int i0) { return ct_phys<N, RM, ST>(i0); }
   __device__ __forceinline__ static int at(int s0, int i0, int q) {
-    if constexpr (add) return s0 + q * STRIDE;
-    else if constexpr (xr) return s0 ^ q;
-    else return ct_phys<N, RM, ST>(i0 + q * STRIDE);
+    if constexpr (add) {
+      return s0 + q * STRIDE;
+    } else if constexpr (lin) {
+      if constexpr (STRIDE >= 16) return (s0 ^ ct_swz<RM>((q * STRIDE) >> 4)) + q * STRIDE;
+      else return s0 ^ ((q * STRIDE) ^ ct_swz<RM>((q * STRIDE) >> 4));
+    } else {
+      return ct_phys<N, RM, ST>(i0 + q * STRIDE);
+    }
   }
 };
 

@@ -15,8 +15,11 @@
 #define SC_COL_TILE 4
 // Largest column-pass CTA (SC_COL_TILE transforms of length <= 2048).
 #define SC_COL_MAX_THREADS 512
-// Largest radix of the compile-time FFT plans of the row and column passes.
-#define SC_ROW_RADIX 8
+// Row pass: radix-16 plans (16 elements per thread, 3 passes) for rows of
+// 1024 and 2048, radix-8 plans for the other compile-time lengths.
+__host__ __device__ constexpr int row_radix(int W) { return W == 1024 || W == 2048 ? 16 : 8; }
+// Resident row-pass CTAs per SM the kernel is compiled for (register cap).
+__host__ __device__ constexpr int row_min_blocks(int W) { return row_radix(W) == 16 ? 2 : 3; }
 // Column pass: radix-16 plans (16 elements per thread) for long columns,
 // radix-8 plans (8 per thread, twice the threads) for short ones.
 __host__ __device__ constexpr int col_radix(int H) { return H >= 512 ? 16 : 8; }
@@ -159,7 +162,10 @@ __host__ __device__ inline size_t sc_align16(size_t x) { return (x + 15) & ~(siz
 __host__ __device__ inline size_t row_slot_bytes(int mode, int zlen, int W, int Wp) {
   size_t z = sc_align16((size_t)zlen * 8);
   if (mode != ROW_ITER && mode != ROW_ITER_YU && mode != ROW_ADJ && mode != ROW_FIXUP) return z;
-  return z + (size_t)(2 * Wp) * 8 + 2 * sc_align16((size_t)(2 * W) * 4);
+  // staged spectrum rows, then one staged real row pair (V for ROW_ITER, the
+  // state for ROW_FIXUP) or two (Y and U, gV and the mask source)
+  const int nreal = mode == ROW_ITER || mode == ROW_FIXUP ? 1 : 2;
+  return z + (size_t)(2 * Wp) * 8 + nreal * sc_align16((size_t)(2 * W) * 4);
 }
 
 // Shared memory of one column-pass CTA; hlen is the (padded) number of

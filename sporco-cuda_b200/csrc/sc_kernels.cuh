@@ -178,7 +178,7 @@ __device__ __forceinline__ float iter_elem(float x, float s0, float s1, const Ro
 // NW > 0: row length W known at compile time (specialised FFT plan);
 // NW == 0: any W (runtime FFT plan).
 template <int MODE, int NW>
-__global__ void __launch_bounds__(SC_ROW_THREADS, 3)
+__global__ void __launch_bounds__(SC_ROW_THREADS, row_min_blocks(NW))
 row_kernel(RowParams P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red_scratch[(SC_ROW_THREADS / 32) * 5];
@@ -186,7 +186,7 @@ row_kernel(RowParams P) {
   const Geom& G = P.g;
   const int b = blockIdx.y;
   const int W = G.W, Wf = G.Wf, Wp = G.Wp, H = G.H;
-  constexpr int RM = SC_ROW_RADIX;
+  constexpr int RM = row_radix(NW);
   const int g = NW > 0 ? ct_threads(NW, RM) : P.gsz;
   const int S = blockDim.x / g;
   const int s = threadIdx.x / g;
@@ -234,7 +234,9 @@ row_kernel(RowParams P) {
     constexpr bool TWO = MODE == ROW_ITER_YU || ADJ;  // two staged real arrays
     float2* fst = reinterpret_cast<float2*>(slot + sc_align16((size_t)zlen * 8));
     float* ysm = reinterpret_cast<float*>(fst + 2 * (size_t)Wp);
-    float* usm = ysm + sc_align16((size_t)(2 * W) * 4) / 4;
+    // one staged real row pair in the iteration from V (ysm) and the fix-up
+    // (usm = ysm), two otherwise
+    float* usm = TWO ? ysm + sc_align16((size_t)(2 * W) * 4) / 4 : ysm;
     // staged per row pair: V (iteration), Y and U (iteration from Y, U), gV
     // and the mask source (adjoint), the state array (fix-up, into usm)
     const float* Yi = (ADJ ? P.gV : VS ? P.U : P.Y) + (size_t)b * img_real;

@@ -135,7 +135,7 @@ struct Plan {
   FftPlan pw, ph;
   // hot row kernels (iteration, fix-up): compile-time plan when available
   int row_g, row_nblk;
-  size_t row_smem, row_smem_tool;
+  size_t row_smem, row_smem_two, row_smem_tool;  // per CTA: V / fix-up, Y and U, tools
   // setup row kernels: runtime plan
   int rowg_g;
   size_t rowg_smem;
@@ -175,8 +175,8 @@ static int plan_geometry(int B, int M, int H, int W, Plan* pl) {
   if (make_fft_plan(W, &pl->pw) || make_fft_plan(H, &pl->ph))
     return set_status(SC_ERR_UNSUPPORTED, "cannot factor %d or %d", W, H);
   const bool srow = spec_row(W), scol = spec_col(H);
-  const int zlen = srow ? ct_len(W, SC_ROW_RADIX, 1) : W;
-  pl->row_g = srow ? ct_threads(W, SC_ROW_RADIX) : group_size(W);
+  const int zlen = srow ? ct_len(W, row_radix(W), 1) : W;
+  pl->row_g = srow ? ct_threads(W, row_radix(W)) : group_size(W);
   const int S = SC_ROW_THREADS / pl->row_g;
   const long rows = (long)M * H;
   const long npairs = (rows + 1) / 2;
@@ -184,6 +184,7 @@ static int plan_geometry(int B, int M, int H, int W, Plan* pl) {
   long cap = std::max(1L, (long)num_sms() * 8 / B);
   pl->row_nblk = (int)std::min(want, cap);
   pl->row_smem = (size_t)S * row_slot_bytes(ROW_ITER, zlen, W, g.Wp);
+  pl->row_smem_two = (size_t)S * row_slot_bytes(ROW_ITER_YU, zlen, W, g.Wp);
   pl->row_smem_tool = (size_t)S * row_slot_bytes(ROW_FWD_REAL, zlen, W, g.Wp);
   pl->rowg_g = group_size(W);
   pl->rowg_smem = (size_t)(SC_ROW_THREADS / pl->rowg_g) * row_slot_bytes(ROW_FWD_REAL, W, W, g.Wp);
@@ -302,8 +303,8 @@ static int launch_row(const Plan& pl, RowParams rp, int B, cudaStream_t s, int n
   rp.gsz = hot ? pl.row_g : pl.rowg_g;
   rp.nblk = nblk > 0 ? nblk : pl.row_nblk;
   dim3 grid(rp.nblk, B);
-  const size_t smem = (MODE == ROW_ITER || MODE == ROW_ITER_YU || MODE == ROW_ADJ ||
-                       MODE == ROW_FIXUP) ? pl.row_smem
+  const size_t smem = (MODE == ROW_ITER || MODE == ROW_FIXUP) ? pl.row_smem
+                      : (MODE == ROW_ITER_YU || MODE == ROW_ADJ) ? pl.row_smem_two
                       : hot ? pl.row_smem_tool : pl.rowg_smem;
   // one slot (row pair in flight) per rp.gsz threads
   const int threads = (SC_ROW_THREADS / rp.gsz) * rp.gsz;

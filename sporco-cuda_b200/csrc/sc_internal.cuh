@@ -139,16 +139,17 @@ enum RowMode {
 // inverse column FFT.
 enum ColMode {
   COL_SOLVE = 0, COL_FWD = 1, COL_INV = 2, COL_SOLVE_W = 3, COL_ADJ = 4, COL_SOLVE_X = 5,
-  COL_SOLVE_P = 6, COL_SOLVE_C8 = 7, COL_SOLVE_C16 = 8
+  COL_SOLVE_P = 6, COL_SOLVE_C8 = 7, COL_SOLVE_C16 = 8, COL_SOLVE_G16 = 9
 };
 // Filter rows (taps) of the convolution column solves.
 __host__ __device__ constexpr int col_taps(int mode) {
-  return mode == COL_SOLVE_C8 ? 8 : mode == COL_SOLVE_C16 ? 16 : 0;
+  return mode == COL_SOLVE_C8 ? 8 : (mode == COL_SOLVE_C16 || mode == COL_SOLVE_G16) ? 16 : 0;
 }
 // Modes that launch as a cluster over the maps of one column tile.
 __host__ __device__ constexpr bool col_clustered(int mode) {
   return mode == COL_SOLVE || mode == COL_SOLVE_W || mode == COL_SOLVE_X || mode == COL_ADJ ||
-         mode == COL_SOLVE_P || mode == COL_SOLVE_C8 || mode == COL_SOLVE_C16;
+         mode == COL_SOLVE_P || mode == COL_SOLVE_C8 || mode == COL_SOLVE_C16 ||
+         mode == COL_SOLVE_G16;
 }
 
 __host__ __device__ inline size_t sc_align16(size_t x) { return (x + 15) & ~(size_t)15; }

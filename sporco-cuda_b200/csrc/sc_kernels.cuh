@@ -20,10 +20,10 @@
 //                          (row half).
 //   finalize_kernel        FP64 reduction of the partials, residuals, stopping
 //                          test, adaptive rho (host code at cbpdn.cu:405-559).
-//   row_kernel<ROW_FIXUP>  only when rho changed: the row spectra corrected
-//                          by (1 - 1/rsf) rowFFT(U); the next row pass reads
-//                          U scaled by 1/rsf (replaces cublasSgeam at
-//                          cbpdn.cu:546-549).
+//   row_kernel<ROW_FIXUP>  only when rho changed: the row spectra of
+//                          Y - U / rsf, transformed afresh from the state V;
+//                          the next row pass reads U scaled by 1/rsf
+//                          (replaces cublasSgeam at cbpdn.cu:546-549).
 //
 // HBM layout: real maps (B, M, H, W) float32; spectra (B, M, H, Wp) complex64
 // with Wp = W/2+1 rounded up to a multiple of 4 (storage padding only).
@@ -214,6 +214,7 @@ row_kernel(RowParams P) {
       if (st.rsf == 1.0) return;
       rsf_c = (float)(1.0 - 1.0 / st.rsf);
       thr_prev = (float)((double)P.lam[b] / st.rho_prev);
+      uscale = (float)st.uscale;
     }
   }
 
@@ -282,10 +283,13 @@ row_kernel(RowParams P) {
     };
 
     if constexpr (MODE == ROW_FIXUP) {
-      // F += (1 - 1/rsf) rowFFT(U) after a change of rho (U is rescaled by
-      // 1/rsf when the next row pass reads it).  The state rows (U, or V with
-      // U = V - Y) are staged one pair ahead (during the transform), F rows
-      // during the next pair's packing.
+      // After a change of rho the next row pass reads U scaled by 1/rsf, so
+      // the column pass needs the row spectra of Y - U / rsf.  From the state
+      // V (Y = shrinkage of V at the previous threshold, U = V - Y) they are
+      // transformed afresh (reads V, writes F); with Y and U kept apart,
+      // F += (1 - 1/rsf) rowFFT(U) (reads U and F, writes F).  The state
+      // rows are staged one pair ahead (during the transform), F rows during
+      // the next pair's packing.
       const bool vstate = P.vstate != 0;
       auto issue_U = [&](long p) {
         if (p < npairs) {
@@ -298,15 +302,17 @@ row_kernel(RowParams P) {
           }
         }
       };
+      // y - u / rsf from v
+      auto ymu = [&](float v, float y) { return y - (v - y) * uscale; };
       const long p0 = (long)blockIdx.x * S + s;
       issue_U(p0);
-      issue_F(p0);
+      if (!vstate) issue_F(p0);
       cp_async_commit();
       for (long pb = (long)blockIdx.x * S; pb < npairs; pb += pstride) {
         const long p = pb + s;
         const bool valid = p < npairs;
         const bool has1 = valid && (2 * p + 1 < rows);
-        cp_async_wait<0>();  // U(p), F(p)
+        cp_async_wait<0>();  // U(p) (or V(p)), F(p)
         __syncthreads();
         if (valid) {
           if (vstate) {
@@ -315,13 +321,14 @@ row_kernel(RowParams P) {
               const float t0 = thr_prev * w0.w, t1 = thr_prev * w1.w;
               for (int k = t; k < W; k += g) {
                 const float v0 = usm[k], v1 = has1 ? usm[W + k] : 0.f;
-                z[zs(k)] = make_float2(v0 - soft_threshold(v0, t0), v1 - soft_threshold(v1, t1));
+                z[zs(k)] = make_float2(ymu(v0, soft_threshold(v0, t0)),
+                                       ymu(v1, soft_threshold(v1, t1)));
               }
             } else {
               for (int k = t; k < W; k += g) {
                 const float v0 = usm[k], v1 = has1 ? usm[W + k] : 0.f;
-                z[zs(k)] = make_float2(v0 - shrink_y(v0, thr_prev, w0, k),
-                                       has1 ? v1 - shrink_y(v1, thr_prev, w1, k) : 0.f);
+                z[zs(k)] = make_float2(ymu(v0, shrink_y(v0, thr_prev, w0, k)),
+                                       has1 ? ymu(v1, shrink_y(v1, thr_prev, w1, k)) : 0.f);
               }
             }
           } else {
@@ -339,17 +346,22 @@ row_kernel(RowParams P) {
             const float2 Zk = z[zs(k)];
             const float2 Zm = z[zs(k == 0 ? 0 : W - k)];
             const float2 A = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
-            const float2 f0 = fst[k];
-            fa[k] = make_float2(f0.x + rsf_c * A.x, f0.y + rsf_c * A.y);
-            if (has1) {
-              const float2 Bv = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
-              const float2 f1 = fst[Wp + k];
-              fa[Wp + k] = make_float2(f1.x + rsf_c * Bv.x, f1.y + rsf_c * Bv.y);
+            const float2 Bv = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
+            if (vstate) {
+              fa[k] = A;
+              if (has1) fa[Wp + k] = Bv;
+            } else {
+              const float2 f0 = fst[k];
+              fa[k] = make_float2(f0.x + rsf_c * A.x, f0.y + rsf_c * A.y);
+              if (has1) {
+                const float2 f1 = fst[Wp + k];
+                fa[Wp + k] = make_float2(f1.x + rsf_c * Bv.x, f1.y + rsf_c * Bv.y);
+              }
             }
           }
         }
         __syncthreads();  // F staging consumed
-        issue_F(p + pstride);
+        if (!vstate) issue_F(p + pstride);
         cp_async_commit();
       }
       cp_async_wait<0>();
@@ -698,7 +710,7 @@ col_kernel(ColParams P) {
       __syncthreads();
     }
     return;
-  } else if constexpr (MODE == COL_SOLVE_C8 || MODE == COL_SOLVE_C16) {
+  } else if constexpr (MODE == COL_SOLVE_C8 || MODE == COL_SOLVE_C16 || MODE == COL_SOLVE_G16) {
     // Plain solve (d = rho) with the column direction done by direct
     // convolution.  In the row-spectral domain (F = row spectra P_m of
     // (Y - U)_m) filter m is E_m(t, kc), t < Kr (the row spectra of its rows),
@@ -711,7 +723,17 @@ col_kernel(ColParams P) {
     // element), one column FFT pair per tile gives SC = S^ - cb and sc, and
     // pass 2 writes every map's result.  Each thread owns L consecutive rows
     // of one column and slides a window of L values along the column.
+    //
+    // COL_SOLVE_G16: the gradient term, one d(kr, kc) = rho + mu w |G|^2 for
+    // every map.  Pass 1 is the same (sum_m Df_m Z^_m, then SC with d); the
+    // solution x^_m = (rho Z^_m + conj(Df_m) SC) / d splits into
+    //   IFFTcol(x^_m)(r) = IFFTcol(rho Z^_m / d)(r) + sum_t conj(E_m(t)) sc'(r + t),
+    //   sc' = IFFTcol(SC / d):
+    // pass 2 transforms each map's tile forward and back (1/d varies along
+    // the column) and adds the convolution term.  The column spectra are
+    // neither written back nor the dictionary spectra read.
     if constexpr (NH > 0) {
+      constexpr bool GRD = MODE == COL_SOLVE_G16;
       constexpr int KMAX = col_taps(MODE);
       constexpr int L = EPT;  // rows per thread; g L = H for every compiled length
       constexpr int NW = L + KMAX - 1;  // window of the L outputs
@@ -840,7 +862,13 @@ col_kernel(ColParams P) {
         for (int i = 0; i < L; ++i) A[rslot(i) * T + cc] = acc[i];
         __syncthreads();
       }
-      // ------------------------- SC = S^ - cb, sc = IFFTcol(SC) / rho
+      // ------------ SC = S^ - cb, sc = IFFTcol(SC) / rho (GRD: IFFTcol(SC / d))
+      // 1 / d at row kr of this thread's column (GRD)
+      const float wg = GRD ? P.mu * P.wgrd[0] : 0.f;
+      const float gw_col = GRD && colok ? 2.f - 2.f * __ldg(&P.twW[c0 + cc]).x : 0.f;
+      auto inv_d = [&](int kr) -> float {
+        return 1.f / (wg * (gw_col + 2.f - 2.f * __ldg(&P.twH[kr]).x) + rho);
+      };
       fft_any<NH, T, RM>(A + cc, P.ph, P.twH, t, g);
 #pragma unroll
       for (int i = 0; i < EPT; ++i) {
@@ -851,10 +879,20 @@ col_kernel(ColParams P) {
           if (colok) {
             const float2 q = A[sl];  // sum_m Df_m Z^_m
             const float2 Sv = __ldg(&Sh[(size_t)kr * Wp + cc]);
-            const float sd = __ldg(&P.Psum[(size_t)kr * Wp + c0 + cc]) * irho;
-            const float qd = 1.f / (1.f + sd);
-            const float2 cb = make_float2((Sv.x * sd + q.x) * qd, (Sv.y * sd + q.y) * qd);
-            v = make_float2((Sv.x - cb.x) * irho, -(Sv.y - cb.y) * irho);  // conj(SC) / rho
+            if constexpr (GRD) {
+              // cb = (S^ Psum / d + rho q / d) / (1 + Psum / d)
+              const float id = inv_d(kr);
+              const float sd = __ldg(&P.Psum[(size_t)kr * Wp + c0 + cc]) * id;
+              const float qd = 1.f / (1.f + sd);
+              const float2 cb = make_float2((Sv.x * sd + rho * q.x * id) * qd,
+                                            (Sv.y * sd + rho * q.y * id) * qd);
+              v = make_float2((Sv.x - cb.x) * id, -(Sv.y - cb.y) * id);  // conj(SC) / d
+            } else {
+              const float sd = __ldg(&P.Psum[(size_t)kr * Wp + c0 + cc]) * irho;
+              const float qd = 1.f / (1.f + sd);
+              const float2 cb = make_float2((Sv.x * sd + q.x) * qd, (Sv.y * sd + q.y) * qd);
+              v = make_float2((Sv.x - cb.x) * irho, -(Sv.y - cb.y) * irho);  // conj(SC) / rho
+            }
           }
           A[sl] = v;
         }
@@ -873,15 +911,21 @@ col_kernel(ColParams P) {
       const float hs = (float)H;
       float2* Fo = Fi + c0 + cc;
       __syncthreads();  // sc complete before the windows are read
-      // w[j] = sc(r0 + j) / rho: the window of all L outputs, the same for
-      // every map
+      // w[j] = sc(r0 + j) / rho (GRD: sc'(r0 + j)): the window of all L
+      // outputs, the same for every map (GRD: re-read per map, so that it is
+      // not held across the transforms)
       float2 w[NW];
+      auto load_window = [&]() {
 #pragma unroll
-      for (int j = 0; j < NW; ++j)
-        w[j] = (j < L + Kr - 1) ? A[rslot(j) * T + cc] : make_float2(0.f, 0.f);
+        for (int j = 0; j < NW; ++j)
+          w[j] = (j < L + Kr - 1) ? A[rslot(j) * T + cc] : make_float2(0.f, 0.f);
+      };
+      if constexpr (!GRD) load_window();
+      // rho / d at this thread's rows (GRD)
+      const float rho_c = rho;
       it = 0;
       for (int m = m0; m < m1; ++m, ++it) {
-        const float2* cur = (it & 1) ? Ct : Bt;
+        float2* cur = (it & 1) ? Ct : Bt;
         const float2* ecur = Es + (it & 1) * KMAX * T;
         if (m + 1 < m1) {
           issue_tile(Fi + (size_t)(m + 1) * plane, (it & 1) ? Bt : Ct);
@@ -891,10 +935,30 @@ col_kernel(ColParams P) {
         cp_async_wait<1>();  // P(m), E(m)
         __syncthreads();
         float2 o[L];
+        if constexpr (GRD) {
+          // IFFTcol(rho Z^_m / d) as conj(FFT(conj(rho FFT(P_m) / d)))
+          fft_any<NH, T, RM>(cur + cc, P.ph, P.twH, t, g);
 #pragma unroll
-        for (int i = 0; i < L; ++i) {
-          const float2 pv = cur[rslot(i) * T + cc];
-          o[i] = make_float2(hs * pv.x, hs * pv.y);
+          for (int i = 0; i < L; ++i) {
+            const int sl = rslot(i) * T + cc;
+            const float f = rho_c * inv_d(r0 + i);
+            const float2 z = cur[sl];
+            cur[sl] = make_float2(f * z.x, -f * z.y);
+          }
+          __syncthreads();
+          fft_any<NH, T, RM>(cur + cc, P.ph, P.twH, t, g);
+#pragma unroll
+          for (int i = 0; i < L; ++i) {
+            const float2 v = cur[rslot(i) * T + cc];
+            o[i] = make_float2(v.x, -v.y);
+          }
+          load_window();
+        } else {
+#pragma unroll
+          for (int i = 0; i < L; ++i) {
+            const float2 pv = cur[rslot(i) * T + cc];
+            o[i] = make_float2(hs * pv.x, hs * pv.y);
+          }
         }
 #pragma unroll
         for (int tp = 0; tp < KMAX; ++tp) {

@@ -552,6 +552,7 @@ struct Solve {
     // Plain problems with short filters (Kr <= 16 rows) and a compiled column
     // length take the convolution column solve.
     col_mode = per_map_d ? COL_SOLVE_W
+               : (p->grd && spec_col(pl.g.H) && p->Kr <= 16) ? COL_SOLVE_G16
                : p->grd  ? COL_SOLVE
                : (spec_col(pl.g.H) && p->Kr <= 8)  ? COL_SOLVE_C8
                : (spec_col(pl.g.H) && p->Kr <= 16) ? COL_SOLVE_C16
@@ -654,6 +655,7 @@ struct Solve {
       case COL_SOLVE: return launch_col<COL_SOLVE>(pl, cp, B, s, G);
       case COL_SOLVE_C8: return launch_col<COL_SOLVE_C8>(pl, cp, B, s, G);
       case COL_SOLVE_C16: return launch_col<COL_SOLVE_C16>(pl, cp, B, s, G);
+      case COL_SOLVE_G16: return launch_col<COL_SOLVE_G16>(pl, cp, B, s, G);
       default: return launch_col<COL_SOLVE_P>(pl, cp, B, s, G);
     }
   }
@@ -663,6 +665,7 @@ struct Solve {
       case COL_SOLVE: return (const void*)col_fn<COL_SOLVE>(pl.g.H);
       case COL_SOLVE_C8: return (const void*)col_fn<COL_SOLVE_C8>(pl.g.H);
       case COL_SOLVE_C16: return (const void*)col_fn<COL_SOLVE_C16>(pl.g.H);
+      case COL_SOLVE_G16: return (const void*)col_fn<COL_SOLVE_G16>(pl.g.H);
       default: return (const void*)col_fn<COL_SOLVE_P>(pl.g.H);
     }
   }

@@ -91,12 +91,13 @@ def test_benchmark_shape_256_fixed_rho():
 
 
 # Column lengths with compiled transform plans and filters of 9..16 rows take
-# the convolution column solve with 16 taps; 48 rows with 13-row filters
-# wrap the circular convolution over more than a quarter of the column;
-# filters of 17+ rows take the transform solve.
+# the convolution column solve with 16 taps (with the gradient term: its
+# transform-and-convolution form); 48 rows with 13-row filters wrap the
+# circular convolution over more than a quarter of the column; filters of
+# 17+ rows take the transform solve.
 @pytest.mark.gpu
 @pytest.mark.parametrize("shape", [(96, 64, 16), (48, 40, 13), (64, 48, 17), (128, 31, 12)])
-@pytest.mark.parametrize("variant", ["cbpdn", "cbpdnmsk"])
+@pytest.mark.parametrize("variant", ["cbpdn", "cbpdnmsk", "cbpdngrd"])
 def test_column_solve_filter_lengths(shape, variant):
     H, W, K = shape
     D, S = _synth(H, W, 6, K, 0.02, 99)
@@ -105,6 +106,12 @@ def test_column_solve_filter_lengths(shape, variant):
            "rho": float(np.float32(50 * np.float32(lam) + 1)), "AutoRho": {"Enabled": False}}
     if variant == "cbpdn":
         X, Xo = cb.cbpdn(D, S, lam, opt), O.cbpdn(D, S, lam, opt)
+    elif variant == "cbpdngrd":
+        mu = 0.2
+        X, Xo = cb.cbpdngrd(D, S, lam, mu, opt), O.cbpdngrd(D, S, lam, mu, opt)
+        assert _rel(X, Xo) < REL_TOL
+        _check_functional(D, S, X, Xo, lam, mu=mu, grd=True)
+        return
     else:
         Wm = (np.random.default_rng(4).random(S.shape) < 0.7).astype(np.float32)
         X, Xo = cb.cbpdnmsk(D, S * Wm, Wm, lam, opt), O.cbpdnmsk(D, S * Wm, Wm, lam, opt)

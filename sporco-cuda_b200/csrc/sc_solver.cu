@@ -338,7 +338,10 @@ static int resident_clusters(const void* fn, int NT, size_t smem, int G, int* ou
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   int n = 0;
-  CU_TRY(cudaOccupancyMaxActiveClusters(&n, fn, &cfg));
+  if (cudaOccupancyMaxActiveClusters(&n, fn, &cfg) != cudaSuccess) {
+    cudaGetLastError();  // a cluster size this device does not offer: none resident
+    n = 0;
+  }
   cache.push_back({dev, fn, G, smem, n});
   *out = n;
   return SC_OK;
@@ -381,10 +384,25 @@ struct TunedG {
 };
 static std::vector<TunedG> g_tuned;
 
-// The autotuner runs unless SPORCO_B200_AUTOTUNE is set to 0.
+// The autotuner runs unless SPORCO_B200_AUTOTUNE is set to 0; set to
+// "verbose" it also reports its trial times on stderr.
 static bool autotune_enabled() {
   const char* e = getenv("SPORCO_B200_AUTOTUNE");
   return !(e && e[0] == '0');
+}
+static bool autotune_verbose() {
+  const char* e = getenv("SPORCO_B200_AUTOTUNE");
+  return e && strcmp(e, "verbose") == 0;
+}
+
+// SPORCO_B200_COL_CLUSTER=G fixes the column pass's cluster size (no model,
+// no autotuner) where G CTAs fit (e.g. to profile a process with the cluster
+// size an unprofiled run chose); 0 or unset: no override.
+static int forced_cluster(int M) {
+  const char* e = getenv("SPORCO_B200_COL_CLUSTER");
+  if (!e || !*e) return 0;
+  const int G = atoi(e);
+  return G >= 1 && G <= 16 ? std::min(G, M) : 0;
 }
 
 static bool tuned_size(const void* fn, const Geom& g, int* G) {
@@ -406,9 +424,14 @@ static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s, int f
     ColFn fn = col_fn<MODE>(cp.g.H);
     int st = prepare_fn((const void*)fn, true);
     if (st) return st;
-    int G = force_G;
+    int G = force_G > 0 ? force_G : forced_cluster(cp.g.M);
     const size_t smem = col_smem_bytes(MODE, pl.col_hlen);
     const long units = (long)pl.col_ntiles * B;
+    if (G > 0 && force_G <= 0) {
+      int n = 0;  // the override only where such a cluster fits
+      if ((st = resident_clusters((const void*)fn, pl.col_NT, smem, G, &n))) return st;
+      if (n < 1) G = 0;
+    }
     if (G <= 0 && !tuned_size((const void*)fn, cp.g, &G) &&
         (st = cluster_size((const void*)fn, pl.col_NT, smem, cp.g.M, units, &G)))
       return st;
@@ -680,7 +703,7 @@ struct Solve {
     const Geom& g = pl.g;
     const void* fn = iter_col_fn();
     int G0 = 0;
-    if (tuned_size(fn, g, &G0)) return SC_OK;
+    if (forced_cluster(g.M) > 0 || tuned_size(fn, g, &G0)) return SC_OK;
     int st = prepare_fn(fn, true);
     if (st) return st;
     const size_t smem = col_smem_bytes(col_mode, pl.col_hlen);
@@ -712,6 +735,11 @@ struct Solve {
     int bi = 0;
     for (int i = 1; i < nc; ++i)
       if (best_ms[i] < best_ms[bi]) bi = i;
+    if (autotune_verbose()) {
+      fprintf(stderr, "sporco_b200 autotune: column pass %dx%d M=%d:", g.H, g.W, g.M);
+      for (int i = 0; i < nc; ++i) fprintf(stderr, " G=%d %.3f ms", cand[i], best_ms[i]);
+      fprintf(stderr, " -> G=%d\n", cand[bi]);
+    }
     int dev = 0;
     CU_TRY(cudaGetDevice(&dev));
     g_tuned.push_back({dev, fn, g.H, g.W, g.M, cand[bi]});

@@ -308,6 +308,62 @@ row_kernel(RowParams P) {
       issue_U(p0);
       if (!vstate) issue_F(p0);
       cp_async_commit();
+      if constexpr (NW > 0 && ct_reg_edges(NW, RM)) {
+        if (vstate) {
+          // Register hand-over: thread t computes the elements t + g m of the
+          // pair's transform input and runs the first pass on registers.
+          constexpr int EM = NW / ct_threads(NW, RM);
+          constexpr int NP = ct_plan(NW, RM).np;
+          for (long pb = (long)blockIdx.x * S; pb < npairs; pb += pstride) {
+            const long p = pb + s;
+            const bool valid = p < npairs;
+            const bool has1 = valid && (2 * p + 1 < rows);
+            cp_async_wait<0>();  // V(p)
+            __syncthreads();
+            float2 v[EM];
+            if (valid) {
+              const RowW w0 = roww(2 * p, true), w1 = roww(2 * p + 1, has1);
+              if (!w0.mrow && !w1.mrow && !w0.wr && !w1.wr) {
+                const float t0 = thr_prev * w0.w, t1 = thr_prev * w1.w;
+#pragma unroll
+                for (int m = 0; m < EM; ++m) {
+                  const int k = t + g * m;
+                  const float v0 = usm[k], v1 = has1 ? usm[W + k] : 0.f;
+                  v[m] = make_float2(ymu(v0, soft_threshold(v0, t0)),
+                                     ymu(v1, soft_threshold(v1, t1)));
+                }
+              } else {
+#pragma unroll
+                for (int m = 0; m < EM; ++m) {
+                  const int k = t + g * m;
+                  const float v0 = usm[k], v1 = has1 ? usm[W + k] : 0.f;
+                  v[m] = make_float2(ymu(v0, shrink_y(v0, thr_prev, w0, k)),
+                                     has1 ? ymu(v1, shrink_y(v1, thr_prev, w1, k)) : 0.f);
+                }
+              }
+            } else {
+#pragma unroll
+              for (int m = 0; m < EM; ++m) v[m] = make_float2(0.f, 0.f);
+            }
+            ct_first_from_regs<NW, RM, 1>(z, v, t);  // the staged rows are consumed
+            issue_U(p + pstride);
+            cp_async_commit();
+            fft_ct_passes<NW, RM, ct_threads(NW, RM), 1, 1, NP>(z, P.twW, t);
+            if (valid) {
+              float2* fa = Fi + 2 * p * Wp;
+              for (int k = t; k < Wf; k += g) {
+                const float2 Zk = z[zs(k)];
+                const float2 Zm = z[zs(k == 0 ? 0 : W - k)];
+                fa[k] = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
+                if (has1) fa[Wp + k] = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
+              }
+            }
+            __syncthreads();
+          }
+          cp_async_wait<0>();
+          return;
+        }
+      }
       for (long pb = (long)blockIdx.x * S; pb < npairs; pb += pstride) {
         const long p = pb + s;
         const bool valid = p < npairs;

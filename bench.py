@@ -136,9 +136,20 @@ def graded_kernel_bytes(H, W, M):
 
 # DRAM bytes per launch and map measured by ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum) for kernels whose traffic grows in proportion to the
-# maps; from the 2048x2048, M=24 capture summarised in
-# profiles/launch_list_2048x2048_m24.md.
-MEASURED_TRAFFIC_PER_MAP = {(2048, 2048): {"row_kernel": (807e6 + 744e6) / 24}}
+# maps, with the capture they come from: the 2048x2048, M=24 launch list
+# (profiles/launch_list_2048x2048_m24.md) and, at 512x512, the mean of the
+# two column solves of the default bench, M=100 and 101 maps
+# (profiles/col_kernel_conv_solves_512x512_m100.md).
+MEASURED_TRAFFIC_PER_MAP = {
+    (2048, 2048): {"row_kernel": ((807e6 + 744e6) / 24,
+                                  "ncu capture at 2048x2048, M=24, scaled by the maps"),
+                   "col_kernel": ((827.5e6 + 352.6e6) / 24,
+                                  "ncu capture at 2048x2048, M=24 (clusters of 2), "
+                                  "scaled by the maps")},
+    (512, 512): {"col_kernel": (((216.1e6 + 49.3e6) + (218.5e6 + 56.2e6)) / 2 / 100,
+                                "ncu captures at 512x512, M=100 (default bench), "
+                                "mean of the gradient and masked column solves")},
+}
 
 
 def design_bytes(H, W, M, variant="cbpdn", K=None):
@@ -421,14 +432,13 @@ def run_ours(args, cfg, rank, world, local_rank):
             gb += graded_kernel_bytes(cfg["H"], cfg["W"], M).get(name, 0.0)
         gb /= len(cfg["variants"])
         t = kern[name]["ms_per_launch"]
-        tr = MEASURED_TRAFFIC_PER_MAP.get((cfg["H"], cfg["W"]), {}).get(name)
+        tr, src = MEASURED_TRAFFIC_PER_MAP.get((cfg["H"], cfg["W"]), {}).get(name, (None, None))
         dom = {"name": name, "share": kern[name]["share"],
                "algorithmic_bytes_per_launch": gb,
                "achieved": gb / (t / 1e3) / 1e9 if t > 0 and gb > 0 else None,
                "frac": gb / (t / 1e3) / 1e9 / peak if t > 0 and gb > 0 else None,
                "traffic": tr * cfg["M"] if tr else None,
-               "traffic_source": "ncu capture at 2048x2048, M=24, scaled by the maps"
-               if tr else None}
+               "traffic_source": src}
     out = None
     if rank == 0:
         cpu = cpu_sample(cfg, D.cpu().numpy(), Sn, Wn) if world == 1 and not args.no_cpu else None
@@ -450,7 +460,9 @@ def run_ours(args, cfg, rank, world, local_rank):
                          "finalize_kernel + fixup_kernel)",
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": achieved / peak if achieved else None,
-                         "traffic": None,
+                         # DRAM bytes per launch of the dominant kernel (ncu)
+                         "traffic": dom["traffic"] if dom else None,
+                         "traffic_kernel": dom["name"] if dom and dom["traffic"] else None,
                          "algorithmic_bytes_per_iteration": bytes_it / n_solve_it,
                          "design_bytes_per_iteration": design_it / n_solve_it,
                          "design_frac": (design_it / (ms / 1e3) / 1e9 / peak)

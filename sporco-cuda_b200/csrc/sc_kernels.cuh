@@ -58,6 +58,17 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// Programmatic dependent launch: the iteration's kernels are launched with
+// programmatic stream serialisation, so a kernel's CTAs can be scheduled
+// while the kernel before it in the stream drains.  Each waits here for that
+// kernel to complete (its writes visible) before touching global memory,
+// then lets the next kernel be scheduled.  Launched without the attribute,
+// both instructions return at once.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
 // Soft threshold as the reference's shrink kernels compute it
 // (cbpdn_kernels.cu:129-311): sign(v) max(|v| - t, 0), t may be negative.
 __device__ __forceinline__ float soft_threshold(float v, float t) {
@@ -182,6 +193,7 @@ __global__ void __launch_bounds__(SC_ROW_THREADS, row_min_blocks(NW))
 row_kernel(RowParams P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red_scratch[(SC_ROW_THREADS / 32) * 5];
+  pdl_enter();
 
   const Geom& G = P.g;
   const int b = blockIdx.y;
@@ -707,6 +719,7 @@ row_kernel(RowParams P) {
 template <int MODE, int NH>
 __global__ void __launch_bounds__(SC_COL_MAX_THREADS)
 col_kernel(ColParams P) {
+  pdl_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int T = SC_COL_TILE;
   constexpr int RM = col_radix(NH);
@@ -1611,6 +1624,7 @@ __global__ void psum_kernel(const float2* __restrict__ Dh, float* __restrict__ P
 // 2010 3.3-3.4; Wohlberg 2015).
 __global__ void finalize_kernel(const double* __restrict__ partials, int nblk,
                                 ImgState* st, FinParams F) {
+  pdl_enter();
   __shared__ double scratch[(256 / 32) * 5];
   const int b = blockIdx.x;
   ImgState& S = st[b];

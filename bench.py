@@ -3,13 +3,15 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--config C] [--impl ours|reference]
 
-Workload (default --config 1): one 512x512 float32 image, 100 unit-norm 12x12
-Gaussian filters, S synthesised from Bernoulli(0.005) x N(0,1) sparse maps plus
-N(0, 0.01^2) noise and mean-subtracted (seed 12346); a step is one cbpdngrd solve
-(lambda 0.05, mu 0.1) plus one cbpdnmsk solve (Bernoulli(0.7) mask, 101 maps
-with the AMS impulse), AutoRho on, 500 ADMM iterations each (no early stop).
-Configs 0 (256x256, M=64, 200 iterations, fixed rho) and 4 (2048x2048,
-M=256, 100 iterations, AutoRho) are selectable.  Data are synthetic.
+Workload (default --config 4, the largest single-GPU configuration): one
+2048x2048 float32 image, 256 unit-norm 16x16 Gaussian filters, S synthesised
+from Bernoulli(0.01) x N(0,1) sparse maps plus N(0, 0.01^2) noise and
+mean-subtracted (seeded); a step is one cbpdn solve (lambda 0.02, AutoRho on)
+of 100 ADMM iterations (no early stop).  Configs 0 (256x256, M=64, fixed rho),
+1 (cbpdngrd + cbpdnmsk at 512x512, M=100), 2 (batched, 64 uneven images) and
+3 (forward + adjoint of 200 unrolled iterations) are selectable.  Data are
+synthetic, drawn on the host (torch CPU generator, float64 FFTs) so that both
+arms see the same problem.
 
 Printed JSON line (rank 0): ``value`` = ADMM iterations per second with inputs
 resident in device memory, summed over ranks (each rank runs an independent
@@ -19,11 +21,14 @@ copies inside the timed region); ``roofline`` = algorithmic HBM bytes of one
 ADMM iteration (4R + 6C + 2C_D, R = 4 M H W, C = C_D = 8 M H (W/2+1)) over the
 measured device time of one iteration (CUDA events around every kernel of the
 timed solves), against the measured HBM copy bandwidth; ``cpu_baseline`` = the
-FP64 CPU restatement of the algorithm timed on this host on a bounded sample.
+FP64 CPU restatement of the algorithm timed on this host on a bounded sample
+(the first n iterations); ``rel_err`` = the GPU solver's coefficient maps and
+functional after those n iterations against that FP64 run.
 
 ``--impl reference`` times the reference algorithm's CPU implementation (the
-FP64 restatement; the reference ships no CPU solver of its own) on this host's
-cores, on the same workload, one bounded sample per step.
+FP64 restatement with every host thread; the reference ships no CPU solver of
+its own) on the same workload: each step continues one solve by a bounded
+number of iterations.  It loads nothing of this package.
 """
 
 from __future__ import annotations
@@ -53,13 +58,14 @@ METRIC = ("ADMM iters/s & HBM GB/s (plain vs batched vs fwd+adjoint), "
 CONFIGS = {
     0: dict(workload="cbpdn 256x256 M=64 8x8, 200 iterations, fixed rho",
             H=256, W=256, M=64, K=8, density=0.01, lmbda=0.05, mu=0.0,
-            variants=["cbpdn"], iters=200, autorho=False, mask_p=None),
+            variants=["cbpdn"], iters=200, autorho=False, mask_p=None, check_iters=40),
     1: dict(workload="cbpdngrd + cbpdnmsk 512x512 M=100 12x12, 500 iterations, AutoRho",
             H=512, W=512, M=100, K=12, density=0.005, lmbda=0.05, mu=0.1,
-            variants=["cbpdngrd", "cbpdnmsk"], iters=500, autorho=True, mask_p=0.7),
+            variants=["cbpdngrd", "cbpdnmsk"], iters=500, autorho=True, mask_p=0.7,
+            check_iters=20),
     4: dict(workload="cbpdn 2048x2048 M=256 16x16, 100 iterations, AutoRho",
             H=2048, W=2048, M=256, K=16, density=0.01, lmbda=0.02, mu=0.0,
-            variants=["cbpdn"], iters=100, autorho=True, mask_p=None),
+            variants=["cbpdn"], iters=100, autorho=True, mask_p=None, check_iters=2),
     2: dict(workload="batched cbpdnmsk: 64 images, sides from {128..1024} (H, W independent), "
                      "M=64 12x12, per-image masks and lambda, AutoRho, RelStopTol 1e-4, cap 1000",
             H=None, W=None, M=64, K=12, density=0.005, lmbda=None, mu=0.0,
@@ -74,12 +80,13 @@ CONFIGS = {
     # kernel profiles
     10: dict(workload="cbpdn 1024x1024 M=256 16x16, 20 iterations, AutoRho (profiling case)",
              H=1024, W=1024, M=256, K=16, density=0.01, lmbda=0.02, mu=0.0,
-             variants=["cbpdn"], iters=20, autorho=True, mask_p=None),
+             variants=["cbpdn"], iters=20, autorho=True, mask_p=None, check_iters=3),
     # small 2048x2048 case for kernel profiles (2 GB on the device)
     9: dict(workload="cbpdn 2048x2048 M=24 16x16, 20 iterations, AutoRho (profiling case)",
             H=2048, W=2048, M=24, K=16, density=0.01, lmbda=0.02, mu=0.0,
-            variants=["cbpdn"], iters=20, autorho=True, mask_p=None),
+            variants=["cbpdn"], iters=20, autorho=True, mask_p=None, check_iters=5),
 }
+DEFAULT_CONFIG = 4
 
 
 # ---------------------------------------------------------------- helpers --
@@ -93,9 +100,10 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def opt_for(cfg, variant):
+def opt_for(cfg, variant, iters=None):
     lam = np.float32(cfg["lmbda"])
-    opt = {"Verbose": False, "MaxMainIter": cfg["iters"], "RelStopTol": 0.0, "AbsStopTol": 0.0,
+    opt = {"Verbose": False, "MaxMainIter": iters or cfg["iters"], "RelStopTol": 0.0,
+           "AbsStopTol": 0.0,
            "RelaxParam": 1.8, "L1Weight": 1.0, "GradWeight": 1.0,
            "AutoRho": {"Enabled": cfg["autorho"], "Period": 1, "Scaling": 1000.0,
                        "RsdlRatio": 1.2, "RsdlTarget": None, "AutoScaling": True,
@@ -135,20 +143,19 @@ def graded_kernel_bytes(H, W, M):
 
 
 # DRAM bytes per launch and map measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum) for kernels whose traffic grows in proportion to the
-# maps, with the capture they come from: the 2048x2048, M=24 launch list
-# (profiles/launch_list_2048x2048_m24.md) and, at 512x512, the mean of the
-# two column solves of the default bench, M=100 and 101 maps
-# (profiles/col_kernel_conv_solves_512x512_m100.md).
+# dram__bytes_write.sum, one-kernel captures) for kernels whose traffic grows
+# in proportion to the maps, with the capture each comes from (kernels as of
+# the commit named there).
 MEASURED_TRAFFIC_PER_MAP = {
     (2048, 2048): {"row_kernel": ((807e6 + 744e6) / 24,
-                                  "ncu capture at 2048x2048, M=24, scaled by the maps"),
+                                  "ncu capture at 2048x2048, M=24, scaled by the maps "
+                                  "(captured at commit 2d8664f)"),
                    "col_kernel": ((827.5e6 + 352.6e6) / 24,
                                   "ncu capture at 2048x2048, M=24 (clusters of 2), "
-                                  "scaled by the maps")},
+                                  "scaled by the maps (captured at commit 2d8664f)")},
     (512, 512): {"col_kernel": (((216.1e6 + 49.3e6) + (218.5e6 + 56.2e6)) / 2 / 100,
-                                "ncu captures at 512x512, M=100 (default bench), "
-                                "mean of the gradient and masked column solves")},
+                                "ncu captures at 512x512, M=100, mean of the gradient and "
+                                "masked column solves (captured at commit 2d8664f)")},
 }
 
 
@@ -170,38 +177,38 @@ def design_bytes(H, W, M, variant="cbpdn", K=None):
     return 2 * R + 2 * Cs + col
 
 
-def synth(cfg, seed, device):
-    """Unit-norm Gaussian filters, sparse maps, S = sum_m d_m * x_m + noise,
-    mean-subtracted.  Spectral products use this package's own FFT."""
+def synth(cfg, seed):
+    """Unit-norm Gaussian filters D (M, K, K), S = sum_m d_m * x_m + noise
+    (x_m Bernoulli(density) x N(0, 1), drawn as that many uniformly placed
+    nonzeros), mean-subtracted, and the Bernoulli observation mask of the
+    masked configurations; float32 numpy arrays.  Drawn with the torch CPU
+    generator and float64 FFTs on the host, so that every arm of the
+    benchmark (including the reference arm, which loads nothing of this
+    package) solves the same problem."""
     import torch
-    from sporco_cuda import _lib
     H, W, M, K = cfg["H"], cfg["W"], cfg["M"], cfg["K"]
-    g = torch.Generator(device=device).manual_seed(seed)
-    D = torch.randn((M, K, K), generator=g, device=device)
+    g = torch.Generator().manual_seed(seed)
+    D = torch.randn((M, K, K), generator=g, dtype=torch.float64)
     D /= torch.sqrt(torch.sum(D * D, dim=(1, 2), keepdim=True))
-    Dp = torch.zeros((M, H, W), device=device)
-    Dp[:, :K, :K] = D
-    X0 = (torch.rand((M, H, W), generator=g, device=device) < cfg["density"]).float() * \
-        torch.randn((M, H, W), generator=g, device=device)
-    Wf = W // 2 + 1
-    s = torch.cuda.current_stream().cuda_stream
-    Df = torch.empty((M, H, Wf), dtype=torch.complex64, device=device)
-    Xf = torch.empty((M, H, Wf), dtype=torch.complex64, device=device)
-    _lib.check(_lib.sc_rfft2(C.c_void_p(Dp.data_ptr()), C.c_void_p(Df.data_ptr()), M, H, W,
-                             C.c_void_p(s)))
-    _lib.check(_lib.sc_rfft2(C.c_void_p(X0.data_ptr()), C.c_void_p(Xf.data_ptr()), M, H, W,
-                             C.c_void_p(s)))
-    Sf = torch.sum(Df * Xf, dim=0).contiguous()
-    S = torch.empty((1, H, W), device=device)
-    _lib.check(_lib.sc_irfft2(C.c_void_p(Sf.data_ptr()), C.c_void_p(S.data_ptr()), 1, H, W,
-                              C.c_void_p(s)))
-    S = S[0] + 0.01 * torch.randn((H, W), generator=g, device=device)
+    Sf = torch.zeros((H, W // 2 + 1), dtype=torch.complex128)
+    for m0 in range(0, M, 16):
+        m1 = min(M, m0 + 16)
+        n = (m1 - m0) * H * W
+        nnz = int(round(cfg["density"] * n))
+        X0 = torch.zeros(n, dtype=torch.float64)
+        X0.index_put_((torch.randint(0, n, (nnz,), generator=g),),
+                      torch.randn(nnz, generator=g, dtype=torch.float64), accumulate=True)
+        Dp = torch.zeros((m1 - m0, H, W), dtype=torch.float64)
+        Dp[:, :K, :K] = D[m0:m1]
+        Sf += torch.sum(torch.fft.rfft2(Dp) * torch.fft.rfft2(X0.reshape(m1 - m0, H, W)), dim=0)
+    S = torch.fft.irfft2(Sf, s=(H, W)) + 0.01 * torch.randn((H, W), generator=g,
+                                                           dtype=torch.float64)
     S = S - S.mean()
     mask = None
     if cfg["mask_p"] is not None:
-        mask = (torch.rand((H, W), generator=g, device=device) < cfg["mask_p"]).float()
-    del Dp, X0, Df, Xf, Sf
-    return D.contiguous(), S.contiguous(), mask
+        mask = (torch.rand((H, W), generator=g, dtype=torch.float64) < cfg["mask_p"]).numpy() \
+            .astype(np.float32)
+    return D.numpy().astype(np.float32), S.numpy().astype(np.float32), mask
 
 
 class ClockSampler:
@@ -261,40 +268,48 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_sample(cfg, D, S, mask, budget_s=15.0):
-    """FP64 CPU restatement on this host: iterations/s on a bounded sample of
-    the workload (the first n ADMM iterations of each variant)."""
-    from oracle import cbpdn_oracle as O
-    Dn = np.ascontiguousarray(np.moveaxis(D, 0, 2))
-    lam = cfg["lmbda"]
+def _oracle_args(cfg, variant, D, S, mask, iters):
+    """Arguments of the oracle entry point for one variant: D (K, K, M)."""
+    Dk = np.ascontiguousarray(np.moveaxis(D, 0, 2))
+    opt = opt_for(cfg, variant, iters)
+    if variant == "cbpdnmsk":
+        return dict(variant=variant, D=Dk, S=S * mask, lmbda=cfg["lmbda"], opt=opt, W=mask)
+    return dict(variant=variant, D=Dk, S=S, lmbda=cfg["lmbda"], opt=opt, mu=cfg["mu"])
 
-    def run(variant, n):
-        opt = opt_for(cfg, variant)
-        opt["MaxMainIter"] = n
-        if variant == "cbpdn":
-            O.cbpdn(Dn, S, lam, opt)
-        elif variant == "cbpdngrd":
-            O.cbpdngrd(Dn, S, lam, cfg["mu"], opt)
-        elif variant == "cbpdnmsk":
-            O.cbpdnmsk(Dn, S * mask, mask, lam, opt)
+
+def cpu_leg(cfg, D, S, mask, iters):
+    """The FP64 CPU restatement (map-chunked, torch on every host thread) on
+    a bounded sample of the workload: the first `iters` ADMM iterations of
+    each variant.  Returns the cpu_baseline record and, per variant, the
+    FP64 coefficient maps (H, W, M) and the run's information."""
+    import torch
+    from oracle import cbpdn_oracle_torch as OT
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    out = {}
     t0 = time.perf_counter()
     for v in cfg["variants"]:
-        run(v, 1)
-    per = (time.perf_counter() - t0) / len(cfg["variants"])
-    n = max(1, int(budget_s / max(per, 1e-6) / len(cfg["variants"])))
-    n = min(n, cfg["iters"])
-    t0 = time.perf_counter()
-    for v in cfg["variants"]:
-        run(v, n)
+        out[v] = OT.solve(**_oracle_args(cfg, v, D, S, mask, iters))
     dt = time.perf_counter() - t0
-    total = n * len(cfg["variants"])
-    return {"value": total / dt, "unit": "iter/s", "cores": os.cpu_count(), "kind": "port",
-            "sample": "%s: first %d ADMM iterations of each of %s (FP64 numpy/scipy, "
-                      "scipy.fft workers=%d)" % (cfg["workload"], n, "+".join(cfg["variants"]),
-                                                 os.cpu_count())}
+    total = iters * len(cfg["variants"])
+    rec = {"value": total / dt, "unit": "iter/s", "cores": threads, "kind": "port",
+           "sample": "%s: the first %d ADMM iterations of %s from zero (FP64 restatement, "
+                     "maps in chunks of 16, torch CPU with %d threads; set-up included)"
+                     % (cfg["workload"], iters, " and ".join(cfg["variants"]), threads)}
+    return rec, out
 
 
 # ------------------------------------------------------------------ arms --
+
+def config_dict(cfg, world):
+    """The `config` object of the JSON line (the same in both arms)."""
+    return {"workload": cfg["workload"], "H": cfg["H"], "W": cfg["W"], "M": cfg["M"],
+            "K": cfg["K"], "iterations_per_solve": cfg["iters"],
+            "solves_per_step": len(cfg["variants"]),
+            "parallelism": "replicas%d" % world if world > 1 else "single",
+            "l2": "working set larger than L2 (no flush)" if
+            graded_bytes(cfg["H"], cfg["W"], cfg["M"]) > 126e6 else "working set fits in L2"}
+
 
 def run_ours(args, cfg, rank, world, local_rank):
     import torch
@@ -302,9 +317,13 @@ def run_ours(args, cfg, rank, world, local_rank):
     from sporco_cuda import _lib, replicas
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    D, S, mask = synth(cfg, 12345 + args.config, dev)
+    Dh, Sh, maskh = synth(cfg, 12345 + args.config + 1000 * rank)
+    D = torch.from_numpy(Dh).to(dev)
+    S = torch.from_numpy(Sh).to(dev)
+    mask = torch.from_numpy(maskh).to(dev) if maskh is not None else None
     lam = cfg["lmbda"]
-    # device-resident solves
+    # device-resident solves (one for the timed steps, one with an event pair
+    # around every kernel launch for the per-kernel split)
     solves = []
     for v in cfg["variants"]:
         opt = opt_for(cfg, v)
@@ -371,32 +390,30 @@ def run_ours(args, cfg, rank, world, local_rank):
     value = replicas.job_rate(iters_per_step * args.steps, ms)
     ms = replicas.max_over_ranks(ms)
 
-    # end-to-end through the reference-facing API (numpy host buffers)
-    Dn = np.ascontiguousarray(D.permute(1, 2, 0).cpu().numpy())
-    Sn = S.cpu().numpy()
-    Wn = mask.cpu().numpy() if mask is not None else None
+    # end to end through the reference-facing API (numpy host buffers in and
+    # out, every host<->device copy inside the timed region)
+    Dn = np.ascontiguousarray(np.moveaxis(Dh, 0, 2))
 
     def e2e_step():
         for v in cfg["variants"]:
             opt = opt_for(cfg, v)
             if v == "cbpdn":
-                cb.cbpdn(Dn, Sn, lam, opt)
+                cb.cbpdn(Dn, Sh, lam, opt)
             elif v == "cbpdngrd":
-                cb.cbpdngrd(Dn, Sn, lam, cfg["mu"], opt)
+                cb.cbpdngrd(Dn, Sh, lam, cfg["mu"], opt)
             else:
-                cb.cbpdnmsk(Dn, Sn * Wn, Wn, lam, opt)
-    e_steps = max(1, min(args.steps, 3))
+                cb.cbpdnmsk(Dn, Sh * maskh, maskh, lam, opt)
     if not args.no_e2e:
         e2e_step()
         barrier()
         t0 = time.perf_counter()
-        for _ in range(e_steps):
+        for _ in range(args.steps):
             e2e_step()
         barrier()
         e_ms = (time.perf_counter() - t0) * 1e3
+        e_value = replicas.job_rate(iters_per_step * args.steps, e_ms)
     else:
-        e_ms = float("nan")
-    e_value = replicas.job_rate(iters_per_step * e_steps, e_ms)
+        e_value = None
     h2d = d2h = 0
     for v in cfg["variants"]:
         M = cfg["M"] + (1 if v == "cbpdnmsk" else 0)
@@ -439,21 +456,53 @@ def run_ours(args, cfg, rank, world, local_rank):
                "frac": gb / (t / 1e3) / 1e9 / peak if t > 0 and gb > 0 else None,
                "traffic": tr * cfg["M"] if tr else None,
                "traffic_source": src}
+
+    # CPU baseline and relative error: the FP64 restatement's first n
+    # iterations (rank 0 of a one-GPU run) against the same n iterations of
+    # the device solver
+    cpu = rel_err = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        n = cfg["check_iters"]
+        cpu, ref = cpu_leg(cfg, Dh, Sh, maskh, n)
+        from oracle import cbpdn_oracle_torch as OT
+        rel_err = {"iterations": n, "X": {}, "functional": {}, "rho": {},
+                   "reference": "FP64 CPU restatement, the same first %d iterations of the "
+                                "same problem" % n}
+        Dm = Dh.astype(np.float64)
+        for v, ds, _ in solves:
+            keep = ds.opts.max_iter
+            ds.opts.max_iter = n
+            Y = ds.run()[0]
+            torch.cuda.synchronize()
+            rho_gpu = ds.state()["rho"][0]
+            ds.opts.max_iter = keep
+            if v == "cbpdnmsk":
+                Y = Y[1:]
+            Yg = Y.cpu().numpy()
+            Xo, info = ref[v]
+            Yo = np.moveaxis(Xo, 2, 0)
+            rel_err["X"][v] = float(np.linalg.norm((Yg - Yo).ravel()) /
+                                    np.linalg.norm(Yo.ravel()))
+            kw = {}
+            if v == "cbpdngrd":
+                kw = dict(mu=cfg["mu"], wgrd=np.ones(cfg["M"]))
+            Ss = Sh
+            if v == "cbpdnmsk":
+                kw = dict(mask=maskh)
+                Ss = Sh * maskh
+            J = OT.objective(Dm, Ss, Yg, np.float32(lam), **kw)
+            Jo = OT.objective(Dm, Ss, Yo, np.float32(lam), **kw)
+            rel_err["functional"][v] = abs(J - Jo) / abs(Jo)
+            rel_err["rho"][v] = abs(rho_gpu - info["rho"]) / info["rho"]
+            del Y, Yg
     out = None
     if rank == 0:
-        cpu = cpu_sample(cfg, D.cpu().numpy(), Sn, Wn) if world == 1 and not args.no_cpu else None
         out = {
             "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": cfg["workload"], "H": cfg["H"], "W": cfg["W"],
-                       "M": cfg["M"], "K": cfg["K"], "iterations_per_solve": cfg["iters"],
-                       "solves_per_step": len(cfg["variants"]),
-                       "parallelism": "replicas%d" % world if world > 1 else "single",
-                       "l2": "working set larger than L2 (no flush)" if
-                       graded_bytes(cfg["H"], cfg["W"], cfg["M"]) > 126e6 else
-                       "working set fits in L2"},
+            "config": config_dict(cfg, world),
             "e2e": {"value": e_value, "unit": "iter/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "kernel": "ADMM iteration (col_kernel + row_kernel + "
@@ -470,6 +519,7 @@ def run_ours(args, cfg, rank, world, local_rank):
                          "iteration_ms": ms / n_solve_it,
                          "kernel_sum_ms_per_iteration": it_ms / max(1, n_it), "kernels": kern,
                          "dominant_kernel": dom},
+            "rel_err": rel_err,
             "cpu_baseline": cpu,
             "gpu_launches": launches,
             "clocks": clk.summary(),
@@ -478,31 +528,24 @@ def run_ours(args, cfg, rank, world, local_rank):
 
 
 def synth_images(cfg, seed, device):
-    """Config 2: uneven images from one dictionary, masks, lambdas."""
+    """Config 2: uneven images from one dictionary, masks, lambdas (drawn on
+    the device with torch; torch.fft for the synthesis only)."""
     import torch
-    from sporco_cuda import _lib
     rng = np.random.default_rng(seed)
     M, K = cfg["M"], cfg["K"]
     g = torch.Generator(device=device).manual_seed(seed)
     D = torch.randn((M, K, K), generator=g, device=device)
     D /= torch.sqrt(torch.sum(D * D, dim=(1, 2), keepdim=True))
     imgs, masks = [], []
-    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     for _ in range(cfg["nimg"]):
         H, W = (int(rng.choice(cfg["sides"])) for _ in range(2))
         Dp = torch.zeros((M, H, W), device=device)
         Dp[:, :K, :K] = D
         X0 = (torch.rand((M, H, W), generator=g, device=device) < cfg["density"]).float() * \
             torch.randn((M, H, W), generator=g, device=device)
-        Wf = W // 2 + 1
-        Df = torch.empty((M, H, Wf), dtype=torch.complex64, device=device)
-        Xf = torch.empty((M, H, Wf), dtype=torch.complex64, device=device)
-        _lib.check(_lib.sc_rfft2(C.c_void_p(Dp.data_ptr()), C.c_void_p(Df.data_ptr()), M, H, W, st))
-        _lib.check(_lib.sc_rfft2(C.c_void_p(X0.data_ptr()), C.c_void_p(Xf.data_ptr()), M, H, W, st))
-        Sf = torch.sum(Df * Xf, dim=0).contiguous()
-        S = torch.empty((1, H, W), device=device)
-        _lib.check(_lib.sc_irfft2(C.c_void_p(Sf.data_ptr()), C.c_void_p(S.data_ptr()), 1, H, W, st))
-        S = S[0] + 0.01 * torch.randn((H, W), generator=g, device=device)
+        Sf = torch.sum(torch.fft.rfft2(Dp) * torch.fft.rfft2(X0), dim=0)
+        S = torch.fft.irfft2(Sf, s=(H, W))
+        S = S + 0.01 * torch.randn((H, W), generator=g, device=device)
         S = S - S.mean()
         p = float(rng.uniform(0.5, 0.9))
         mk = (torch.rand((H, W), generator=g, device=device) < p).float()
@@ -630,10 +673,10 @@ def run_adjoint(args, cfg, rank, world, local_rank):
     imgs = []
     D = None
     for b in range(B):
-        Db, Sb, _ = synth(cfg, 12345 + args.config + 100 * b + rank, dev)
+        Db, Sb, _ = synth(cfg, 12345 + args.config + 100 * b + 1000 * rank)
         if D is None:
-            D = Db
-        imgs.append(Sb)
+            D = torch.from_numpy(Db).to(dev)
+        imgs.append(torch.from_numpy(Sb).to(dev))
     # one dictionary for the batch: re-synthesise every clean image from D
     g = torch.Generator(device=dev).manual_seed(777 + rank)
     H, W, M, K = cfg["H"], cfg["W"], cfg["M"], cfg["K"]
@@ -709,37 +752,70 @@ def run_adjoint(args, cfg, rank, world, local_rank):
     }
 
 
-def run_reference(args, cfg, rank):
-    """The reference algorithm on the host cores (FP64 restatement)."""
+def run_reference(args, cfg, rank, world):
+    """The reference algorithm's CPU implementation on this host's cores: the
+    FP64 restatement (the reference ships no CPU solver; sporco, whose
+    ConvBPDN it mirrors, is not installed), torch on every host thread, maps
+    in chunks.  Each step continues one solve of the workload by a bounded
+    number of iterations (SC_REF_STEP_SECONDS, default 8 s, at least one
+    iteration).  Nothing of this package is loaded."""
     if rank != 0:
         return None
-    import torch  # noqa: F401  (device only for synthesis when available)
-    dev = "cuda" if torch.cuda.is_available() else "cpu"
-    if dev == "cuda":
-        D, S, mask = synth(cfg, 12345 + args.config, torch.device("cuda", 0))
-        D, S = D.cpu().numpy(), S.cpu().numpy()
-        mask = mask.cpu().numpy() if mask is not None else None
-    else:
-        rng = np.random.default_rng(12345 + args.config)
-        D = rng.standard_normal((cfg["M"], cfg["K"], cfg["K"])).astype(np.float32)
-        S = rng.standard_normal((cfg["H"], cfg["W"])).astype(np.float32)
-        mask = (rng.random((cfg["H"], cfg["W"])) < (cfg["mask_p"] or 1)).astype(np.float32)
-    per_step = []
+    if args.config in (2, 3):
+        return {"impl": "reference",
+                "unavailable": "the CPU restatement is timed on the single-solve workloads "
+                               "(configs 0, 1, 4) only"}
+    import torch
+    from oracle import cbpdn_oracle_torch as OT
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    D, S, mask = synth(cfg, 12345 + args.config)
     budget = float(os.environ.get("SC_REF_STEP_SECONDS", "8"))
+    gens = []
+    for v in cfg["variants"]:
+        a = _oracle_args(cfg, v, D, S, mask, cfg["iters"])
+        a.pop("variant")
+        prob, res, xi = OT.problem(v, **a)
+        gens.append(OT.iterate(prob, res, xi, record=False))
+    per_it = None
+    times, counts = [], []
+    done = 0
     for i in range(args.warmup + args.steps):
-        r = cpu_sample(cfg, D, S, mask, budget_s=budget)
+        n = 1 if per_it is None else max(1, int(budget / per_it))
+        n = max(1, min(n, cfg["iters"] - done))
+        t0 = time.perf_counter()
+        for _ in range(n):
+            for gen in gens:
+                next(gen, None)
+        dt = time.perf_counter() - t0
+        done += n
+        if i > 0 or per_it is None:
+            per_it = dt / n
         if i >= args.warmup:
-            per_step.append(r)
-    value = statistics.mean(r["value"] for r in per_step)
+            times.append(dt)
+            counts.append(n * len(gens))
+        if done >= cfg["iters"]:  # the solve is over: start it again
+            gens = []
+            for v in cfg["variants"]:
+                a = _oracle_args(cfg, v, D, S, mask, cfg["iters"])
+                a.pop("variant")
+                prob, res, xi = OT.problem(v, **a)
+                gens.append(OT.iterate(prob, res, xi, record=False))
+            done = 0
+    value = sum(counts) / sum(times)
+    sample = ("%s: %d timed steps of one continuing FP64 solve (%d ADMM iterations of %s in "
+              "all, set-up in the untimed warm-up; torch CPU, %d threads, maps in chunks of 16)"
+              % (cfg["workload"], args.steps, sum(counts), " and ".join(cfg["variants"]),
+                 threads))
     return {
-        "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "impl": "reference",
-        "config": {"workload": cfg["workload"], "H": cfg["H"], "W": cfg["W"], "M": cfg["M"],
-                   "K": cfg["K"]},
-        "cpu_baseline": {"value": value, "unit": "iter/s", "cores": os.cpu_count(),
-                         "kind": "port", "sample": per_step[-1]["sample"]},
+        "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": config_dict(cfg, world),
+        "cpu_baseline": {"value": value, "unit": "iter/s", "cores": threads, "kind": "port",
+                         "sample": sample},
         "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -750,7 +826,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", type=int, default=1, choices=sorted(CONFIGS))
+    ap.add_argument("--config", type=int, default=DEFAULT_CONFIG, choices=sorted(CONFIGS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end arm")
@@ -765,7 +841,7 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
-        out = run_reference(args, cfg, rank)
+        out = run_reference(args, cfg, rank, world)
         if out is not None:
             print(json.dumps(out), flush=True)
         return

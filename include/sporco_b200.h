@@ -124,6 +124,10 @@ typedef struct sc_options {
   int record_itstat;    /* keep per-iteration statistics on the device (see sc_read_state) */
   int check_every;      /* host polls the stop flag every this many iterations (0: never) */
   int profile;          /* time every iteration kernel with CUDA events (sc_last_profile) */
+  int nonneg;           /* NonNegCoef: project the coefficients onto >= 0 */
+  int no_bndry_cross;   /* NoBndryCross: zero the last Kr - 1 rows and Kc - 1
+                           columns of every map (filters crossing the bottom /
+                           right boundary); neither touches the AMS map */
 } sc_options;
 
 /* L1 weight layouts. */
@@ -203,8 +207,11 @@ int sc_irfft2(const void *xf, float *x, int count, int H, int W, void *stream);
  * critical path: its scratch (W + H twiddles) lives in a 64 KiB static
  * device array that every GPU loading this library holds until the process
  * exits.  Rejects H + W > 8192 with SC_ERR_UNSUPPORTED.  The first call on a
- * device looks up that array's device address; make it before any stream
- * capture.  All calls share the array, so calls that overlap on the GPU race. */
+ * device looks up that array's device address and keeps it; make it before
+ * any stream capture, and make no call on a device after cudaDeviceReset of
+ * that device in the same process (the kept address belongs to the old
+ * context).  All calls share the array, so calls that overlap on the GPU
+ * race. */
 int sc_rfft2_noalloc(const float *x, void *xf, int count, int H, int W, void *stream);
 
 /* Per-kernel device time of the last solve run with options.profile set:

@@ -205,6 +205,73 @@ class Problem:
     wl1: np.ndarray
     wgrd: np.ndarray | None
     mask: np.ndarray | None
+    nonneg: bool = False              # NonNegCoef
+    nobndry: tuple | None = None      # (Kr, Kc) with NoBndryCross, else None
+
+
+def _finalize(sums, rho, k, n, res: Resolved, xi: float, hist):
+    """Residuals, stopping test and adaptive rho of iteration k from the five
+    sums of squares (||X||^2, ||Y||^2, ||U||^2, ||X - Y||^2, ||Yold - Y||^2)
+    (cbpdn.cu:405-436, 519-559; Boyd et al. 2010 3.3-3.4; Wohlberg 2015).
+    Returns (new rho, rsf, stop)."""
+    nX, nY, nU = math.sqrt(sums[0]), math.sqrt(sums[1]), math.sqrt(sums[2])
+    r = math.sqrt(sums[3])
+    s = rho * math.sqrt(sums[4])
+    epri = math.sqrt(n) * res.AbsStopTol + max(nX, nY) * res.RelStopTol
+    edua = math.sqrt(n) * res.AbsStopTol + rho * nU * res.RelStopTol
+    if not res.StdResiduals:
+        rn = max(nX, nY)
+        rn = 1.0 if rn == 0.0 else rn
+        sn = rho * (1.0 if nU == 0.0 else nU)
+        r, s, epri, edua = r / rn, s / sn, epri / rn, edua / sn
+    if hist is not None:
+        hist["r"].append(r)
+        hist["s"].append(s)
+        hist["rho"].append(rho)
+        hist["epri"].append(epri)
+        hist["edua"].append(edua)
+    rsf = 1.0
+    if res.AutoRho and k > 1 and k % res.Period == 0:
+        if res.AutoScaling:
+            rhomlt = math.sqrt(r / (s * xi)) if s * xi > 0 else math.inf
+            if rhomlt < 1.0:
+                rhomlt = 1.0 / rhomlt if rhomlt > 0 else math.inf
+            rhomlt = min(rhomlt, res.Scaling)
+        else:
+            rhomlt = res.Scaling
+        if r > xi * res.RsdlRatio * s:
+            rsf = rhomlt
+        if s > (res.RsdlRatio / xi) * r:
+            rsf = 1.0 / rhomlt
+    return rsf * rho, rsf, (r <= epri and s <= edua)
+
+
+def y_step(V, prob: Problem, rho, m0, wl1):
+    """Y of the iteration from V = X_r + U for maps m0, m0 + 1, ... (V holds
+    a run of consecutive maps starting at map m0).
+
+    The soft threshold at lambda w / rho (cuda_Shrink_CalU_*,
+    cbpdn_kernels.cu:129-311), then, when requested, sporco's projections,
+    which the reference parses (cbpdn.pyx:70-71) but never applies: with
+    NonNegCoef negative coefficients are set to zero, with NoBndryCross the
+    coefficients whose filter would cross the bottom or right image boundary
+    (the last Kr - 1 rows and last Kc - 1 columns of every map) are set to
+    zero (sporco ConvBPDN.ystep / GenericConvBPDN.ystep).  Last, on map 0 of
+    masked problems the AMS step Y_0 = (1 - W) V_0 replaces all of that
+    (cuda_Cal_X_minus_U_W, cbpdn_kernels.cu:1137-1155).
+    """
+    Yn = np.sign(V) * np.maximum(np.abs(V) - (prob.lmbda / rho) * wl1, 0.0)
+    if prob.nonneg:
+        Yn[Yn < 0.0] = 0.0
+    if prob.nobndry is not None:
+        Kr, Kc = prob.nobndry
+        if Kr > 1:
+            Yn[:, V.shape[1] - (Kr - 1):, :] = 0.0
+        if Kc > 1:
+            Yn[:, :, V.shape[2] - (Kc - 1):] = 0.0
+    if prob.mask is not None and m0 == 0:
+        Yn[0] = (1.0 - prob.mask) * V[0]
+    return Yn
 
 
 def admm(prob: Problem, res: Resolved, xi: float, record=True, Y0=None, U0=None,
@@ -238,7 +305,6 @@ def admm(prob: Problem, res: Resolved, xi: float, record=True, Y0=None, U0=None,
         Gh = gradient_spectrum(H, W)[None]
         wg = np.asarray(prob.wgrd, dtype=np.float64).reshape(M, 1, 1)
     wl1 = np.broadcast_to(np.asarray(prob.wl1, dtype=np.float64), (M, H, W))
-    mask = prob.mask
     alpha = res.RelaxParam
     rho = res.rho0
     Y = np.zeros((M, H, W)) if Y0 is None else np.array(Y0, dtype=np.float64)
@@ -258,50 +324,102 @@ def admm(prob: Problem, res: Resolved, xi: float, record=True, Y0=None, U0=None,
         X = irfft2(Xf, (H, W))
         Xr = alpha * X + (1.0 - alpha) * Y if alpha != 1.0 else X
         V = Xr + U
-        Yn = np.sign(V) * np.maximum(np.abs(V) - (prob.lmbda / rho) * wl1, 0.0)
-        if mask is not None:
-            Yn[0] = (1.0 - mask) * V[0]
+        Yn = y_step(V, prob, rho, 0, wl1)
         U = V - Yn
         Yold, Y = Y, Yn
-        nX = math.sqrt(float(np.sum(X * X)))
-        nY = math.sqrt(float(np.sum(Y * Y)))
-        nU = math.sqrt(float(np.sum(U * U)))
-        r = math.sqrt(float(np.sum((X - Y) ** 2)))
-        s = rho * math.sqrt(float(np.sum((Yold - Y) ** 2)))
-        epri = math.sqrt(n) * res.AbsStopTol + max(nX, nY) * res.RelStopTol
-        edua = math.sqrt(n) * res.AbsStopTol + rho * nU * res.RelStopTol
-        if not res.StdResiduals:
-            rn = max(nX, nY)
-            rn = 1.0 if rn == 0.0 else rn
-            sn = rho * (1.0 if nU == 0.0 else nU)
-            r, s, epri, edua = r / rn, s / sn, epri / rn, edua / sn
-        if record:
-            hist["r"].append(r)
-            hist["s"].append(s)
-            hist["rho"].append(rho)
-            hist["epri"].append(epri)
-            hist["edua"].append(edua)
-        if res.AutoRho and k > 1 and k % res.Period == 0:
-            if res.AutoScaling:
-                rhomlt = math.sqrt(r / (s * xi)) if s * xi > 0 else math.inf
-                if rhomlt < 1.0:
-                    rhomlt = 1.0 / rhomlt if rhomlt > 0 else math.inf
-                rhomlt = min(rhomlt, res.Scaling)
-            else:
-                rhomlt = res.Scaling
-            rsf = 1.0
-            if r > xi * res.RsdlRatio * s:
-                rsf = rhomlt
-            if s > (res.RsdlRatio / xi) * r:
-                rsf = 1.0 / rhomlt
-            rho = rsf * rho
+        sums = (float(np.sum(X * X)), float(np.sum(Y * Y)), float(np.sum(U * U)),
+                float(np.sum((X - Y) ** 2)), float(np.sum((Yold - Y) ** 2)))
+        rho, rsf, stop = _finalize(sums, rho, k, n, res, xi, hist if record else None)
+        if rsf != 1.0:
             if emulate_ref_rescale:
                 Uf = U.reshape(-1).copy()
                 Uf[:min(Uf.size, H * M * H)] /= rsf
                 U = Uf.reshape(U.shape)
             else:
                 U = U / rsf
-        if r <= epri and s <= edua:
+        if stop:
+            break
+    info = {"iterations": k, "rho": rho, "hist": hist, "Y": Y, "U": U}
+    return Y, info
+
+
+def admm_lean(prob: Problem, res: Resolved, xi: float, chunk=16, record=True,
+              store_dict_bytes=4 << 30):
+    """The iterations of :func:`admm` with the maps processed in chunks, for
+    problems whose full-size float64 temporaries do not fit in host memory
+    (2048 x 2048 with 256 maps: about 9 GB per array).
+
+    Same mathematics and the same per-iteration steps as :func:`admm`
+    (cbpdn.cu:319-567); only the summation order of the sums over the maps
+    differs.  Per iteration: pass 1 accumulates sum_m Df_m b_m / d_m and
+    sum_m |Df_m|^2 / d_m chunk by chunk; pass 2 forms b again, solves, takes
+    the inverse transform and does the element-wise steps chunk by chunk.
+    Y and U are the only full-size arrays kept (plus the dictionary spectra
+    when they take at most ``store_dict_bytes``; otherwise they are
+    recomputed per chunk).  No U0 / Y0 and no reference-rescale emulation.
+    """
+    D, S = prob.D, prob.S
+    M = D.shape[0]
+    H, W = S.shape
+    n = M * H * W
+    Wf = W // 2 + 1
+    Sf = rfft2(S.astype(np.float64))
+    keep = M * H * Wf * 16 <= store_dict_bytes
+    Dfull = pad_dict_spectrum(D, H, W) if keep else None
+    grd = prob.wgrd is not None
+    Gh = gradient_spectrum(H, W)[None] if grd else None
+    wl1 = np.asarray(prob.wl1, dtype=np.float64)
+    alpha = res.RelaxParam
+    rho = res.rho0
+    Y = np.zeros((M, H, W))
+    U = np.zeros((M, H, W))
+    hist = {"r": [], "s": [], "rho": [], "epri": [], "edua": []}
+    chunks = [(m0, min(M, m0 + chunk)) for m0 in range(0, M, chunk)]
+
+    def dict_chunk(m0, m1):
+        return Dfull[m0:m1] if keep else pad_dict_spectrum(D[m0:m1], H, W)
+
+    def d_chunk(m0, m1):
+        if not grd:
+            return rho
+        wg = np.asarray(prob.wgrd, dtype=np.float64)[m0:m1].reshape(-1, 1, 1)
+        return prob.mu * wg * Gh + rho
+
+    def wl1_chunk(m0, m1):
+        return wl1[m0:m1] if wl1.shape[0] > 1 else wl1
+
+    k = 0
+    for k in range(1, res.MaxMainIter + 1):
+        num = np.zeros((H, Wf), dtype=np.complex128)
+        sden = np.zeros((H, Wf))
+        for m0, m1 in chunks:
+            Dc = dict_chunk(m0, m1)
+            d = d_chunk(m0, m1)
+            b = np.conj(Dc) * Sf[None] + rho * rfft2(Y[m0:m1] - U[m0:m1])
+            num += np.sum(Dc * b / d, axis=0)
+            sden += np.sum((Dc.real ** 2 + Dc.imag ** 2) / d, axis=0)
+        cb = num / (1.0 + sden)
+        sums = [0.0] * 5
+        for m0, m1 in chunks:
+            Dc = dict_chunk(m0, m1)
+            d = d_chunk(m0, m1)
+            b = np.conj(Dc) * Sf[None] + rho * rfft2(Y[m0:m1] - U[m0:m1])
+            X = irfft2((b - np.conj(Dc) * cb[None]) / d, (H, W))
+            Yc, Uc = Y[m0:m1], U[m0:m1]
+            V = (alpha * X + (1.0 - alpha) * Yc if alpha != 1.0 else X) + Uc
+            Yn = y_step(V, prob, rho, m0, wl1_chunk(m0, m1))
+            Un = V - Yn
+            sums[0] += float(np.sum(X * X))
+            sums[1] += float(np.sum(Yn * Yn))
+            sums[2] += float(np.sum(Un * Un))
+            sums[3] += float(np.sum((X - Yn) ** 2))
+            sums[4] += float(np.sum((Yc - Yn) ** 2))
+            Y[m0:m1] = Yn
+            U[m0:m1] = Un
+        rho, rsf, stop = _finalize(sums, rho, k, n, res, xi, hist if record else None)
+        if rsf != 1.0:
+            U /= rsf
+        if stop:
             break
     info = {"iterations": k, "rho": rho, "hist": hist, "Y": Y, "U": U}
     return Y, info
@@ -389,7 +507,7 @@ def _ams(D, opt, grd):
 
 
 def _run(Dk, S, W, lmbda, mu, opt, grd, wl1=None, wg=None, return_info=False,
-         emulate_ref_rescale=False):
+         emulate_ref_rescale=False, lean_chunk=0):
     Dk = np.asarray(Dk, dtype=np.float32)
     S = np.asarray(S, dtype=np.float32)
     M = Dk.shape[2]
@@ -412,41 +530,50 @@ def _run(Dk, S, W, lmbda, mu, opt, grd, wl1=None, wg=None, return_info=False,
         wl1=wl1a,
         wgrd=wga,
         mask=mask,
+        nonneg=bool(_get(opt, "NonNegCoef", False)),
+        nobndry=tuple(Dk.shape[0:2]) if _get(opt, "NoBndryCross", False) else None,
     )
-    Y, info = admm(prob, res, rsdl_target(res, lmbda),
-                   emulate_ref_rescale=emulate_ref_rescale)
+    if lean_chunk > 0:
+        Y, info = admm_lean(prob, res, rsdl_target(res, lmbda), chunk=lean_chunk)
+    else:
+        Y, info = admm(prob, res, rsdl_target(res, lmbda),
+                       emulate_ref_rescale=emulate_ref_rescale)
     X = np.moveaxis(Y, 0, 2)
     return (X, info) if return_info else X
 
 
-def cbpdn(D, S, lmbda, opt, dev=0, return_info=False, emulate_ref_rescale=False):
-    """Oracle for sporco_cuda.cbpdn.cbpdn (cbpdn.pyx:86-102)."""
+def cbpdn(D, S, lmbda, opt, dev=0, return_info=False, emulate_ref_rescale=False,
+          lean_chunk=0):
+    """Oracle for sporco_cuda.cbpdn.cbpdn (cbpdn.pyx:86-102).  lean_chunk > 0:
+    the map-chunked iterations of admm_lean (large problems)."""
     return _run(D, S, None, lmbda, 0.0, opt, False, return_info=return_info,
-                emulate_ref_rescale=emulate_ref_rescale)
+                emulate_ref_rescale=emulate_ref_rescale, lean_chunk=lean_chunk)
 
 
-def cbpdnmsk(D, S, W, lmbda, opt, dev=0, return_info=False, emulate_ref_rescale=False):
+def cbpdnmsk(D, S, W, lmbda, opt, dev=0, return_info=False, emulate_ref_rescale=False,
+             lean_chunk=0):
     """Oracle for sporco_cuda.cbpdn.cbpdnmsk (cbpdn.pyx:108-152)."""
     Di, wl1, _ = _ams(np.asarray(D, dtype=np.float32), opt, False)
     out = _run(Di, S, W, lmbda, 0.0, opt, False, wl1=wl1, return_info=return_info,
-               emulate_ref_rescale=emulate_ref_rescale)
+               emulate_ref_rescale=emulate_ref_rescale, lean_chunk=lean_chunk)
     if return_info:
         return out[0][..., 1:], out[1]
     return out[..., 1:]
 
 
-def cbpdngrd(D, S, lmbda, mu, opt, dev=0, return_info=False, emulate_ref_rescale=False):
+def cbpdngrd(D, S, lmbda, mu, opt, dev=0, return_info=False, emulate_ref_rescale=False,
+             lean_chunk=0):
     """Oracle for sporco_cuda.cbpdn.cbpdngrd (cbpdn.pyx:207-223)."""
     return _run(D, S, None, lmbda, mu, opt, True, return_info=return_info,
-                emulate_ref_rescale=emulate_ref_rescale)
+                emulate_ref_rescale=emulate_ref_rescale, lean_chunk=lean_chunk)
 
 
 def cbpdngrdmsk(D, S, W, lmbda, mu, opt, dev=0, return_info=False,
-                emulate_ref_rescale=False):
+                emulate_ref_rescale=False, lean_chunk=0):
     """Oracle for sporco_cuda.cbpdn.cbpdngrdmsk (cbpdn.pyx:229-291)."""
     Di, wl1, g = _ams(np.asarray(D, dtype=np.float32), opt, True)
     out = _run(Di, S, W, lmbda, mu, opt, True, wl1=wl1, wg=g, return_info=return_info,
-               emulate_ref_rescale=emulate_ref_rescale)
+               emulate_ref_rescale=emulate_ref_rescale, lean_chunk=lean_chunk)
     if return_info:
         return out[0][..., 1:], out[1]
     return out[..., 1:]

@@ -78,6 +78,9 @@ struct RowParams {
   float l1_scalar;
   const float* l1w;
   const int32_t* mask;     // (B, H, W) or NULL
+  int nonneg;              // NonNegCoef: Y >= 0
+  int bnd_r, bnd_c;        // NoBndryCross: rows >= bnd_r and columns >= bnd_c
+                           // of every map are zero (H, W: none)
   float relax;
   float invN;              // 1 / (H W)
   double* partials;        // (B, nblk, 5)

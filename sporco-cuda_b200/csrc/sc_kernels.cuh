@@ -126,18 +126,34 @@ __device__ __forceinline__ float2 pack_inverse(const float2* a, const float2* bb
 
 // Threshold weight of one image row: scalar w, or the row wr of a full
 // weight array; mrow: the AMS mask row when the row belongs to map 0 of a
-// masked problem.
+// masked problem; nonneg and kcut: the projections of NonNegCoef (Y >= 0)
+// and NoBndryCross (elements k >= kcut are zero: the last Kc - 1 columns,
+// the whole row in the last Kr - 1 rows; SC_NO_CUT: none).
+#define SC_NO_CUT 0x40000000
 struct RowW {
   float w;
   const float* wr;
   const int32_t* mrow;
+  int kcut;
+  bool nonneg;
+  // scalar threshold, no AMS row, no projection: the fast element path
+  __device__ __forceinline__ bool plain() const {
+    return !mrow && !wr && !nonneg && kcut == SC_NO_CUT;
+  }
 };
 
 // Y of the shrinkage step at element k of a row: the AMS step (1 - mask) v
 // on map 0 of masked problems, else the soft threshold at th times the
-// row's weight (cbpdn_kernels.cu:129-311, 1137-1155).
+// row's weight (cbpdn_kernels.cu:129-311, 1137-1155), followed by the
+// projections the reference parses but never applies (cbpdn.pyx:70-71;
+// sporco's ConvBPDN y-step): NonNegCoef sets negative values to zero,
+// NoBndryCross zeroes the coefficients whose filter would cross the bottom
+// or right image boundary.
 __device__ __forceinline__ float shrink_y(float v, float th, const RowW& r, int k) {
-  return r.mrow ? (float)(1 - r.mrow[k]) * v : soft_threshold(v, th * (r.wr ? r.wr[k] : r.w));
+  if (r.mrow) return (float)(1 - r.mrow[k]) * v;
+  float y = soft_threshold(v, th * (r.wr ? r.wr[k] : r.w));
+  if (r.nonneg) y = fmaxf(y, 0.f);
+  return k >= r.kcut ? 0.f : y;
 }
 
 // Per-launch constants of the iteration's element-wise step.
@@ -258,12 +274,15 @@ row_kernel(RowParams P) {
     const int32_t* mk = P.mask ? P.mask + (size_t)b * H * W : nullptr;
     // threshold weights and AMS mask row of image row r of this image
     auto roww = [&](long r, bool ok) -> RowW {
-      RowW o{P.l1_scalar, nullptr, nullptr};
+      RowW o{P.l1_scalar, nullptr, nullptr, SC_NO_CUT, false};
       if (!ok) return o;
       const int m = (int)(r / H), h = (int)(r - (long)m * H);
       if (P.l1_kind == 1) o.w = P.l1w[m];
       if (P.l1_kind == 2) o.wr = P.l1w + ((size_t)m * H + h) * W;
       if (mk && m == 0) o.mrow = mk + (size_t)h * W;
+      o.nonneg = P.nonneg != 0;
+      if (P.bnd_r > 0 && h >= P.bnd_r) o.kcut = 0;
+      else if (P.bnd_c > 0 && P.bnd_c < W) o.kcut = P.bnd_c;
       return o;
     };
 
@@ -335,7 +354,7 @@ row_kernel(RowParams P) {
             float2 v[EM];
             if (valid) {
               const RowW w0 = roww(2 * p, true), w1 = roww(2 * p + 1, has1);
-              if (!w0.mrow && !w1.mrow && !w0.wr && !w1.wr) {
+              if (w0.plain() && w1.plain()) {
                 const float t0 = thr_prev * w0.w, t1 = thr_prev * w1.w;
 #pragma unroll
                 for (int m = 0; m < EM; ++m) {
@@ -385,7 +404,7 @@ row_kernel(RowParams P) {
         if (valid) {
           if (vstate) {
             const RowW w0 = roww(2 * p, true), w1 = roww(2 * p + 1, has1);
-            if (!w0.mrow && !w1.mrow && !w0.wr && !w1.wr) {
+            if (w0.plain() && w1.plain()) {
               const float t0 = thr_prev * w0.w, t1 = thr_prev * w1.w;
               for (int k = t; k < W; k += g) {
                 const float v0 = usm[k], v1 = has1 ? usm[W + k] : 0.f;
@@ -526,7 +545,7 @@ row_kernel(RowParams P) {
           }
         } else if (!ADJ && valid) {
           const RowW w0 = roww(r0, true), w1 = roww(r1, has1);
-          const bool fast = has1 && !w0.mrow && !w1.mrow && !w0.wr && !w1.wr;
+          const bool fast = has1 && w0.plain() && w1.plain();
           const float tc0 = thr * w0.w, tc1 = thr * w1.w;
           const float tq0 = thr_prev * w0.w, tq1 = thr_prev * w1.w;
           float* O0 = out0(r0);
@@ -605,7 +624,7 @@ row_kernel(RowParams P) {
           }
         } else if (!ADJ && valid) {
           const RowW w0 = roww(r0, true), w1 = roww(r1, has1);
-          const bool fast = has1 && !w0.mrow && !w1.mrow && !w0.wr && !w1.wr;
+          const bool fast = has1 && w0.plain() && w1.plain();
           const float tc0 = thr * w0.w, tc1 = thr * w1.w;
           const float tq0 = thr_prev * w0.w, tq1 = thr_prev * w1.w;
           float* O0 = out0(r0);
@@ -1728,7 +1747,8 @@ __global__ void state_yu_kernel(const float* __restrict__ V, float* __restrict__
                                 float* __restrict__ U, const ImgState* __restrict__ st,
                                 const float* __restrict__ lam, int M, int H, int W, int l1_kind,
                                 float l1_scalar, const float* __restrict__ l1w,
-                                const int32_t* __restrict__ mask) {
+                                const int32_t* __restrict__ mask, int nonneg, int bnd_r,
+                                int bnd_c) {
   const int b = blockIdx.y;
   const ImgState& S = st[b];
   const bool first = S.k == 0;
@@ -1748,6 +1768,9 @@ __global__ void state_yu_kernel(const float* __restrict__ V, float* __restrict__
       } else {
         const float w = l1_kind == 1 ? l1w[m] : l1_kind == 2 ? l1w[i] : l1_scalar;
         y = soft_threshold(v, thr * w);
+        if (nonneg) y = fmaxf(y, 0.f);
+        const int h = (int)(hw / W), c = (int)(hw - (size_t)h * W);
+        if (h >= bnd_r || c >= bnd_c) y = 0.f;
       }
       u = (v - y) * us;
     }

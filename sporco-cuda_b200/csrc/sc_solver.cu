@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -150,16 +151,31 @@ struct Plan {
       off_it, off_xi, off_ndone, off_objspec, off_objpart, total;
 };
 
-static int g_num_sms = 0;
+// Process-wide caches of this file (kernel attributes, occupancy answers,
+// autotuned cluster sizes, FFT-tool twiddles, SM counts) are shared by every
+// host thread and guarded by this mutex; the solves themselves keep all of
+// their state in the caller's workspace.
+static std::mutex g_cache_mu;
 
+#define SC_MAX_DEVICES 64
+static std::atomic<int> g_num_sms[SC_MAX_DEVICES];
+
+// SM count of the current device (cached per device).
 static int num_sms() {
-  if (g_num_sms == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (g_num_sms <= 0) g_num_sms = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return 148;
+  if (dev >= SC_MAX_DEVICES) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
   }
-  return g_num_sms;
+  int n = g_num_sms[dev].load();
+  if (n == 0) {
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+    g_num_sms[dev].store(n);
+  }
+  return n;
 }
 
 static int plan_geometry(int B, int M, int H, int W, Plan* pl) {
@@ -275,20 +291,23 @@ static ColFn col_fn(int H) {
   return col_kernel<MODE, 0>;
 }
 
-// Opt every kernel instantiation into large dynamic shared memory once.
+// Opt every kernel instantiation into large dynamic shared memory (the
+// device's opt-in maximum) once per device.
 static int prepare_fn(const void* fn, bool cluster) {
-  static std::vector<const void*> done;
-  for (const void* d : done)
-    if (d == fn) return SC_OK;
+  struct Done { int dev; const void* fn; };
+  static std::vector<Done> done;
   int dev = 0, optin = 0;
   CU_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_cache_mu);
+  for (const Done& d : done)
+    if (d.dev == dev && d.fn == fn) return SC_OK;
   CU_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   cudaFuncAttributes fa;
   CU_TRY(cudaFuncGetAttributes(&fa, fn));
   CU_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               optin - (int)fa.sharedSizeBytes));
   if (cluster) CU_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-  done.push_back(fn);
+  done.push_back({dev, fn});
   return SC_OK;
 }
 
@@ -348,6 +367,7 @@ static int resident_clusters(const void* fn, int NT, size_t smem, int G, int* ou
   static std::vector<Entry> cache;
   int dev = 0;
   CU_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_cache_mu);
   for (const Entry& e : cache)
     if (e.dev == dev && e.fn == fn && e.G == G && e.smem == smem) {
       *out = e.n;
@@ -435,6 +455,7 @@ static int forced_cluster(int M) {
 static bool tuned_size(const void* fn, const Geom& g, int* G) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  std::lock_guard<std::mutex> lock(g_cache_mu);
   for (const TunedG& e : g_tuned)
     if (e.dev == dev && e.fn == fn && e.H == g.H && e.W == g.W && e.M == g.M) {
       *G = e.G;
@@ -546,6 +567,8 @@ extern "C" void sc_options_from_algopt(const AlgOpt* a, sc_options* o) {
   o->std_residuals = a->StdResiduals;
   o->record_itstat = a->Verbose ? 1 : 0;
   o->check_every = 32;
+  o->nonneg = a->NonNegCoef > 0 ? 1 : 0;
+  o->no_bndry_cross = a->NoBndryCross > 0 ? 1 : 0;
 }
 
 // One solve of a batch of equal-sized images: set-up, iteration launches in
@@ -664,6 +687,9 @@ struct Solve {
     rp.g = g; rp.pw = pl.pw; rp.twW = twW; rp.F = F; rp.Y = p->Y; rp.Yo = p->Y; rp.U = U;
     rp.lam = p->lmbda; rp.l1_kind = p->l1_kind; rp.l1_scalar = p->l1_scalar; rp.l1w = p->l1w;
     rp.mask = p->mask; rp.relax = o->relax; rp.invN = (float)(1.0 / ((double)g.H * g.W));
+    rp.nonneg = o->nonneg ? 1 : 0;
+    rp.bnd_r = o->no_bndry_cross && p->Kr > 1 ? g.H - (p->Kr - 1) : g.H;
+    rp.bnd_c = o->no_bndry_cross && p->Kc > 1 ? g.W - (p->Kc - 1) : g.W;
     rp.partials = part; rp.st = sts; rp.vstate = vstate ? 1 : 0;
     cp.g = g; cp.ph = pl.ph; cp.twH = twH; cp.twW = twW; cp.F = F; cp.Dh = Dh; cp.Sh = Sh;
     cp.grd = p->grd; cp.mu = p->mu; cp.wgrd = p->wgrd; cp.Psum = Psum; cp.st = sts;
@@ -777,7 +803,14 @@ struct Solve {
     }
     int dev = 0;
     CU_TRY(cudaGetDevice(&dev));
-    g_tuned.push_back({dev, fn, g.H, g.W, g.M, cand[bi]});
+    {
+      // a shape tuned meanwhile by another thread keeps its first answer
+      std::lock_guard<std::mutex> lock(g_cache_mu);
+      bool known = false;
+      for (const TunedG& e : g_tuned)
+        known = known || (e.dev == dev && e.fn == fn && e.H == g.H && e.W == g.W && e.M == g.M);
+      if (!known) g_tuned.push_back({dev, fn, g.H, g.W, g.M, cand[bi]});
+    }
     return init_iterates();
   }
 
@@ -895,7 +928,8 @@ struct Solve {
     const size_t n = (size_t)g.M * g.H * g.W;
     dim3 grid((unsigned)std::min<size_t>((n + 255) / 256, 1024), g.B);
     state_yu_kernel<<<grid, 256, 0, s>>>(U, y, u, sts, p->lmbda, g.M, g.H, g.W, p->l1_kind,
-                                         p->l1_scalar, p->l1w, p->mask);
+                                         p->l1_scalar, p->l1w, p->mask, rp.nonneg, rp.bnd_r,
+                                         rp.bnd_c);
     CU_TRY(cudaGetLastError());
     ++g_launches;
     return SC_OK;
@@ -953,7 +987,7 @@ extern "C" int sc_cbpdn_solve(const sc_problem* p, const sc_options* o, void* wo
   // Per-kernel event timing (profile mode only); events come from a
   // grow-only pool so that profiling adds no per-launch host allocation.
   struct EvRec { cudaEvent_t a, b; int kind; };
-  static std::vector<cudaEvent_t> ev_pool;
+  static thread_local std::vector<cudaEvent_t> ev_pool;
   std::vector<EvRec> evs;
   size_t ev_next = 0;
   auto get_ev = [&](cudaEvent_t* e) -> int {
@@ -1291,6 +1325,7 @@ static std::vector<TwEntry> g_tw_cache;
 static int tool_twiddles(int W, int H, cudaStream_t s, float2** out) {
   int dev = 0;
   CU_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_cache_mu);
   for (auto& e : g_tw_cache)
     if (e.dev == dev && e.W == W && e.H == H) {
       *out = e.tw;
@@ -1301,6 +1336,8 @@ static int tool_twiddles(int W, int H, cudaStream_t s, float2** out) {
   twiddle_kernel<<<(W + 255) / 256, 256, 0, s>>>(tw, W);
   twiddle_kernel<<<(H + 255) / 256, 256, 0, s>>>(tw + W, H);
   CU_TRY(cudaGetLastError());
+  // other threads may use the table at once, from other streams
+  CU_TRY(cudaStreamSynchronize(s));
   g_tw_cache.push_back({dev, W, H, tw});
   *out = tw;
   return SC_OK;
@@ -1363,7 +1400,8 @@ extern "C" int sc_irfft2(const void* xf, float* x, int count, int H, int W, void
 #define SC_NOALLOC_MAX_DEVICES 64
 static __device__ __align__(256) float2 sc_noalloc_tw[SC_NOALLOC_TWIDDLES];
 // Device address of sc_noalloc_tw per device (the host-side symbol is only a
-// stand-in for it), looked up once per device by the first call there.
+// stand-in for it), looked up once per device by the first call there, under
+// g_cache_mu.
 static float2* g_noalloc_tw[SC_NOALLOC_MAX_DEVICES] = {};
 
 extern "C" int sc_rfft2_noalloc(const float* x, void* xf, int count, int H, int W, void* stream) {
@@ -1384,12 +1422,16 @@ extern "C" int sc_rfft2_noalloc(const float* x, void* xf, int count, int H, int 
   if (dev < 0 || dev >= SC_NOALLOC_MAX_DEVICES)
     return set_status(SC_ERR_UNSUPPORTED, "device %d beyond the %d this entry point tracks", dev,
                       SC_NOALLOC_MAX_DEVICES);
-  if (!g_noalloc_tw[dev]) {
-    void* addr = nullptr;
-    CU_TRY(cudaGetSymbolAddress(&addr, sc_noalloc_tw));
-    g_noalloc_tw[dev] = (float2*)addr;
+  float2* tw = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    if (!g_noalloc_tw[dev]) {
+      void* addr = nullptr;
+      CU_TRY(cudaGetSymbolAddress(&addr, sc_noalloc_tw));
+      g_noalloc_tw[dev] = (float2*)addr;
+    }
+    tw = g_noalloc_tw[dev];
   }
-  float2* tw = g_noalloc_tw[dev];
   cudaStream_t s = (cudaStream_t)stream;
   pl.g.Wp = pl.g.Wf;  // dense numpy layout
   twiddle_kernel<<<(W + 255) / 256, 256, 0, s>>>(tw, W);
@@ -1399,8 +1441,10 @@ extern "C" int sc_rfft2_noalloc(const float* x, void* xf, int count, int H, int 
   rp.g = pl.g; rp.pw = pl.pw; rp.twW = tw; rp.F = (float2*)xf; rp.src = x;
   rp.gsz = pl.rowg_g;
   rp.nblk = pl.row_nblk;
-  CU_TRY(cudaFuncSetAttribute(row_kernel<ROW_FWD_REAL, 0>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.rowg_smem));
+  // the same one-time opt-in to the device's shared-memory maximum as every
+  // other launch of these kernels (never lowered per call)
+  if ((st = prepare_fn((const void*)row_kernel<ROW_FWD_REAL, 0>, false))) return st;
+  if ((st = prepare_fn((const void*)col_kernel<COL_FWD, 0>, false))) return st;
   row_kernel<ROW_FWD_REAL, 0><<<dim3(rp.nblk, count), (SC_ROW_THREADS / rp.gsz) * rp.gsz,
                                  pl.rowg_smem, s>>>(rp);
   CU_TRY(cudaGetLastError());
@@ -1409,8 +1453,6 @@ extern "C" int sc_rfft2_noalloc(const float* x, void* xf, int count, int H, int 
   cp.gsz = pl.colg_g;
   cp.Hs = pl.Hs;
   cp.G = 1;
-  CU_TRY(cudaFuncSetAttribute(col_kernel<COL_FWD, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)pl.colg_smem));
   col_kernel<COL_FWD, 0><<<dim3(1, pl.col_ntiles, count), pl.colg_NT, pl.colg_smem, s>>>(cp);
   CU_TRY(cudaGetLastError());
   g_launches += 4;

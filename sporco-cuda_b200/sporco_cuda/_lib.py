@@ -85,6 +85,8 @@ class ScOptions(C.Structure):
         ("record_itstat", C.c_int),
         ("check_every", C.c_int),
         ("profile", C.c_int),
+        ("nonneg", C.c_int),
+        ("no_bndry_cross", C.c_int),
     ]
 
 

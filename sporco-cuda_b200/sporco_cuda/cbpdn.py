@@ -24,7 +24,9 @@ Differences from the reference, all deliberate: errors raise
 keys (the reference's C defaults fill them); ``opt`` is never mutated; a
 user ``AutoRho.RsdlTarget`` is honoured; the solve coefficients always follow
 the current rho (the reference's are stale after a rho change unless
-``HighMemSolve``); after a rho change all of U is rescaled.
+``HighMemSolve``); after a rho change all of U is rescaled; ``NonNegCoef``
+and ``NoBndryCross``, which the reference parses but ignores
+(cbpdn.pyx:70-71), are applied as sporco's ConvBPDN applies them.
 """
 
 from __future__ import annotations
@@ -226,6 +228,8 @@ def _sc_options(r, record_itstat=False, check_every=32, profile=False):
     o.record_itstat = int(bool(record_itstat or r["Verbose"]))
     o.check_every = int(check_every)
     o.profile = int(bool(profile))
+    o.nonneg = r["NonNegCoef"]
+    o.no_bndry_cross = r["NoBndryCross"]
     return o
 
 

@@ -132,9 +132,10 @@ def _check_functional(D, S, X, Xo, lam, mu=0.0, grd=False, mask=None):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("variant", ["cbpdngrd", "cbpdnmsk"])
-def test_autorho_trajectory_512(variant):
-    """512x512 shapes with adaptive rho: the GPU rho trajectory and result
-    follow the FP64 oracle (the oracle run is cut to 30 iterations)."""
+def test_autorho_128x128(variant):
+    """128 x 128, 16 filters 12 x 12, adaptive rho, 30 iterations: the GPU
+    result follows the FP64 oracle (the 512 x 512 benchmark shapes are in
+    test_gpu_benchmark_shapes.py)."""
     D, S = _synth(128, 128, 16, 12, 0.005, 7)
     lam, mu = 0.05, 0.1
     opt = {"MaxMainIter": 30, "RelStopTol": 0.0, "AutoRho": {"Enabled": True}}

@@ -44,6 +44,23 @@ def test_noalloc_rfft2_matches_allocating_entry_point_twice():
         assert np.linalg.norm(got - exact) / np.linalg.norm(exact) < TOL
 
 
+@pytest.mark.gpu
+def test_allocating_entry_points_still_work_after_noalloc():
+    """A call at a small size with no compile-time plan, then the allocating
+    transform at larger sizes with none (their kernels need more shared
+    memory than the small call did): both still run and match numpy."""
+    rng = np.random.default_rng(7)
+    for (h0, w0), (H, W) in (((32, 31), (500, 300)), ((20, 27), (333, 601))):
+        x0 = rng.standard_normal((2, h0, w0)).astype(np.float32)
+        got0 = _call(_lib.sc_rfft2_noalloc, x0)
+        ex0 = np.fft.rfft2(x0.astype(np.float64))
+        assert np.linalg.norm(got0 - ex0) / np.linalg.norm(ex0) < TOL
+        x = rng.standard_normal((2, H, W)).astype(np.float32)
+        got = _call(_lib.sc_rfft2, x)
+        exact = np.fft.rfft2(x.astype(np.float64))
+        assert np.linalg.norm(got - exact) / np.linalg.norm(exact) < TOL, (H, W)
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch():
     st = _lib.sc_rfft2_noalloc(C.c_void_p(1), C.c_void_p(1), 1, 4096, 8192, None)
     assert st == 2  # SC_ERR_UNSUPPORTED

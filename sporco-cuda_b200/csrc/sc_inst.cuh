@@ -1,0 +1,24 @@
+// Helpers of the kernel instantiation units (sc_inst_*.cu): the table of
+// one row or column mode over the compile-time lengths.
+#pragma once
+
+#include "sc_dispatch.cuh"
+#include "sc_kernels.cuh"
+
+template <int MODE>
+RowFn row_table(int n) {
+#define SC_ROW_CASE(k) case k: return row_kernel<MODE, k>;
+  if constexpr (row_specialised(MODE)) {
+    switch (n) { SC_SPEC_ROW(SC_ROW_CASE) default: break; }
+  }
+#undef SC_ROW_CASE
+  return row_kernel<MODE, 0>;
+}
+
+template <int MODE>
+ColFn col_table(int n) {
+#define SC_COL_CASE(k) case k: return col_kernel<MODE, k>;
+  switch (n) { SC_SPEC_COL(SC_COL_CASE) default: break; }
+#undef SC_COL_CASE
+  return col_kernel<MODE, 0>;
+}

@@ -23,7 +23,8 @@
 #include <vector>
 
 #include "../../include/sporco_b200.h"
-#include "sc_kernels.cuh"
+#include "sc_aux_kernels.cuh"
+#include "sc_dispatch.cuh"
 
 #define SC_VERSION "0.1.0"
 
@@ -112,11 +113,6 @@ static int group_size(int n) {
   return std::max(32, g);
 }
 
-// Transform lengths with compile-time FFT plans (all benchmark sizes).
-#define SC_SPEC_ROW(X) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) \
-  X(48) X(96) X(192) X(384) X(768) X(1536)
-#define SC_SPEC_COL(X) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) \
-  X(48) X(96) X(192) X(384) X(768) X(1536)
 #define SC_CASE_LABEL(n) case n:
 
 static bool spec_row(int n) {
@@ -260,36 +256,7 @@ extern "C" size_t sc_workspace_size(const sc_problem* p, const sc_options* o) {
 }
 
 // --------------------------------------------------------------- launchers --
-typedef void (*RowFn)(RowParams);
-typedef void (*ColFn)(ColParams);
-
-// Row modes with compile-time FFT plans: the iteration, the rho fix-up and
-// the 2-D FFT tools (used inside the adjoint); set-up modes use the runtime
-// plan.
-template <int MODE>
-constexpr bool row_specialised() {
-  return MODE == ROW_ITER || MODE == ROW_ITER_YU || MODE == ROW_FIXUP || MODE == ROW_FWD_REAL ||
-         MODE == ROW_INV_REAL ||
-         MODE == ROW_ADJ;
-}
-
-template <int MODE>
-static RowFn row_fn(int W) {
-#define SC_ROW_CASE(n) case n: return row_kernel<MODE, n>;
-  if constexpr (row_specialised<MODE>()) {
-    switch (W) { SC_SPEC_ROW(SC_ROW_CASE) default: break; }
-  }
-#undef SC_ROW_CASE
-  return row_kernel<MODE, 0>;
-}
-
-template <int MODE>
-static ColFn col_fn(int H) {
-#define SC_COL_CASE(n) case n: return col_kernel<MODE, n>;
-  switch (H) { SC_SPEC_COL(SC_COL_CASE) default: break; }
-#undef SC_COL_CASE
-  return col_kernel<MODE, 0>;
-}
+// (the kernel tables row_fn / col_fn: sc_dispatch.cuh)
 
 // Opt every kernel instantiation into large dynamic shared memory (the
 // device's opt-in maximum) once per device.
@@ -334,7 +301,7 @@ static void set_pdl(cudaLaunchAttribute* a) {
 
 template <int MODE>
 static int launch_row(const Plan& pl, RowParams rp, int B, cudaStream_t s, int nblk = 0) {
-  const bool hot = row_specialised<MODE>() && spec_row(rp.g.W);
+  const bool hot = row_specialised(MODE) && spec_row(rp.g.W);
   RowFn fn = row_fn<MODE>(rp.g.W);
   int st = prepare_fn((const void*)fn, false);
   if (st) return st;
@@ -1443,18 +1410,25 @@ extern "C" int sc_rfft2_noalloc(const float* x, void* xf, int count, int H, int 
   rp.nblk = pl.row_nblk;
   // the same one-time opt-in to the device's shared-memory maximum as every
   // other launch of these kernels (never lowered per call)
-  if ((st = prepare_fn((const void*)row_kernel<ROW_FWD_REAL, 0>, false))) return st;
-  if ((st = prepare_fn((const void*)col_kernel<COL_FWD, 0>, false))) return st;
-  row_kernel<ROW_FWD_REAL, 0><<<dim3(rp.nblk, count), (SC_ROW_THREADS / rp.gsz) * rp.gsz,
-                                 pl.rowg_smem, s>>>(rp);
-  CU_TRY(cudaGetLastError());
+  const RowFn rfn = row_fn<ROW_FWD_REAL>(0);  // the runtime-plan instantiations
+  const ColFn cfn = col_fn<COL_FWD>(0);
+  if ((st = prepare_fn((const void*)rfn, false))) return st;
+  if ((st = prepare_fn((const void*)cfn, false))) return st;
+  {
+    void* args[] = {&rp};
+    CU_TRY(cudaLaunchKernel((const void*)rfn, dim3(rp.nblk, count),
+                            dim3((SC_ROW_THREADS / rp.gsz) * rp.gsz), args, pl.rowg_smem, s));
+  }
   ColParams cp = {};
   cp.g = pl.g; cp.ph = pl.ph; cp.twH = tw + W; cp.twW = tw; cp.F = (float2*)xf;
   cp.gsz = pl.colg_g;
   cp.Hs = pl.Hs;
   cp.G = 1;
-  col_kernel<COL_FWD, 0><<<dim3(1, pl.col_ntiles, count), pl.colg_NT, pl.colg_smem, s>>>(cp);
-  CU_TRY(cudaGetLastError());
+  {
+    void* args[] = {&cp};
+    CU_TRY(cudaLaunchKernel((const void*)cfn, dim3(1, pl.col_ntiles, count), dim3(pl.colg_NT),
+                            args, pl.colg_smem, s));
+  }
   g_launches += 4;
   return SC_OK;
 }

@@ -128,6 +128,13 @@ typedef struct sc_options {
   int no_bndry_cross;   /* NoBndryCross: zero the last Kr - 1 rows and Kc - 1
                            columns of every map (filters crossing the bottom /
                            right boundary); neither touches the AMS map */
+  int warm_start;       /* 0: start from Y = U = 0 (or U0) at rho0.  1: continue
+                           the state an earlier solve of the same problem left
+                           in this workspace (iterates, rho, iteration count;
+                           max_iter more iterations), re-reading D and S (a
+                           dictionary update between calls, as in dictionary
+                           learning).  2: as 1, with D and S unchanged (their
+                           spectra in the workspace are reused). */
 } sc_options;
 
 /* L1 weight layouts. */
@@ -156,7 +163,7 @@ typedef struct sc_problem {
 } sc_problem;
 
 typedef struct sc_result {
-  int iterations;        /* largest iteration count over the batch */
+  int iterations;        /* largest iteration count of this call over the batch */
   double rho;            /* final rho of image 0 */
   double r, s;           /* final (normalised) residuals of image 0 */
 } sc_result;
@@ -183,8 +190,9 @@ int sc_cbpdn_solve_batch(const sc_problem *probs, int nprob, const sc_options *o
 /* Values per image and iteration in the statistics (sc_read_state). */
 #define SC_ITSTAT_FIELDS 8
 
-/* Per-image iteration counts / final rho / itstat after a solve, copied from
- * the workspace of that solve (host pointers; itstat may be NULL).  itstat is
+/* Per-image iteration counts (of the last solve call on this workspace) /
+ * final rho / itstat after a solve, copied from the workspace of that solve
+ * (host pointers; itstat may be NULL).  itstat is
  * (B, max_iter, 8) doubles per iteration: r, s, rho, eps_pri, eps_dua, then
  * the functional at Y, its data fidelity 0.5 ||sum_m d_m * y_m - s||^2 and
  * its L1 sum ||w y||_1 (the reference's Verbose columns, cbpdn.cu:438-517;

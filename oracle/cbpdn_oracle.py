@@ -275,7 +275,7 @@ def y_step(V, prob: Problem, rho, m0, wl1):
 
 
 def admm(prob: Problem, res: Resolved, xi: float, record=True, Y0=None, U0=None,
-         emulate_ref_rescale=False):
+         emulate_ref_rescale=False, rho_start=None, k_start=0):
     """Run the CBPDN / CBPDN-GradReg ADMM iterations in float64.
 
     Loop structure: cbpdn.cu:319-567 (grd: cbpdn_grd.cu:358-606).
@@ -291,6 +291,11 @@ def admm(prob: Problem, res: Resolved, xi: float, record=True, Y0=None, U0=None,
       U'    = U + Xr - Y'
       r = ||X - Y'||, s = rho ||Y - Y'||, norms of X, Y', U'  (695-783)
       stopping test and adaptive rho                       (cbpdn.cu:405-559)
+
+    Y0, U0, rho_start and k_start continue an earlier run (its returned Y,
+    U, rho and iteration count), as sporco's solve() continues its state:
+    the iteration numbers (which the adaptive-rho period tests) go on from
+    k_start, and MaxMainIter more iterations run.
     """
     D, S = prob.D, prob.S
     M = D.shape[0]
@@ -306,12 +311,12 @@ def admm(prob: Problem, res: Resolved, xi: float, record=True, Y0=None, U0=None,
         wg = np.asarray(prob.wgrd, dtype=np.float64).reshape(M, 1, 1)
     wl1 = np.broadcast_to(np.asarray(prob.wl1, dtype=np.float64), (M, H, W))
     alpha = res.RelaxParam
-    rho = res.rho0
+    rho = res.rho0 if rho_start is None else rho_start
     Y = np.zeros((M, H, W)) if Y0 is None else np.array(Y0, dtype=np.float64)
     U = np.zeros((M, H, W)) if U0 is None else np.array(U0, dtype=np.float64)
     hist = {"r": [], "s": [], "rho": [], "epri": [], "edua": []}
-    k = 0
-    for k in range(1, res.MaxMainIter + 1):
+    k = k_start
+    for k in range(k_start + 1, k_start + res.MaxMainIter + 1):
         b = DSf + rho * rfft2(Y - U)
         if grd:
             d = prob.mu * wg * Gh + rho
@@ -507,7 +512,7 @@ def _ams(D, opt, grd):
 
 
 def _run(Dk, S, W, lmbda, mu, opt, grd, wl1=None, wg=None, return_info=False,
-         emulate_ref_rescale=False, lean_chunk=0):
+         emulate_ref_rescale=False, lean_chunk=0, start=None):
     Dk = np.asarray(Dk, dtype=np.float32)
     S = np.asarray(S, dtype=np.float32)
     M = Dk.shape[2]
@@ -536,36 +541,41 @@ def _run(Dk, S, W, lmbda, mu, opt, grd, wl1=None, wg=None, return_info=False,
     if lean_chunk > 0:
         Y, info = admm_lean(prob, res, rsdl_target(res, lmbda), chunk=lean_chunk)
     else:
+        cont = {}
+        if start is not None:  # continue the state of an earlier run's info
+            cont = dict(Y0=start["Y"], U0=start["U"], rho_start=start["rho"],
+                        k_start=start["iterations"])
         Y, info = admm(prob, res, rsdl_target(res, lmbda),
-                       emulate_ref_rescale=emulate_ref_rescale)
+                       emulate_ref_rescale=emulate_ref_rescale, **cont)
     X = np.moveaxis(Y, 0, 2)
     return (X, info) if return_info else X
 
 
 def cbpdn(D, S, lmbda, opt, dev=0, return_info=False, emulate_ref_rescale=False,
-          lean_chunk=0):
+          lean_chunk=0, start=None):
     """Oracle for sporco_cuda.cbpdn.cbpdn (cbpdn.pyx:86-102).  lean_chunk > 0:
-    the map-chunked iterations of admm_lean (large problems)."""
+    the map-chunked iterations of admm_lean (large problems); start: the
+    info of an earlier run to continue (warm start)."""
     return _run(D, S, None, lmbda, 0.0, opt, False, return_info=return_info,
-                emulate_ref_rescale=emulate_ref_rescale, lean_chunk=lean_chunk)
+                emulate_ref_rescale=emulate_ref_rescale, lean_chunk=lean_chunk, start=start)
 
 
 def cbpdnmsk(D, S, W, lmbda, opt, dev=0, return_info=False, emulate_ref_rescale=False,
-             lean_chunk=0):
+             lean_chunk=0, start=None):
     """Oracle for sporco_cuda.cbpdn.cbpdnmsk (cbpdn.pyx:108-152)."""
     Di, wl1, _ = _ams(np.asarray(D, dtype=np.float32), opt, False)
     out = _run(Di, S, W, lmbda, 0.0, opt, False, wl1=wl1, return_info=return_info,
-               emulate_ref_rescale=emulate_ref_rescale, lean_chunk=lean_chunk)
+               emulate_ref_rescale=emulate_ref_rescale, lean_chunk=lean_chunk, start=start)
     if return_info:
         return out[0][..., 1:], out[1]
     return out[..., 1:]
 
 
 def cbpdngrd(D, S, lmbda, mu, opt, dev=0, return_info=False, emulate_ref_rescale=False,
-             lean_chunk=0):
+             lean_chunk=0, start=None):
     """Oracle for sporco_cuda.cbpdn.cbpdngrd (cbpdn.pyx:207-223)."""
     return _run(D, S, None, lmbda, mu, opt, True, return_info=return_info,
-                emulate_ref_rescale=emulate_ref_rescale, lean_chunk=lean_chunk)
+                emulate_ref_rescale=emulate_ref_rescale, lean_chunk=lean_chunk, start=start)
 
 
 def cbpdngrdmsk(D, S, W, lmbda, mu, opt, dev=0, return_info=False,

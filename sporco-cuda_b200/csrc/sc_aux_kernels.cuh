@@ -56,8 +56,9 @@ __global__ void finalize_kernel(const double* __restrict__ partials, int nblk,
     edua /= sn;
   }
   const int k = S.k + 1;
+  const int kc = k - S.k0;  // iterations of this solve call
   if (F.itstat) {
-    double* it = F.itstat + ((size_t)b * F.max_iter + (k - 1)) * SC_ITSTAT_FIELDS;
+    double* it = F.itstat + ((size_t)b * F.max_iter + (kc - 1)) * SC_ITSTAT_FIELDS;
     it[0] = r; it[1] = s; it[2] = rho; it[3] = epri; it[4] = edua;
   }
   double rsf = 1.0;
@@ -83,7 +84,7 @@ __global__ void finalize_kernel(const double* __restrict__ partials, int nblk,
   // by 1/rsf (U <- U / rsf, cbpdn.cu:543-549)
   S.uscale = 1.0 / rsf;
   S.k = k;
-  bool done = (r <= epri && s <= edua) || k >= F.max_iter;
+  bool done = (r <= epri && s <= edua) || kc >= F.max_iter;
   if (!isfinite(r) || !isfinite(s)) {
     S.status = 5;  // SC_ERR_NONFINITE
     done = true;
@@ -108,8 +109,20 @@ __global__ void init_state_kernel(ImgState* st, const float* rho0, int B, int* n
   s.k = 0;
   s.done = 0;
   s.status = 0;
-  s.pad = 0;
+  s.k0 = 0;
   st[b] = s;
+}
+
+// A warm-started solve call continues the state of the previous one: rho,
+// the iterates and the iteration count carry over; the call's own cap counts
+// from the current count, and the finished flags start afresh.
+__global__ void warm_state_kernel(ImgState* st, int B, int* ndone) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b == 0 && ndone) *ndone = 0;
+  if (b >= B) return;
+  st[b].k0 = st[b].k;
+  st[b].done = 0;
+  st[b].status = 0;
 }
 
 // tw[j] = exp(-2 pi i j / n), evaluated in double precision.
@@ -236,7 +249,7 @@ __global__ void objective_final_kernel(const double* __restrict__ pspec,
                                        double* itstat, int max_iter, int B) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= B) return;
-  const int k = st[b].k;
+  const int k = st[b].k - st[b].k0;  // iteration of this solve call
   if (k < 1 || k > max_iter) return;
   double df = 0.0, gr = 0.0, l1 = 0.0;
   for (int i = 0; i < nblk; ++i) {

@@ -35,10 +35,10 @@ struct ImgState {
   double r, s;   // last residuals (normalised unless StdResiduals)
   double epri, edua;
   double nX, nY, nU;
-  int k;         // iterations completed
+  int k;         // iterations completed (over all solves of a warm-started state)
   int done;      // 1: converged, iteration cap reached, or failed
   int status;    // sc_status of this image
-  int pad;
+  int k0;        // k at the start of the current solve call (its cap counts from here)
 };
 
 // Scalar options the finalize kernel needs.

@@ -607,14 +607,18 @@ struct Solve {
                                                    : COL_SOLVE_P;
     float2* Erows = (float2*)((unsigned char*)workspace + pl.off_E);
 
-    twiddle_kernel<<<(g.W + 255) / 256, 256, 0, s>>>(twW, g.W);
-    twiddle_kernel<<<(g.H + 255) / 256, 256, 0, s>>>(twH, g.H);
-    CU_TRY(cudaGetLastError());
-    g_launches += 2;
+    // warm_start 2: the spectra of D and S in the workspace are still valid
+    const bool spectra = o->warm_start != 2;
+    if (spectra) {
+      twiddle_kernel<<<(g.W + 255) / 256, 256, 0, s>>>(twW, g.W);
+      twiddle_kernel<<<(g.H + 255) / 256, 256, 0, s>>>(twH, g.H);
+      CU_TRY(cudaGetLastError());
+      g_launches += 2;
+    }
 
     // Dictionary spectrum: rfft2 of the zero-padded filters (cuda_Pad_Dict +
     // R2C, cbpdn.cu:277-289), computed without materialising the padding.
-    {
+    if (spectra) {
       RowParams r = {};
       r.g = g; r.g.B = 1;
       r.pw = pl.pw; r.twW = twW; r.F = Dh; r.D = p->D; r.Kr = p->Kr; r.Kc = p->Kc;
@@ -632,7 +636,7 @@ struct Solve {
       ++g_launches;
     }
     // Signal spectra (B images, one map each).
-    {
+    if (spectra) {
       RowParams r = {};
       r.g = g; r.g.M = 1;
       r.pw = pl.pw; r.twW = twW; r.F = Sh; r.src = p->S;
@@ -644,8 +648,14 @@ struct Solve {
       c.g = g; c.g.M = 1; c.ph = pl.ph; c.twH = twH; c.twW = twW; c.F = Sh;
       if ((st = launch_col<COL_FWD>(pl, c, g.B, s))) return st;
     }
-    if ((st = init_iterates())) return st;
-    init_state_kernel<<<(g.B + 127) / 128, 128, 0, s>>>(sts, p->rho0, g.B, ndone);
+    if (o->warm_start) {
+      // continue the state an earlier solve of this problem left in the
+      // workspace: iterates, spectra of Y - U, rho, iteration count
+      warm_state_kernel<<<(g.B + 127) / 128, 128, 0, s>>>(sts, g.B, ndone);
+    } else {
+      if ((st = init_iterates())) return st;
+      init_state_kernel<<<(g.B + 127) / 128, 128, 0, s>>>(sts, p->rho0, g.B, ndone);
+    }
     xi_kernel<<<(g.B + 127) / 128, 128, 0, s>>>(xi, p->lmbda, g.B, o->rsdl_target,
                                                  o->std_residuals);
     CU_TRY(cudaGetLastError());
@@ -672,7 +682,7 @@ struct Solve {
     // solve early; the host then never waits on the device mid-solve.
     can_stop = o->rel_tol > 0.f || o->abs_tol > 0.f;
     finished = o->max_iter <= 0;
-    if (tune && autotune_enabled() && o->max_iter > 0) {
+    if (tune && !o->warm_start && autotune_enabled() && o->max_iter > 0) {
       if ((st = tune_col())) return st;
     }
     return SC_OK;
@@ -926,14 +936,14 @@ struct Solve {
     ImgState h0;
     CU_TRY(cudaMemcpyAsync(&h0, sts, sizeof(ImgState), cudaMemcpyDeviceToHost, s));
     CU_TRY(cudaStreamSynchronize(s));
-    res->iterations = h0.k;
+    res->iterations = h0.k - h0.k0;
     res->rho = h0.rho;
     res->r = h0.r;
     res->s = h0.s;
     if (B > 1) {
       std::vector<ImgState> hs(B);
       CU_TRY(cudaMemcpy(hs.data(), sts, sizeof(ImgState) * B, cudaMemcpyDeviceToHost));
-      for (auto& x : hs) res->iterations = std::max(res->iterations, x.k);
+      for (auto& x : hs) res->iterations = std::max(res->iterations, x.k - x.k0);
       for (auto& x : hs)
         if (x.status) return set_status(x.status, "non-finite residual");
     }
@@ -1274,7 +1284,7 @@ extern "C" int sc_read_state(const sc_problem* p, const sc_options* o, const voi
                            cudaMemcpyDeviceToHost, s));
   CU_TRY(cudaStreamSynchronize(s));
   for (int b = 0; b < pl.g.B; ++b) {
-    if (iterations) iterations[b] = hs[b].k;
+    if (iterations) iterations[b] = hs[b].k - hs[b].k0;
     if (rho) rho[b] = hs[b].rho;
   }
   return SC_OK;

@@ -87,6 +87,7 @@ class ScOptions(C.Structure):
         ("profile", C.c_int),
         ("nonneg", C.c_int),
         ("no_bndry_cross", C.c_int),
+        ("warm_start", C.c_int),
     ]
 
 

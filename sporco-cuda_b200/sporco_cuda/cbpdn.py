@@ -40,7 +40,7 @@ from . import _lib
 F32 = np.float32
 
 __all__ = ["cbpdn", "cbpdnmsk", "cbpdngrd", "cbpdngrdmsk", "SolverError",
-           "solve_device", "resolve_options"]
+           "solve_device", "resolve_options", "ConvBPDN", "cbpdn_batched"]
 
 SolverError = _lib.SolverError
 
@@ -253,15 +253,45 @@ class DeviceSolve:
         self.ws = ws
         self.keep = keep
         self.result = _lib.ScResult()
+        self.last_iters = opts.max_iter  # MaxMainIter of the last run (its itstat rows)
 
-    def run(self, stream=None):
+    def run(self, stream=None, warm=False, iters=None):
+        """Launch the solve on `stream` (default: the current torch stream)
+        and return Y (B, M, H, W).
+
+        warm=False starts from Y = U = 0 at rho0 (or from the warm-start
+        iterates given to prepare_device).  warm=True continues the state
+        the previous run left in the workspace (iterates, rho, iteration
+        count, as sporco's solve() continues its own), re-reading D and S
+        (so a dictionary changed with :meth:`set_dict` in between is used);
+        warm="same" also keeps their spectra (D and S unchanged).  iters:
+        iterations of this run (default MaxMainIter)."""
         import torch
         s = stream if stream is not None else torch.cuda.current_stream()
-        st = _lib.sc_cbpdn_solve(C.byref(self.prob), C.byref(self.opts),
-                                 C.c_void_p(self.ws.data_ptr()), self.ws.numel(),
-                                 C.byref(self.result), C.c_void_p(s.cuda_stream))
+        keep_iters, keep_warm = self.opts.max_iter, self.opts.warm_start
+        if iters is not None:
+            self.opts.max_iter = int(iters)
+        self.opts.warm_start = 2 if warm == "same" else (1 if warm else 0)
+        try:
+            st = _lib.sc_cbpdn_solve(C.byref(self.prob), C.byref(self.opts),
+                                     C.c_void_p(self.ws.data_ptr()), self.ws.numel(),
+                                     C.byref(self.result), C.c_void_p(s.cuda_stream))
+        finally:
+            self.last_iters = self.opts.max_iter
+            self.opts.max_iter, self.opts.warm_start = keep_iters, keep_warm
         _lib.check(st)
         return self.keep["Y"]
+
+    def set_dict(self, Dm):
+        """Replace the dictionary (M, Kr, Kc) in place (same shape); the next
+        run, cold or warm=True, uses it."""
+        import torch
+        D = self.keep["D"]
+        Dm = torch.as_tensor(Dm, device=D.device, dtype=torch.float32)
+        if Dm.shape != D.shape:
+            raise ValueError("dictionary shape %s differs from %s" % (tuple(Dm.shape),
+                                                                     tuple(D.shape)))
+        D.copy_(Dm)
 
     def state(self):
         import torch
@@ -269,9 +299,11 @@ class DeviceSolve:
         iters = (C.c_int * B)()
         rho = (C.c_double * B)()
         it = None
-        if self.opts.record_itstat:
-            it = np.zeros((B, max(1, self.opts.max_iter), ITSTAT_FIELDS), dtype=np.float64)
-        st = _lib.sc_read_state(C.byref(self.prob), C.byref(self.opts),
+        opts = _lib.ScOptions.from_buffer_copy(self.opts)
+        opts.max_iter = self.last_iters  # the itstat layout of the last run
+        if opts.record_itstat:
+            it = np.zeros((B, max(1, opts.max_iter), ITSTAT_FIELDS), dtype=np.float64)
+        st = _lib.sc_read_state(C.byref(self.prob), C.byref(opts),
                                 C.c_void_p(self.ws.data_ptr()), iters, rho,
                                 it.ctypes.data_as(C.POINTER(C.c_double)) if it is not None else None,
                                 C.c_void_p(torch.cuda.current_stream().cuda_stream))
@@ -316,7 +348,7 @@ def prepare_device(Dm, S, lmbda, opt, mu=0.0, grd=False, l1=1.0, gw=1.0, mask=No
     rho0 = torch.as_tensor(rho0, device=dev, dtype=torch.float32).reshape(-1).expand(B).contiguous()
     prob = _lib.ScProblem()
     prob.B, prob.H, prob.W, prob.M, prob.Kr, prob.Kc = B, H, W, M, Kr, Kc
-    keep = {"D": Dm.contiguous(), "S": S.contiguous(), "lam": lam, "rho0": rho0}
+    keep = {"D": Dm.contiguous().clone(), "S": S.contiguous(), "lam": lam, "rho0": rho0}
     prob.D = keep["D"].data_ptr()
     prob.S = keep["S"].data_ptr()
     prob.lmbda = lam.data_ptr()
@@ -464,6 +496,95 @@ def cbpdngrdmsk(D, S, W, lmbda, mu, opt, dev=0):
     X = _host_solve(np.ascontiguousarray(np.rollaxis(Di, 2, 0)), np.ascontiguousarray(S),
                     np.ascontiguousarray(W, dtype=np.int32), lmbda, mu, opt, l1, g, dev, True)
     return np.rollaxis(X, 0, 3)[..., 1:]
+
+
+# ------------------------------------------------- persistent (warm) solver --
+
+class ConvBPDN:
+    """A persistent solver object for the outer loop of dictionary learning.
+
+    No counterpart in the reference, whose functions solve from zero on every
+    call; its main external caller, sporco's ConvBPDNDictLearn, alternates a
+    few ADMM iterations of the coefficient step with a dictionary update and
+    continues the coefficient step's state (iterates, rho, iteration count)
+    across them.  This object keeps that state in device memory:
+
+        b = ConvBPDN(D, S, lmbda, opt)      # (Kr, Kc, M), (H, W)
+        X = b.solve()                      # MaxMainIter iterations from zero
+        b.setdict(D2)                      # new filters, same shape
+        X = b.solve()                      # MaxMainIter more, warm
+        X = b.getcoef()
+
+    ``mu`` (not None) adds the gradient term of ``cbpdngrd``; a mask ``W``
+    gives the AMS problem of ``cbpdnmsk`` / ``cbpdngrdmsk`` (impulse filter
+    prepended, its map dropped from the results).  Results are numpy arrays
+    for numpy inputs and torch tensors for torch inputs."""
+
+    def __init__(self, D, S, lmbda, opt, mu=None, W=None, dev=0):
+        import torch
+        self._torch = _is_torch(D)
+        device = D.device if self._torch else torch.device("cuda", dev)
+        Dt = torch.as_tensor(D, device=device, dtype=torch.float32)
+        St = torch.as_tensor(S, device=device, dtype=torch.float32)
+        if Dt.ndim != 3 or St.ndim != 2:
+            raise ValueError("D must be (Kr, Kc, M) and S must be (H, W)")
+        self._grd = mu is not None
+        self._ams = W is not None
+        l1 = _opt_get(opt, "L1Weight")
+        gw = _opt_get(opt, "GradWeight") if self._grd else 1.0
+        mask = None
+        if self._ams:
+            l1, gw = _ams_weights(St.shape, Dt.shape[2] + 1,
+                                  {"L1Weight": _np(l1), "GradWeight": _np(gw)}, self._grd)
+            mask = torch.as_tensor(W, device=device).to(torch.int32).reshape(1, *St.shape)
+        if hasattr(l1, "ndim") and np.ndim(l1) == 3:
+            l1 = np.ascontiguousarray(np.rollaxis(_np(l1), 2, 0))
+        self._ds = prepare_device(self._dict(Dt), St[None], lmbda, opt,
+                                  mu=0.0 if mu is None else mu, grd=self._grd, l1=l1, gw=gw,
+                                  mask=mask, record_itstat=bool(_opt_get(opt, "Verbose")))
+        self._started = False
+
+    def _dict(self, Dt):
+        import torch
+        if self._ams:
+            d0 = torch.zeros((Dt.shape[0], Dt.shape[1], 1), dtype=Dt.dtype, device=Dt.device)
+            d0[0, 0] = 1.0
+            Dt = torch.cat((d0, Dt), dim=2)
+        return Dt.permute(2, 0, 1).contiguous()
+
+    def solve(self, iters=None):
+        """MaxMainIter (or `iters`) ADMM iterations, continuing the state of
+        the previous call; returns the coefficient maps (H, W, M)."""
+        self._ds.run(warm=self._started, iters=iters)
+        self._started = True
+        return self.getcoef()
+
+    def setdict(self, D):
+        """Replace the filters (Kr, Kc, M) (same shape); the next solve uses
+        them and keeps the iterates, rho and the iteration count."""
+        import torch
+        Dt = torch.as_tensor(D, device=self._ds.keep["D"].device, dtype=torch.float32)
+        self._ds.set_dict(self._dict(Dt))
+
+    def getcoef(self):
+        X = self._ds.keep["Y"][0].permute(1, 2, 0)
+        if self._ams:
+            X = X[..., 1:]
+        return X if self._torch else X.contiguous().cpu().numpy()
+
+    def getitstat(self):
+        """Per-iteration statistics of the last solve (recorded when the
+        options ask for Verbose): dict of arrays r, s, rho, epri, edua, fnc,
+        dfid, regl1."""
+        st = self._ds.state()
+        if st["itstat"] is None:
+            return None
+        k = st["iterations"][0]
+        return {n: st["itstat"][0, :k, i].copy() for i, n in enumerate(ITSTAT_NAMES)}
+
+    @property
+    def rho(self):
+        return self._ds.state()["rho"][0]
 
 
 # ------------------------------------------------------------- batched form --

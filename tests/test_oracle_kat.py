@@ -220,3 +220,17 @@ def test_torch_chunked_objective_equals_numpy_objective():
         J = O.objective(D, S, Y, 0.2, **kw)
         Jt = OT.objective(D, S, Y, 0.2, chunk=3, **kw)
         assert abs(J - Jt) <= 1e-12 * abs(J)
+
+
+def test_continued_run_equals_one_run():
+    """A run continued from an earlier run's state (the warm start of a
+    dictionary-learning outer loop) takes the iterates of one longer run."""
+    rng = np.random.default_rng(14)
+    D = rng.standard_normal((4, 4, 5)).astype(np.float32)
+    S = rng.standard_normal((20, 18)).astype(np.float32)
+    opt = {"MaxMainIter": 30, "RelStopTol": 0.0, "AutoRho": {"Enabled": True, "Period": 3}}
+    X, info = O.cbpdn(D, S, 0.1, opt, return_info=True)
+    _, i1 = O.cbpdn(D, S, 0.1, dict(opt, MaxMainIter=13), return_info=True)
+    X2, i2 = O.cbpdn(D, S, 0.1, dict(opt, MaxMainIter=17), return_info=True, start=i1)
+    np.testing.assert_array_equal(X2, X)
+    assert i2["iterations"] == 30 and i2["rho"] == info["rho"]

@@ -735,6 +735,16 @@ def run_adjoint(args, cfg, rank, world, local_rank):
     peak, peak_kind = measured_peaks()
     if rank != 0:
         return None
+    # the forward's graded bytes over its device time (K iterations of B images)
+    fwd_bytes = graded_bytes(H, W, M, B) * cfg["iters"]
+    f_step = f_ms / args.steps
+    roof = {"bound": "hbm", "kernel": "unrolled forward (K ADMM iterations, B images)",
+            "achieved": fwd_bytes / (f_step / 1e3) / 1e9, "peak": peak, "peak_kind": peak_kind,
+            "unit": "GB/s", "frac": fwd_bytes / (f_step / 1e3) / 1e9 / peak, "traffic": None,
+            "fused_forward_frac": fwd_bytes / (fused_ms / 1e3) / 1e9 / peak}
+    cpu = rel = None
+    if world == 1 and not args.no_cpu:
+        cpu, rel = adjoint_cpu_leg(cfg, Dk[..., :].float(), S[0], Sc[0])
     return {
         "metric": METRIC, "value": value, "unit": "image-iter/s (forward+backward)",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -747,9 +757,50 @@ def run_adjoint(args, cfg, rank, world, local_rank):
         "backward_over_forward": b_ms / f_ms,
         "fused_forward_solve_ms": fused_ms,
         "backward_over_fused_forward": (b_ms / args.steps) / fused_ms,
-        "e2e": None, "roofline": None, "cpu_baseline": None, "gpu_launches": launches,
-        "clocks": clk.summary(),
+        "e2e": None, "roofline": roof, "rel_err": rel, "cpu_baseline": cpu,
+        "gpu_launches": launches, "clocks": clk.summary(),
     }
+
+
+def adjoint_cpu_leg(cfg, Dk, S1, Sc1, iters=10):
+    """Config 3 on the host: torch FP64 autograd of the plain unrolled solve
+    (the adjoint oracle) for one image and `iters` iterations, timed
+    (forward + backward), and the GPU adjoint's gradients on the same sample
+    against it."""
+    import torch
+    import sporco_cuda.adjoint as adj
+    from oracle import adjoint_oracle as A
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    lam = float(np.float32(cfg["lmbda"]))
+    rho = float(np.float32(50 * lam + 1))
+    alpha = float(np.float32(1.8))
+    Dd = Dk.detach().double().cpu().requires_grad_(True)
+    Sd = S1.detach().double().cpu()[None].requires_grad_(True)
+    t0 = time.perf_counter()
+    L = A.loss(Dd, Sd, Sc1.detach().double().cpu()[None], lam, rho, alpha, iters, 0.01)
+    L.backward()
+    dt = time.perf_counter() - t0
+    cpu = {"value": iters / dt, "unit": "image-iter/s (forward+backward)", "cores": threads,
+           "kind": "port",
+           "sample": "one %dx%d image, M=%d, %d unrolled iterations: FP64 torch autograd of the "
+                     "unrolled restatement (%d threads)" % (cfg["H"], cfg["W"], cfg["M"], iters,
+                                                          threads)}
+    opt = {"MaxMainIter": iters, "RelStopTol": 0.0, "RelaxParam": 1.8, "rho": None,
+           "AutoRho": {"Enabled": False}}
+    Dg = Dk.detach().clone().requires_grad_(True)
+    Sg = S1.detach()[None].clone().requires_grad_(True)
+    X = adj.cbpdn_unrolled(Dg, Sg, cfg["lmbda"], opt)
+    R = adj.reconstruct(Dg, X)
+    Lg = torch.sum((R - Sc1[None]) ** 2) + 0.01 * torch.sum(torch.abs(X))
+    Lg.backward()
+    rel = {"iterations": iters, "images": 1,
+           "gD": float(torch.linalg.norm(Dg.grad.double().cpu() - Dd.grad) /
+                       torch.linalg.norm(Dd.grad)),
+           "gS": float(torch.linalg.norm(Sg.grad.double().cpu() - Sd.grad) /
+                       torch.linalg.norm(Sd.grad)),
+           "reference": "FP64 torch autograd of the unrolled restatement"}
+    return cpu, rel
 
 
 def run_reference(args, cfg, rank, world):

@@ -38,7 +38,9 @@ RowFn sc_row_fn_aux(int mode, int n);
 ColFn sc_col_fn_conv(int mode, int n);
 // sc_inst_col_solve.cu: COL_SOLVE_P, COL_SOLVE, COL_SOLVE_W
 ColFn sc_col_fn_solve(int mode, int n);
-// sc_inst_col_aux.cu: COL_SOLVE_X, COL_ADJ, COL_FWD, COL_INV
+// sc_inst_col_aux.cu: COL_SOLVE_X, COL_ADJ, COL_FWD, COL_INV, and, for
+// compiled lengths below 512 only, COL_SOLVE_C8T, COL_SOLVE_C16T, COL_ADJ_C8,
+// COL_ADJ_C16
 ColFn sc_col_fn_aux(int mode, int n);
 
 // The table entry of MODE for length n.

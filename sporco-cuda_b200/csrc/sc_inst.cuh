@@ -22,3 +22,14 @@ ColFn col_table(int n) {
 #undef SC_COL_CASE
   return col_kernel<MODE, 0>;
 }
+
+// The same over the compiled lengths below 512 only (radix-8 column plans,
+// at most 8 rows per thread), for modes used only there; nullptr otherwise.
+#define SC_SPEC_COL_SMALL(X) X(16) X(32) X(64) X(128) X(256) X(48) X(96) X(192) X(384)
+template <int MODE>
+ColFn col_table_small(int n) {
+#define SC_COL_CASE(k) case k: return col_kernel<MODE, k>;
+  switch (n) { SC_SPEC_COL_SMALL(SC_COL_CASE) default: break; }
+#undef SC_COL_CASE
+  return nullptr;
+}

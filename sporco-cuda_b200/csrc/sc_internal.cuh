@@ -116,9 +116,13 @@ struct ColParams {
   ImgState* st;
   float2* Xtr;             // COL_SOLVE_X: x^ also written here (B, M, H, Wp)
   // adjoint (COL_ADJ)
-  const float2* Xh;        // (B, M, H, Wp) x^ of the step
+  const float2* Xh;        // (B, M, H, Wp) x^ of the step (COL_ADJ_C*: the row spectra of X)
   float2* gDh;             // (B, M, H, Wp) dictionary-gradient spectra, accumulated
   float2* gSh;             // (B, H, Wp) signal-gradient spectra, accumulated
+  // convolution-form adjoint
+  float2* SCtr;            // (B, H, Wp) IFFTcol(S^ - cb) / rho of the step (written by
+                           // COL_SOLVE_C*T, read by COL_ADJ_C*)
+  float2* gE;              // (B, M, Kr, Wp) dictionary gradient as filter-row spectra
 };
 
 enum RowMode {
@@ -140,19 +144,33 @@ enum RowMode {
 // the adjoint).  COL_ADJ: adjoint of the plain cbpdn
 // solve (one d = rho): column FFT, Q^ = A^{-1} G^, gradient accumulation,
 // inverse column FFT.
+// COL_SOLVE_C8T / COL_SOLVE_C16T: COL_SOLVE_C8 / C16 that also keep, for the
+// adjoint, the column pass's output (the row spectra of X) in ColParams::Xtr
+// and the tile's IFFTcol(S^ - cb) / rho in ColParams::SCtr.  COL_ADJ_C8 /
+// COL_ADJ_C16: the adjoint of the plain solve in the same convolution form
+// (the dictionary gradient accumulated as correlations over the Kr filter
+// rows, ColParams::gE).
 enum ColMode {
   COL_SOLVE = 0, COL_FWD = 1, COL_INV = 2, COL_SOLVE_W = 3, COL_ADJ = 4, COL_SOLVE_X = 5,
-  COL_SOLVE_P = 6, COL_SOLVE_C8 = 7, COL_SOLVE_C16 = 8, COL_SOLVE_G16 = 9
+  COL_SOLVE_P = 6, COL_SOLVE_C8 = 7, COL_SOLVE_C16 = 8, COL_SOLVE_G16 = 9,
+  COL_SOLVE_C8T = 10, COL_SOLVE_C16T = 11, COL_ADJ_C8 = 12, COL_ADJ_C16 = 13
 };
 // Filter rows (taps) of the convolution column solves.
 __host__ __device__ constexpr int col_taps(int mode) {
-  return mode == COL_SOLVE_C8 ? 8 : (mode == COL_SOLVE_C16 || mode == COL_SOLVE_G16) ? 16 : 0;
+  return (mode == COL_SOLVE_C8 || mode == COL_SOLVE_C8T || mode == COL_ADJ_C8) ? 8
+         : (mode == COL_SOLVE_C16 || mode == COL_SOLVE_G16 || mode == COL_SOLVE_C16T ||
+            mode == COL_ADJ_C16)
+             ? 16
+             : 0;
+}
+// The convolution-form adjoint.
+__host__ __device__ constexpr bool col_adj_conv(int mode) {
+  return mode == COL_ADJ_C8 || mode == COL_ADJ_C16;
 }
 // Modes that launch as a cluster over the maps of one column tile.
 __host__ __device__ constexpr bool col_clustered(int mode) {
   return mode == COL_SOLVE || mode == COL_SOLVE_W || mode == COL_SOLVE_X || mode == COL_ADJ ||
-         mode == COL_SOLVE_P || mode == COL_SOLVE_C8 || mode == COL_SOLVE_C16 ||
-         mode == COL_SOLVE_G16;
+         mode == COL_SOLVE_P || col_taps(mode) > 0;
 }
 
 __host__ __device__ inline size_t sc_align16(size_t x) { return (x + 15) & ~(size_t)15; }
@@ -179,6 +197,11 @@ __host__ __device__ inline size_t row_slot_bytes(int mode, int zlen, int W, int 
 // The convolution solves use three tiles and two staged filter-row tiles.
 __host__ __device__ inline size_t col_smem_bytes(int mode, int hlen) {
   const size_t tile = (size_t)SC_COL_TILE * hlen * 8;
-  return (col_clustered(mode) ? 3 * tile : tile) +
-         (size_t)2 * col_taps(mode) * SC_COL_TILE * 8;
+  // the convolution adjoint stages one more tile (the forward's SC trace)
+  // and keeps per-warp partial sums of the dictionary gradient (two maps)
+  return (col_clustered(mode) ? (col_adj_conv(mode) ? 4 : 3) * tile : tile) +
+         (size_t)2 * col_taps(mode) * SC_COL_TILE * 8 +
+         (col_adj_conv(mode) ? (size_t)2 * (SC_COL_MAX_THREADS / 32) * col_taps(mode) *
+                                   SC_COL_TILE * 8
+                             : 0);
 }

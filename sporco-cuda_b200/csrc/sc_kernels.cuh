@@ -798,7 +798,7 @@ col_kernel(ColParams P) {
       __syncthreads();
     }
     return;
-  } else if constexpr (MODE == COL_SOLVE_C8 || MODE == COL_SOLVE_C16 || MODE == COL_SOLVE_G16) {
+  } else if constexpr (col_taps(MODE) > 0) {
     // Plain solve (d = rho) with the column direction done by direct
     // convolution.  In the row-spectral domain (F = row spectra P_m of
     // (Y - U)_m) filter m is E_m(t, kc), t < Kr (the row spectra of its rows),
@@ -820,8 +820,27 @@ col_kernel(ColParams P) {
     // pass 2 transforms each map's tile forward and back (1/d varies along
     // the column) and adds the convolution term.  The column spectra are
     // neither written back nor the dictionary spectra read.
+    //
+    // COL_SOLVE_C8T / C16T (the adjoint's recomputation) also keep the pass's
+    // output (the row spectra of X) in Xtr and sc / rho in SCtr.
+    //
+    // COL_ADJ_C8 / C16: the adjoint of the plain solve, A = rho I + conj(Df)
+    // Df^T per frequency, in the same form.  F holds g_m, the row spectra of
+    // a gV; with G^_m = FFTcol(g_m):
+    //   cb = sum_m Df_m G^_m / (rho + Psum)     (pass 1 as above; gS^ += cb)
+    //   IFFTcol(Q^_m)(r) = (H g_m(r) - sum_t conj(E_m(t)) cb'(r + t)) / rho,
+    //   cb' = IFFTcol(cb)                        (pass 2, written to F)
+    // and the dictionary gradient (S^ - sum_j Df_j X^_j) conj(Q^_m) -
+    // cb conj(X^_m), needed only at the Kr filter rows after the inverse
+    // column transform, is a circular correlation there:
+    //   gE_m(t) += sum_s rho sc'(s + t) conj(q_m(s)) - cb'(s + t) conj(x_m(s)),
+    // sc' = SCtr and x_m = Xtr of the step (unnormalised; the caller scales),
+    // q_m the pass-2 output.  Each thread sums over its L rows, the column's
+    // threads are summed by shuffles and per-warp partials, in a fixed order.
     if constexpr (NH > 0) {
       constexpr bool GRD = MODE == COL_SOLVE_G16;
+      constexpr bool TRACE = MODE == COL_SOLVE_C8T || MODE == COL_SOLVE_C16T;
+      constexpr bool ADJ = col_adj_conv(MODE);
       constexpr int KMAX = col_taps(MODE);
       constexpr int L = EPT;  // rows per thread; g L = H for every compiled length
       constexpr int NW = L + KMAX - 1;  // window of the L outputs
@@ -830,6 +849,9 @@ col_kernel(ColParams P) {
       float2* Bt = stg + TL;      // spectrum tiles (pass 1: with A; pass 2: with Ct)
       float2* Ct = stg + 2 * TL;  // partial sums of this CTA
       float2* Es = stg + 3 * TL;  // [2][KMAX][T] filter rows
+      // ADJ: the forward's sc / rho tile, then per-warp correlation partials
+      float2* W4 = Es + 2 * KMAX * T;
+      float2* red = W4 + TL;      // [2][NT / 32][KMAX][T]
       auto issue_tile = [&](const float2* base, float2* dst) {
         for (int q = tid; q < 2 * H; q += NT) {
           const int kr = q >> 1, h = q & 1;
@@ -924,6 +946,7 @@ col_kernel(ColParams P) {
       if (m0 < m1) {
         issue_tile(Fi + (size_t)m0 * plane, Bt);
         issue_E(m0, Es);
+        if constexpr (ADJ) issue_tile(P.SCtr + (size_t)b * plane, W4);
       }
       cp_async_commit();
 
@@ -965,7 +988,17 @@ col_kernel(ColParams P) {
           const int sl = slot(kr) * T + cc;
           float2 v = make_float2(0.f, 0.f);
           if (colok) {
-            const float2 q = A[sl];  // sum_m Df_m Z^_m
+            const float2 q = A[sl];  // sum_m Df_m Z^_m (ADJ: sum_m Df_m G^_m)
+            if constexpr (ADJ) {
+              const float id = 1.f / (rho + __ldg(&P.Psum[(size_t)kr * Wp + c0 + cc]));
+              const float2 cb = make_float2(q.x * id, q.y * id);
+              if (rank == 0) {
+                float2* gs = P.gSh + (size_t)b * plane + (size_t)kr * Wp + c0 + cc;
+                const float2 o = *gs;
+                *gs = make_float2(o.x + cb.x, o.y + cb.y);
+              }
+              v = make_float2(cb.x, -cb.y);  // conj(cb)
+            } else {
             const float2 Sv = __ldg(&Sh[(size_t)kr * Wp + cc]);
             if constexpr (GRD) {
               // cb = (S^ Psum / d + rho q / d) / (1 + Psum / d)
@@ -981,6 +1014,7 @@ col_kernel(ColParams P) {
               const float2 cb = make_float2((Sv.x * sd + q.x) * qd, (Sv.y * sd + q.y) * qd);
               v = make_float2((Sv.x - cb.x) * irho, -(Sv.y - cb.y) * irho);  // conj(SC) / rho
             }
+            }
           }
           A[sl] = v;
         }
@@ -993,6 +1027,9 @@ col_kernel(ColParams P) {
         if (kr < H) {
           const int sl = slot(kr) * T + cc;
           A[sl].y = -A[sl].y;
+          // the forward's sc / rho of this step, for the adjoint
+          if (TRACE && rank == 0 && colok)
+            P.SCtr[(size_t)b * plane + (size_t)kr * Wp + c0 + cc] = A[sl];
         }
       }
       // ------------------------------------------------------------ pass 2
@@ -1005,8 +1042,10 @@ col_kernel(ColParams P) {
       float2 w[NW];
       auto load_window = [&]() {
 #pragma unroll
-        for (int j = 0; j < NW; ++j)
+        for (int j = 0; j < NW; ++j) {
           w[j] = (j < L + Kr - 1) ? A[rslot(j) * T + cc] : make_float2(0.f, 0.f);
+          if constexpr (ADJ) w[j] = make_float2(-w[j].x, -w[j].y);  // -cb'
+        }
       };
       if constexpr (!GRD) load_window();
       // rho / d at this thread's rows (GRD)
@@ -1062,12 +1101,80 @@ col_kernel(ColParams P) {
             }
           }
         }
+        if constexpr (ADJ) {
+#pragma unroll
+          for (int i = 0; i < L; ++i) o[i] = make_float2(o[i].x * irho, o[i].y * irho);  // q_m
+        }
         if (colok) {
           float2* dst = Fo + (size_t)m * plane + (size_t)r0 * Wp;
 #pragma unroll
           for (int i = 0; i < L; ++i) dst[(size_t)i * Wp] = o[i];
+          if constexpr (TRACE) {
+            float2* xt = P.Xtr + (size_t)b * M * plane + c0 + cc + (size_t)m * plane +
+                         (size_t)r0 * Wp;
+#pragma unroll
+            for (int i = 0; i < L; ++i) xt[(size_t)i * Wp] = o[i];
+          }
+        }
+        if constexpr (ADJ) {
+          // gE_m(t) partial sums over this thread's rows: the window w is
+          // -cb', W4 the forward's sc / rho (times rho: sc'), x the forward's
+          // row spectra of X at this step
+          const float2* xs = P.Xh + (size_t)b * M * plane + c0 + cc + (size_t)m * plane +
+                             (size_t)r0 * Wp;
+          float2 xv[L];
+#pragma unroll
+          for (int i = 0; i < L; ++i) xv[i] = colok ? xs[(size_t)i * Wp] : make_float2(0.f, 0.f);
+          const int lane = tid & 31, wid = tid >> 5;
+          float2* rp = red + (size_t)(it & 1) * (NT / 32) * KMAX * T;
+#pragma unroll
+          for (int tp = 0; tp < KMAX; ++tp) {
+            float2 a = make_float2(0.f, 0.f);
+            if (tp < Kr) {
+#pragma unroll
+              for (int i = 0; i < L; ++i) {
+                const float2 c = w[i + tp];                        // -cb'(s + t)
+                const float2 sv = W4[rslot(i + tp) * T + cc];      // sc'(s + t) / rho
+                // a += rho sv conj(q) + c conj(x)
+                a.x = fmaf(rho * sv.x, o[i].x, a.x);
+                a.x = fmaf(rho * sv.y, o[i].y, a.x);
+                a.y = fmaf(rho * sv.y, o[i].x, a.y);
+                a.y = fmaf(-rho * sv.x, o[i].y, a.y);
+                a.x = fmaf(c.x, xv[i].x, a.x);
+                a.x = fmaf(c.y, xv[i].y, a.x);
+                a.y = fmaf(c.y, xv[i].x, a.y);
+                a.y = fmaf(-c.x, xv[i].y, a.y);
+              }
+            }
+            // sum over the lanes of this column in the warp (same tid % T)
+#pragma unroll
+            for (int off = T; off < 32; off <<= 1) {
+              a.x += __shfl_xor_sync(0xffffffffu, a.x, off);
+              a.y += __shfl_xor_sync(0xffffffffu, a.y, off);
+            }
+            if (lane < T) rp[((size_t)wid * KMAX + tp) * T + lane] = a;
+          }
         }
         __syncthreads();  // before the buffer is refilled
+        if constexpr (ADJ) {
+          // gE += the column sums, warps in a fixed order (one thread per
+          // filter row and column)
+          const float2* rp = red + (size_t)(it & 1) * (NT / 32) * KMAX * T;
+          for (int e = tid; e < Kr * T; e += NT) {
+            const int tp = e / T, c = e - tp * T;
+            if (c0 + c < Wf) {
+              float2 sum = make_float2(0.f, 0.f);
+              for (int wv = 0; wv < NT / 32; ++wv) {
+                const float2 v = rp[((size_t)wv * KMAX + tp) * T + c];
+                sum.x += v.x;
+                sum.y += v.y;
+              }
+              float2* ge = P.gE + (((size_t)b * M + m) * Kr + tp) * Wp + c0 + c;
+              const float2 o2 = *ge;
+              *ge = make_float2(o2.x + sum.x, o2.y + sum.y);
+            }
+          }
+        }
       }
       cp_async_commit();
       cp_async_wait<0>();

@@ -559,6 +559,7 @@ struct Solve {
   // result(); with a warm start Y and U are kept apart (ROW_ITER_YU).
   bool vstate = true;
   int col_mode = COL_SOLVE_P;  // the column solve of the iteration
+  int force_G = 0;             // > 0: the column pass's cluster size (the unrolled solve)
   bool tune = true;            // run the column-pass autotuner at set-up
   unsigned gen0 = 0;           // cancellation generation at set-up
   bool cancelled = false;
@@ -682,6 +683,12 @@ struct Solve {
     // solve early; the host then never waits on the device mid-solve.
     can_stop = o->rel_tol > 0.f || o->abs_tol > 0.f;
     finished = o->max_iter <= 0;
+    if (o->warm_start) {
+      // The last iteration of the earlier solve may have changed rho; its
+      // fix-up of the row spectra (Y - U / rsf) did not run because that
+      // solve had finished.  Run it now (a no-op when rho did not change).
+      if ((st = launch_row<ROW_FIXUP>(pl, rp, g.B, s))) return st;
+    }
     if (tune && !o->warm_start && autotune_enabled() && o->max_iter > 0) {
       if ((st = tune_col())) return st;
     }
@@ -711,6 +718,7 @@ struct Solve {
   // The column pass of the iteration at cluster size G (0: tuned or model).
   int launch_iter_col(int G) {
     const int B = pl.g.B;
+    if (G <= 0) G = force_G;
     switch (col_mode) {
       case COL_SOLVE_W: return launch_col<COL_SOLVE_W>(pl, cp, B, s, G);
       case COL_SOLVE: return launch_col<COL_SOLVE>(pl, cp, B, s, G);
@@ -1053,8 +1061,21 @@ struct Unrolled {
   int K = 0, seg = 0, nseg = 0;
   size_t R = 0, C = 0;  // floats of a real array, complex entries of a spectrum array
   size_t ckY = 0, ckU = 0, Ytr = 0, Xtr = 0, gV = 0, Fb = 0, gDh = 0, gSh = 0, gDr = 0;
+  // convolution form (filters of at most 16 rows, compiled column lengths
+  // below 512): the forward and the recomputation use the production
+  // convolution solve, the reverse pass its convolution-form adjoint
+  bool conv = false;
+  int conv_mode = 0, trace_mode = 0, adj_mode = 0;
+  size_t SCtr = 0, gE = 0;
   size_t total = 0;
 };
+
+// SPORCO_B200_ADJOINT=transform keeps the transform-solve adjoint for every
+// problem (the form used before the convolution form; for comparisons).
+static bool adjoint_transform_forced() {
+  const char* e = getenv("SPORCO_B200_ADJOINT");
+  return e && strcmp(e, "transform") == 0;
+}
 
 static int unrolled_plan(const sc_problem* p, const sc_options* o, int seg, Unrolled* u) {
   if (!p || !o) return set_status(SC_ERR_INVALID, "null problem or options");
@@ -1091,8 +1112,29 @@ static int unrolled_plan(const sc_problem* p, const sc_options* o, int seg, Unro
   u->gDh = take(sizeof(float2) * u->C);
   u->gSh = take(sizeof(float2) * (size_t)g.B * g.H * g.Wp);
   u->gDr = take(sizeof(float) * (size_t)g.M * g.H * g.W);
+  u->conv = !adjoint_transform_forced() && spec_col(g.H) && col_radix(g.H) == 8 &&
+            p->Kr <= 16;
+  if (u->conv) {
+    const bool c8 = p->Kr <= 8;
+    u->conv_mode = c8 ? COL_SOLVE_C8 : COL_SOLVE_C16;
+    u->trace_mode = c8 ? COL_SOLVE_C8T : COL_SOLVE_C16T;
+    u->adj_mode = c8 ? COL_ADJ_C8 : COL_ADJ_C16;
+    u->SCtr = take(sizeof(float2) * (size_t)g.B * g.H * g.Wp * seg);
+    u->gE = take(sizeof(float2) * (size_t)g.B * g.M * p->Kr * g.Wp);
+  }
   u->total = off;
   return SC_OK;
+}
+
+// Cluster size of the unrolled forward and of its recomputation, which must
+// sum the maps in the same order (the occupancy model of the trace kernel).
+static int unrolled_cluster(const Unrolled& u, int* G) {
+  const void* fn = u.trace_mode == COL_SOLVE_C8T ? (const void*)col_fn<COL_SOLVE_C8T>(u.pl.g.H)
+                                                 : (const void*)col_fn<COL_SOLVE_C16T>(u.pl.g.H);
+  int st = prepare_fn(fn, true);
+  if (st) return st;
+  return cluster_size(fn, u.pl.col_NT, col_smem_bytes(u.trace_mode, u.pl.col_hlen), u.pl.g.M,
+                      (long)u.pl.col_ntiles * u.pl.g.B, G);
 }
 
 extern "C" size_t sc_unrolled_workspace_size(const sc_problem* p, const sc_options* o, int seg) {
@@ -1125,8 +1167,15 @@ extern "C" int sc_unrolled_forward(const sc_problem* p, const sc_options* o, int
   sv.tune = false;  // forward and recomputation must use the same cluster sizes
   if ((st = sv.setup(&u.p, &u.o, ws, u.pl.total, s))) return st;
   // the same column solve as the recomputation in the reverse pass, so that
-  // both produce the same iterates
-  sv.col_mode = COL_SOLVE;
+  // both produce the same iterates: the production convolution solve (the
+  // recomputation runs its trace-keeping twin) at a fixed cluster size, or
+  // the transform solve
+  if (u.conv) {
+    sv.col_mode = u.conv_mode;
+    if ((st = unrolled_cluster(u, &sv.force_G))) return st;
+  } else {
+    sv.col_mode = COL_SOLVE;
+  }
   for (int j = 0; j < u.nseg; ++j) {
     // (Y, U) of the state at the segment's start
     if ((st = sv.state_yu((float*)(w + u.ckY + sizeof(float) * u.R * j),
@@ -1187,23 +1236,32 @@ extern "C" int sc_unrolled_backward(const sc_problem* p, const sc_options* o, in
   float2* gDh = (float2*)(w + u.gDh);
   float2* gSh = (float2*)(w + u.gSh);
   float* gDr = (float*)(w + u.gDr);
+  float2* SCtr = u.conv ? (float2*)(w + u.SCtr) : nullptr;
+  float2* gE = u.conv ? (float2*)(w + u.gE) : nullptr;
   const Geom& g = u.pl.g;
   const Plan& pl = u.pl;
   const int B = g.B;
+  const int Kr = u.p.Kr;
+  const size_t Cs = (size_t)B * g.H * g.Wp;  // complex entries of one SC trace
+  int G = 0;
+  if (u.conv && (st = unrolled_cluster(u, &G))) return st;
   // set-up writes zeros to the problem's Y: give it a trace slot instead of
   // the caller's result
   u.p.Y = Ytr;
   Solve sv;
   sv.tune = false;
   if ((st = sv.setup(&u.p, &u.o, ws, pl.total, s))) return st;
-  CU_TRY(cudaMemsetAsync(gDh, 0, sizeof(float2) * u.C, s));
-  CU_TRY(cudaMemsetAsync(gSh, 0, sizeof(float2) * (size_t)B * g.H * g.Wp, s));
+  if (u.conv)
+    CU_TRY(cudaMemsetAsync(gE, 0, sizeof(float2) * (size_t)B * g.M * Kr * g.Wp, s));
+  else
+    CU_TRY(cudaMemsetAsync(gDh, 0, sizeof(float2) * u.C, s));
+  CU_TRY(cudaMemsetAsync(gSh, 0, sizeof(float2) * Cs, s));
   CU_TRY(cudaMemcpyAsync(gV, gY, sizeof(float) * u.R, cudaMemcpyDeviceToDevice, s));
 
   RowParams ra = sv.rp;
   ra.F = Fb; ra.gV = gV; ra.first = 1;
   ColParams ca = sv.cp;
-  ca.F = Fb; ca.gDh = gDh; ca.gSh = gSh; ca.Xtr = nullptr;
+  ca.F = Fb; ca.gDh = gDh; ca.gSh = gSh; ca.Xtr = nullptr; ca.gE = gE;
   for (int j = u.nseg - 1; j >= 0; --j) {
     const int n = std::min(u.seg, u.K - j * u.seg);
     // Y of step i of this segment: i = 0 is the checkpoint
@@ -1218,7 +1276,14 @@ extern "C" int sc_unrolled_backward(const sc_problem* p, const sc_options* o, in
     for (int i = 0; i < n; ++i) {
       ColParams cf = sv.cp;
       cf.Xtr = Xtr + u.C * i;
-      if ((st = launch_col<COL_SOLVE_X>(pl, cf, B, s))) return st;
+      if (u.conv) {
+        cf.SCtr = SCtr + Cs * i;
+        st = u.trace_mode == COL_SOLVE_C8T ? launch_col<COL_SOLVE_C8T>(pl, cf, B, s, G)
+                                           : launch_col<COL_SOLVE_C16T>(pl, cf, B, s, G);
+      } else {
+        st = launch_col<COL_SOLVE_X>(pl, cf, B, s);
+      }
+      if (st) return st;
       RowParams rr = sv.rp;
       rr.Y = Yat(i);
       rr.Yo = Yat(i + 1);
@@ -1230,7 +1295,14 @@ extern "C" int sc_unrolled_backward(const sc_problem* p, const sc_options* o, in
     ra.first = 0;
     for (int i = n - 1; i >= 0; --i) {
       ca.Xh = Xtr + u.C * i;
-      if ((st = launch_col<COL_ADJ>(pl, ca, B, s))) return st;
+      if (u.conv) {
+        ca.SCtr = SCtr + Cs * i;
+        st = u.adj_mode == COL_ADJ_C8 ? launch_col<COL_ADJ_C8>(pl, ca, B, s)
+                                      : launch_col<COL_ADJ_C16>(pl, ca, B, s);
+      } else {
+        st = launch_col<COL_ADJ>(pl, ca, B, s);
+      }
+      if (st) return st;
       if (i > 0) {
         ra.Ymask = Yat(i);
         if ((st = launch_row<ROW_ADJ>(pl, ra, B, s))) return st;
@@ -1238,20 +1310,37 @@ extern "C" int sc_unrolled_backward(const sc_problem* p, const sc_options* o, in
     }
   }
   // dictionary gradient: sum over the images, inverse FFT, crop to the filters
-  const size_t per = (size_t)g.M * g.H * g.Wp;
-  sum_images_kernel<<<(unsigned)std::min<size_t>((per + 255) / 256, 4096), 256, 0, s>>>(gDh, B,
-                                                                                       per);
-  CU_TRY(cudaGetLastError());
-  ++g_launches;
-  {
+  if (u.conv) {
+    // gE holds, per filter row t, H^2 IFFTcol(gD^)(t) in the row-spectral
+    // domain: the inverse row transform with 1 / (H^2 W) gives the spatial
+    // gradient at the filter rows
+    const size_t per = (size_t)g.M * Kr * g.Wp;
+    sum_images_kernel<<<(unsigned)std::min<size_t>((per + 255) / 256, 4096), 256, 0, s>>>(gE, B,
+                                                                                         per);
+    CU_TRY(cudaGetLastError());
+    ++g_launches;
+    RowParams ri = sv.rp;
+    ri.g.B = 1; ri.g.H = Kr; ri.F = gE; ri.dst = gDr;
+    ri.invN = (float)(1.0 / ((double)g.H * g.H * g.W));
+    if ((st = launch_row<ROW_INV_REAL>(pl, ri, 1, s))) return st;
+    const int nk = g.M * Kr * u.p.Kc;
+    crop_kernel<<<(nk + 255) / 256, 256, 0, s>>>(gDr, gD, g.M, Kr, g.W, Kr, u.p.Kc);
+    CU_TRY(cudaGetLastError());
+    ++g_launches;
+  } else {
+    const size_t per = (size_t)g.M * g.H * g.Wp;
+    sum_images_kernel<<<(unsigned)std::min<size_t>((per + 255) / 256, 4096), 256, 0, s>>>(gDh, B,
+                                                                                         per);
+    CU_TRY(cudaGetLastError());
+    ++g_launches;
     ColParams ci = sv.cp;
     ci.g.B = 1; ci.F = gDh;
     if ((st = launch_col<COL_INV>(pl, ci, 1, s))) return st;
     RowParams ri = sv.rp;
     ri.g.B = 1; ri.F = gDh; ri.dst = gDr;
     if ((st = launch_row<ROW_INV_REAL>(pl, ri, 1, s))) return st;
-    const int n = g.M * u.p.Kr * u.p.Kc;
-    crop_kernel<<<(n + 255) / 256, 256, 0, s>>>(gDr, gD, g.M, g.H, g.W, u.p.Kr, u.p.Kc);
+    const int nk = g.M * u.p.Kr * u.p.Kc;
+    crop_kernel<<<(nk + 255) / 256, 256, 0, s>>>(gDr, gD, g.M, g.H, g.W, u.p.Kr, u.p.Kc);
     CU_TRY(cudaGetLastError());
     ++g_launches;
   }

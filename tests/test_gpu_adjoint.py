@@ -70,17 +70,28 @@ def test_unrolled_forward_matches_oracle():
         assert rel < 1e-4
 
 
-# (B, H, W, M, K, iterations): generic-plan sizes with three segments; a row
-# length that is not a multiple of 4 and a short last segment; compile-time
-# plan sizes (64 x 64) with one segment per iteration count square.
-SHAPES = [(2, 24, 20, 3, 5, 12), (1, 32, 30, 4, 5, 10), (2, 64, 64, 8, 7, 9)]
+# (B, H, W, M, K, iterations): generic-plan sizes with three segments (the
+# transform-solve adjoint); a row length that is not a multiple of 4 and a
+# short last segment (8-tap convolution adjoint); compile-time plan sizes
+# (64 x 64, 8 taps) with one segment per iteration count square; 11 x 11
+# filters at 128 x 128 (16 taps) over 200 iterations (15 segments of 14).
+SHAPES = [(2, 24, 20, 3, 5, 12), (1, 32, 30, 4, 5, 10), (2, 64, 64, 8, 7, 9),
+          (1, 128, 128, 8, 11, 200)]
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("form", ["default", "transform"])
 @pytest.mark.parametrize("shape", SHAPES)
-def test_unrolled_gradients_match_fp64_autograd_and_fd(shape):
+def test_unrolled_gradients_match_fp64_autograd_and_fd(shape, form, monkeypatch):
+    """Against torch FP64 autograd and FP64 central differences; "transform"
+    forces the transform-solve adjoint (SPORCO_B200_ADJOINT) where the
+    convolution form would run."""
     import sporco_cuda.adjoint as adj
     B, H, W, M, K, iters = shape
+    if form == "transform":
+        if shape[0:2] == (2, 24):
+            pytest.skip("the transform form is the default here")
+        monkeypatch.setenv("SPORCO_B200_ADJOINT", "transform")
     D, S, Sc = _problem(B, H, W, M, K)
     lam, rho, alpha = _consts()
     opt = dict(_opt(), MaxMainIter=iters)

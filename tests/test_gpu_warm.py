@@ -48,16 +48,20 @@ def _prepare(D, S, mask=None, **kw):
 @pytest.mark.parametrize("masked", [False, True])
 @pytest.mark.parametrize("warm", [True, "same"])
 def test_warm_continuation_equals_one_solve_bitwise(shape, masked, warm):
+    """Split after iteration 11 (no adaptive-rho step) and after iteration 12
+    (a rho change whose fix-up of the row spectra the continuation runs)."""
     D, S, Wm = _problem(*shape, 31)
     mask = Wm if masked else None
-    ds = _prepare(D, S * (Wm if masked else 1), mask)
-    ds.run(iters=11)
-    Y = ds.run(warm=warm, iters=19).clone()
-    assert ds.state()["iterations"][0] == 19
     ref = _prepare(D, S * (Wm if masked else 1), mask)
-    Yr = ref.run(iters=30)
-    assert torch.equal(Y, Yr)
-    assert ds.state()["rho"] == ref.state()["rho"]
+    Yr = ref.run(iters=30).clone()
+    rhos = ref.state()["rho"]
+    for first in (11, 12):
+        ds = _prepare(D, S * (Wm if masked else 1), mask)
+        ds.run(iters=first)
+        Y = ds.run(warm=warm, iters=30 - first)
+        assert ds.state()["iterations"][0] == 30 - first
+        assert torch.equal(Y, Yr), first
+        assert ds.state()["rho"] == rhos
 
 
 @pytest.mark.gpu
@@ -97,6 +101,10 @@ def test_convbpdn_object_torch_inputs_and_statistics():
     st2 = b.getitstat()
     assert torch.is_tensor(X2) and X2.shape == (64, 48, 5)
     assert len(st1["rho"]) == 8 and len(st2["rho"]) == 8
-    ref = cb.cbpdn(D, S, 0.05, dict(opt, MaxMainIter=16, Verbose=False))
-    assert np.array_equal(X2.cpu().numpy(), ref)
+    ref = cb.ConvBPDN(torch.tensor(D, device="cuda"), torch.tensor(S, device="cuda"), 0.05,
+                      dict(opt, MaxMainIter=16)).solve()
+    assert torch.equal(X2, ref)
     assert not torch.equal(X1, X2)
+    # and through the reference-facing C ABI, to float32 rounding
+    Xn = cb.cbpdn(D, S, 0.05, dict(opt, MaxMainIter=16, Verbose=False))
+    assert _rel(Xn, ref.cpu().numpy().astype(np.float64)) < 1e-6

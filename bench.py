@@ -766,7 +766,10 @@ def adjoint_cpu_leg(cfg, Dk, S1, Sc1, iters=10):
     """Config 3 on the host: torch FP64 autograd of the plain unrolled solve
     (the adjoint oracle) for one image and `iters` iterations, timed
     (forward + backward), and the GPU adjoint's gradients on the same sample
-    against it."""
+    against it: against the FP64 loss along the GPU forward's own shrinkage
+    pattern (a float32 and a float64 forward can put a near-threshold
+    element on different sides of its kink), and against the plain FP64
+    gradient, with the number of elements whose pattern differs."""
     import torch
     import sporco_cuda.adjoint as adj
     from oracle import adjoint_oracle as A
@@ -775,10 +778,13 @@ def adjoint_cpu_leg(cfg, Dk, S1, Sc1, iters=10):
     lam = float(np.float32(cfg["lmbda"]))
     rho = float(np.float32(50 * lam + 1))
     alpha = float(np.float32(1.8))
+    Sc64 = Sc1.detach().double().cpu()[None]
     Dd = Dk.detach().double().cpu().requires_grad_(True)
     Sd = S1.detach().double().cpu()[None].requires_grad_(True)
+    trace = []
     t0 = time.perf_counter()
-    L = A.loss(Dd, Sd, Sc1.detach().double().cpu()[None], lam, rho, alpha, iters, 0.01)
+    Y64 = A.unrolled(Dd, Sd, lam, rho, alpha, iters, trace=trace)
+    L = torch.sum((A.reconstruct(Dd, Y64) - Sc64) ** 2) + 0.01 * torch.sum(torch.abs(Y64))
     L.backward()
     dt = time.perf_counter() - t0
     cpu = {"value": iters / dt, "unit": "image-iter/s (forward+backward)", "cores": threads,
@@ -794,12 +800,24 @@ def adjoint_cpu_leg(cfg, Dk, S1, Sc1, iters=10):
     R = adj.reconstruct(Dg, X)
     Lg = torch.sum((R - Sc1[None]) ** 2) + 0.01 * torch.sum(torch.abs(X))
     Lg.backward()
+    masks = []
+    for k in range(1, iters + 1):
+        Xk = adj.cbpdn_unrolled(Dk.detach(), S1.detach()[None], cfg["lmbda"],
+                                dict(opt, MaxMainIter=k))
+        masks.append((Xk != 0).permute(0, 3, 1, 2).cpu())
+    flips = int(sum(int(torch.sum((y != 0) != m)) for y, m in zip(trace, masks)))
+    Dm = Dk.detach().double().cpu().requires_grad_(True)
+    Sm = S1.detach().double().cpu()[None].requires_grad_(True)
+    A.loss(Dm, Sm, Sc64, lam, rho, alpha, iters, 0.01, masks=masks).backward()
+
+    def r(a, b):
+        return float(torch.linalg.norm(a.double().cpu() - b) / torch.linalg.norm(b))
     rel = {"iterations": iters, "images": 1,
-           "gD": float(torch.linalg.norm(Dg.grad.double().cpu() - Dd.grad) /
-                       torch.linalg.norm(Dd.grad)),
-           "gS": float(torch.linalg.norm(Sg.grad.double().cpu() - Sd.grad) /
-                       torch.linalg.norm(Sd.grad)),
-           "reference": "FP64 torch autograd of the unrolled restatement"}
+           "gD": r(Dg.grad, Dm.grad), "gS": r(Sg.grad, Sm.grad),
+           "reference": "FP64 torch autograd of the unrolled restatement along the GPU "
+                        "forward's shrinkage pattern",
+           "gD_plain": r(Dg.grad, Dd.grad), "gS_plain": r(Sg.grad, Sd.grad),
+           "pattern_differences": flips}
     return cpu, rel
 
 

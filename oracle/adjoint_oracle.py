@@ -15,8 +15,16 @@ import numpy as np
 import torch
 
 
-def unrolled(D, S, lmbda, rho, alpha, K, wl1=1.0):
-    """D (Kr, Kc, M), S (B, H, W) float64 tensors -> Y_K (B, M, H, W)."""
+def unrolled(D, S, lmbda, rho, alpha, K, wl1=1.0, masks=None, trace=None):
+    """D (Kr, Kc, M), S (B, H, W) float64 tensors -> Y_K (B, M, H, W).
+
+    masks: optional K boolean tensors (B, M, H, W), the shrinkage pattern
+    (Y_k != 0) of another computation of the same iterations; step k then
+    keeps V - t sign(V) where masks[k] is set and zero elsewhere, so that the
+    loss is the smooth function of D and S that coincides with the unrolled
+    solve on the region where that computation's thresholds fall the same
+    way (its gradient there is what an adjoint of that computation returns).
+    trace: optional list that receives Y_k of every step (detached)."""
     B, H, W = S.shape
     Kr, Kc, M = D.shape
     Dp = torch.zeros((M, H, W), dtype=torch.float64)
@@ -29,15 +37,20 @@ def unrolled(D, S, lmbda, rho, alpha, K, wl1=1.0):
     U = torch.zeros_like(Y)
     wl1 = torch.as_tensor(np.asarray(wl1, dtype=np.float64))
     t = lmbda * wl1 / rho
-    for _ in range(K):
+    for k in range(K):
         b = torch.conj(Df)[None] * Sf[:, None] + rho * torch.fft.rfft2(Y - U)
         c = torch.sum(Df[None] * b, dim=1) / den[None]
         Xf = (b - torch.conj(Df)[None] * c[:, None]) / rho
         X = torch.fft.irfft2(Xf, s=(H, W))
         V = alpha * X + (1.0 - alpha) * Y + U
-        Yn = torch.sign(V) * torch.relu(torch.abs(V) - t)
+        if masks is None:
+            Yn = torch.sign(V) * torch.relu(torch.abs(V) - t)
+        else:
+            Yn = torch.where(masks[k], V - t * torch.sign(V), torch.zeros_like(V))
         U = V - Yn
         Y = Yn
+        if trace is not None:
+            trace.append(Y.detach())
     return Y
 
 
@@ -52,8 +65,9 @@ def reconstruct(D, Y):
                             s=(H, W))
 
 
-def loss(D, S, Sc, lmbda, rho, alpha, K, beta):
-    """||D * Y_K - S_clean||^2 + beta ||Y_K||_1 of the unrolled solve."""
-    Y = unrolled(D, S, lmbda, rho, alpha, K)
+def loss(D, S, Sc, lmbda, rho, alpha, K, beta, masks=None):
+    """||D * Y_K - S_clean||^2 + beta ||Y_K||_1 of the unrolled solve (masks:
+    see :func:`unrolled`)."""
+    Y = unrolled(D, S, lmbda, rho, alpha, K, masks=masks)
     R = reconstruct(D, Y)
     return torch.sum((R - Sc) ** 2) + beta * torch.sum(torch.abs(Y))

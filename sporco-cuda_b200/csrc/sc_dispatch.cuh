@@ -43,6 +43,18 @@ ColFn sc_col_fn_solve(int mode, int n);
 // COL_ADJ_C16
 ColFn sc_col_fn_aux(int mode, int n);
 
+// Radix-8 column plans at lengths 512, 768, 1024 (nullptr elsewhere):
+// sc_inst_col_conv.cu (C8, C16, G16), sc_inst_col_solve.cu (P, SOLVE,
+// SOLVE_W).
+ColFn sc_col_fn_conv_r8(int mode, int n);
+ColFn sc_col_fn_solve_r8(int mode, int n);
+// The column-pass modes with a radix-8 alternative.
+__host__ __device__ constexpr bool col_has_r8(int mode) {
+  return mode == COL_SOLVE_C8 || mode == COL_SOLVE_C16 || mode == COL_SOLVE_G16 ||
+         mode == COL_SOLVE_P || mode == COL_SOLVE || mode == COL_SOLVE_W;
+}
+__host__ __device__ constexpr bool col_len_r8(int n) { return n == 512 || n == 768 || n == 1024; }
+
 // The table entry of MODE for length n.
 template <int MODE>
 inline RowFn row_fn(int n) {
@@ -57,4 +69,15 @@ inline ColFn col_fn(int n) {
     return sc_col_fn_solve(MODE, n);
   else
     return sc_col_fn_aux(MODE, n);
+}
+
+// The radix-8 alternative of MODE at length n (nullptr when there is none).
+template <int MODE>
+inline ColFn col_fn_r8(int n) {
+  if constexpr (MODE == COL_SOLVE_C8 || MODE == COL_SOLVE_C16 || MODE == COL_SOLVE_G16)
+    return sc_col_fn_conv_r8(MODE, n);
+  else if constexpr (MODE == COL_SOLVE_P || MODE == COL_SOLVE || MODE == COL_SOLVE_W)
+    return sc_col_fn_solve_r8(MODE, n);
+  else
+    return nullptr;
 }

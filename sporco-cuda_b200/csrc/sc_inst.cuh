@@ -33,3 +33,15 @@ ColFn col_table_small(int n) {
 #undef SC_COL_CASE
   return nullptr;
 }
+
+// Radix-8 column plans at the compiled lengths 512, 768 and 1024 (whose
+// default plans are radix 16): twice the threads per column, half the rows
+// per thread; the autotuner chooses between the two.  nullptr otherwise.
+#define SC_SPEC_COL_R8(X) X(512) X(768) X(1024)
+template <int MODE>
+ColFn col_table_r8(int n) {
+#define SC_COL_CASE(k) case k: return col_kernel<MODE, k, 8>;
+  switch (n) { SC_SPEC_COL_R8(SC_COL_CASE) default: break; }
+#undef SC_COL_CASE
+  return nullptr;
+}

@@ -735,13 +735,15 @@ row_kernel(RowParams P) {
 // keep their HBM layout in shared memory: element (kr, c) of the tile at
 // [slot(kr) * T + c]; thread tid works on column c = tid % T and, in the
 // element loops, on rows kr = tid / T + i g.
-template <int MODE, int NH>
+// RADIX: the radix of the column transform plan (0: col_radix(NH)); it sets
+// the threads per column (NH / RADIX) and the rows per thread.
+template <int MODE, int NH, int RADIX = 0>
 __global__ void __launch_bounds__(SC_COL_MAX_THREADS)
 col_kernel(ColParams P) {
   pdl_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int T = SC_COL_TILE;
-  constexpr int RM = col_radix(NH);
+  constexpr int RM = RADIX > 0 ? RADIX : col_radix(NH);
   // elements of the tile per thread (compile-time bound)
   constexpr int EPT = NH > 0 ? (NH + ct_threads(NH, RM) - 1) / ct_threads(NH, RM) : SC_MAXE;
   const Geom& G = P.g;

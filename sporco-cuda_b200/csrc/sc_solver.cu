@@ -392,9 +392,10 @@ static int cluster_size(const void* fn, int NT, size_t smem, int M, long units, 
 // the same cluster size (the map reduction's summation order depends on it).
 struct TunedG {
   int dev;
-  const void* fn;
+  const void* fn;  // the kernel of the default radix (the key)
   int H, W, M;
   int G;
+  int rm;          // column-transform radix (8, or the default col_radix(H))
 };
 static std::vector<TunedG> g_tuned;
 
@@ -419,42 +420,71 @@ static int forced_cluster(int M) {
   return G >= 1 && G <= 16 ? std::min(G, M) : 0;
 }
 
-static bool tuned_size(const void* fn, const Geom& g, int* G) {
+static bool tuned_size(const void* fn, const Geom& g, int* G, int* rm = nullptr) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return false;
   std::lock_guard<std::mutex> lock(g_cache_mu);
   for (const TunedG& e : g_tuned)
     if (e.dev == dev && e.fn == fn && e.H == g.H && e.W == g.W && e.M == g.M) {
       *G = e.G;
+      if (rm) *rm = e.rm;
       return true;
     }
   return false;
 }
 
-// force_G > 0: launch with that cluster size (the autotuner's trials).
+// Threads per column, threads per CTA and shared-memory slots per column of
+// the compiled column transform of length H with radix rm.
+struct ColShape {
+  int g, NT, hlen;
+};
+static ColShape col_shape(int H, int rm) {
+  const int g = ct_threads(H, rm);
+  return {g, SC_COL_TILE * g, ct_len(H, rm, SC_COL_TILE)};
+}
+
+// force_G > 0: launch with that cluster size, force_rm > 0 with that column
+// radix (the autotuner's trials); otherwise the tuned choice for the shape,
+// else the occupancy model's cluster size at the default radix.
 template <int MODE>
-static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s, int force_G = 0) {
+static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s, int force_G = 0,
+                      int force_rm = 0) {
   cp.Hs = pl.Hs;
   if (col_clustered(MODE)) {
-    ColFn fn = col_fn<MODE>(cp.g.H);
+    const ColFn fn0 = col_fn<MODE>(cp.g.H);  // default radix: the tuning key
+    int G = force_G > 0 ? force_G : forced_cluster(cp.g.M);
+    int rm = force_rm;
+    if (G <= 0) {
+      int tG = 0, trm = 0;
+      if (tuned_size((const void*)fn0, cp.g, &tG, &trm)) {
+        G = tG;
+        if (rm <= 0) rm = trm;
+      }
+    }
+    if (rm <= 0) rm = col_radix(cp.g.H);
+    ColFn fn = fn0;
+    ColShape sh{pl.col_g, pl.col_NT, pl.col_hlen};
+    if (rm != col_radix(cp.g.H)) {
+      fn = col_fn_r8<MODE>(cp.g.H);
+      if (!fn) return set_status(SC_ERR_INVALID, "no radix-%d column plan at %d", rm, cp.g.H);
+      sh = col_shape(cp.g.H, rm);
+    }
     int st = prepare_fn((const void*)fn, true);
     if (st) return st;
-    int G = force_G > 0 ? force_G : forced_cluster(cp.g.M);
-    const size_t smem = col_smem_bytes(MODE, pl.col_hlen);
+    const size_t smem = col_smem_bytes(MODE, sh.hlen);
     const long units = (long)pl.col_ntiles * B;
     if (G > 0 && force_G <= 0) {
-      int n = 0;  // the override only where such a cluster fits
-      if ((st = resident_clusters((const void*)fn, pl.col_NT, smem, G, &n))) return st;
+      int n = 0;  // an override or a tuned size only where such a cluster fits
+      if ((st = resident_clusters((const void*)fn, sh.NT, smem, G, &n))) return st;
       if (n < 1) G = 0;
     }
-    if (G <= 0 && !tuned_size((const void*)fn, cp.g, &G) &&
-        (st = cluster_size((const void*)fn, pl.col_NT, smem, cp.g.M, units, &G)))
+    if (G <= 0 && (st = cluster_size((const void*)fn, sh.NT, smem, cp.g.M, units, &G)))
       return st;
-    cp.gsz = pl.col_g;
+    cp.gsz = sh.g;
     cp.G = G;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(G, pl.col_ntiles, B);
-    cfg.blockDim = dim3(pl.col_NT);
+    cfg.blockDim = dim3(sh.NT);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[2];
@@ -715,64 +745,80 @@ struct Solve {
     return SC_OK;
   }
 
-  // The column pass of the iteration at cluster size G (0: tuned or model).
-  int launch_iter_col(int G) {
+  // The column pass of the iteration at cluster size G and column radix rm
+  // (0: the tuned choice, else the model at the default radix).
+  int launch_iter_col(int G, int rm = 0) {
     const int B = pl.g.B;
     if (G <= 0) G = force_G;
     switch (col_mode) {
-      case COL_SOLVE_W: return launch_col<COL_SOLVE_W>(pl, cp, B, s, G);
-      case COL_SOLVE: return launch_col<COL_SOLVE>(pl, cp, B, s, G);
-      case COL_SOLVE_C8: return launch_col<COL_SOLVE_C8>(pl, cp, B, s, G);
-      case COL_SOLVE_C16: return launch_col<COL_SOLVE_C16>(pl, cp, B, s, G);
-      case COL_SOLVE_G16: return launch_col<COL_SOLVE_G16>(pl, cp, B, s, G);
-      default: return launch_col<COL_SOLVE_P>(pl, cp, B, s, G);
+      case COL_SOLVE_W: return launch_col<COL_SOLVE_W>(pl, cp, B, s, G, rm);
+      case COL_SOLVE: return launch_col<COL_SOLVE>(pl, cp, B, s, G, rm);
+      case COL_SOLVE_C8: return launch_col<COL_SOLVE_C8>(pl, cp, B, s, G, rm);
+      case COL_SOLVE_C16: return launch_col<COL_SOLVE_C16>(pl, cp, B, s, G, rm);
+      case COL_SOLVE_G16: return launch_col<COL_SOLVE_G16>(pl, cp, B, s, G, rm);
+      default: return launch_col<COL_SOLVE_P>(pl, cp, B, s, G, rm);
     }
   }
-  const void* iter_col_fn() const {
+  // The iteration's column kernel at the default radix (r8: the radix-8
+  // alternative, nullptr when the length has none).
+  const void* iter_col_fn(bool r8 = false) const {
+    const int H = pl.g.H;
     switch (col_mode) {
-      case COL_SOLVE_W: return (const void*)col_fn<COL_SOLVE_W>(pl.g.H);
-      case COL_SOLVE: return (const void*)col_fn<COL_SOLVE>(pl.g.H);
-      case COL_SOLVE_C8: return (const void*)col_fn<COL_SOLVE_C8>(pl.g.H);
-      case COL_SOLVE_C16: return (const void*)col_fn<COL_SOLVE_C16>(pl.g.H);
-      case COL_SOLVE_G16: return (const void*)col_fn<COL_SOLVE_G16>(pl.g.H);
-      default: return (const void*)col_fn<COL_SOLVE_P>(pl.g.H);
+      case COL_SOLVE_W: return r8 ? (const void*)col_fn_r8<COL_SOLVE_W>(H) : (const void*)col_fn<COL_SOLVE_W>(H);
+      case COL_SOLVE: return r8 ? (const void*)col_fn_r8<COL_SOLVE>(H) : (const void*)col_fn<COL_SOLVE>(H);
+      case COL_SOLVE_C8: return r8 ? (const void*)col_fn_r8<COL_SOLVE_C8>(H) : (const void*)col_fn<COL_SOLVE_C8>(H);
+      case COL_SOLVE_C16: return r8 ? (const void*)col_fn_r8<COL_SOLVE_C16>(H) : (const void*)col_fn<COL_SOLVE_C16>(H);
+      case COL_SOLVE_G16: return r8 ? (const void*)col_fn_r8<COL_SOLVE_G16>(H) : (const void*)col_fn<COL_SOLVE_G16>(H);
+      default: return r8 ? (const void*)col_fn_r8<COL_SOLVE_P>(H) : (const void*)col_fn<COL_SOLVE_P>(H);
     }
   }
 
   // Autotuner of the column pass: the first solve of a shape in a process
-  // times the iteration's column pass at every cluster size the device can
-  // hold (8, 4, 2 CTAs, at most M; two rounds, the faster time of each kept)
-  // on the freshly initialised state, keeps the fastest for later launches
-  // of that shape and initialises the iterates again (the trials overwrite
-  // the spectra).  It waits for the device once, at that first set-up.
+  // times the iteration's column pass for every column plan the length has
+  // (the default radix, and radix 8 where the default is 16: twice the
+  // threads per column, half the rows per thread) at every cluster size the
+  // device can hold with it (8, 4, 2 CTAs, at most M; two rounds, the faster
+  // time of each kept) on the freshly initialised state, keeps the fastest
+  // (radix, cluster size) for later launches of that shape and initialises
+  // the iterates again (the trials overwrite the spectra).  It waits for the
+  // device once, at that first set-up.
   int tune_col() {
     const Geom& g = pl.g;
     const void* fn = iter_col_fn();
     int G0 = 0;
     if (forced_cluster(g.M) > 0 || tuned_size(fn, g, &G0)) return SC_OK;
-    int st = prepare_fn(fn, true);
-    if (st) return st;
-    const size_t smem = col_smem_bytes(col_mode, pl.col_hlen);
-    int cand[3], nc = 0;
-    for (int G = 8; G >= 2; G /= 2) {
-      int n = 0;
-      if (G > g.M) continue;
-      if ((st = resident_clusters(fn, pl.col_NT, smem, G, &n))) return st;
-      if (n >= 1) cand[nc++] = G;
+    int st;
+    struct Cand { int rm, G; float ms; };
+    std::vector<Cand> cand;
+    const int rdef = col_radix(g.H);
+    for (int r8 = 0; r8 < 2; ++r8) {
+      const void* f = iter_col_fn(r8 != 0);
+      if (!f || (r8 && rdef == 8)) continue;
+      const int rm = r8 ? 8 : rdef;
+      const ColShape sh = col_shape(g.H, rm);
+      if ((st = prepare_fn(f, true))) return st;
+      const size_t smem = col_smem_bytes(col_mode, sh.hlen);
+      for (int G = 8; G >= 2; G /= 2) {
+        int n = 0;
+        if (G > g.M) continue;
+        if ((st = resident_clusters(f, sh.NT, smem, G, &n))) return st;
+        if (n >= 1) cand.push_back({rm, G, 1e30f});
+      }
     }
+    const int nc = (int)cand.size();
     if (nc < 2) return SC_OK;  // nothing to choose
     cudaEvent_t e0, e1;
     CU_TRY(cudaEventCreate(&e0));
     CU_TRY(cudaEventCreate(&e1));
-    float best_ms[3] = {1e30f, 1e30f, 1e30f};
+    st = SC_OK;
     for (int round = 0; round < 2 && !st; ++round) {
       for (int i = 0; i < nc && !st; ++i) {
         float ms = 0.f;
         if (cudaEventRecord(e0, s) != cudaSuccess) { st = SC_ERR_CUDA; break; }
-        st = launch_iter_col(cand[i]);
+        st = launch_iter_col(cand[i].G, cand[i].rm);
         if (!st && cudaEventRecord(e1, s) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
             cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
-          best_ms[i] = std::min(best_ms[i], ms);
+          cand[i].ms = std::min(cand[i].ms, ms);
       }
     }
     cudaEventDestroy(e0);
@@ -780,11 +826,12 @@ struct Solve {
     if (st) return st;
     int bi = 0;
     for (int i = 1; i < nc; ++i)
-      if (best_ms[i] < best_ms[bi]) bi = i;
+      if (cand[i].ms < cand[bi].ms) bi = i;
     if (autotune_verbose()) {
       fprintf(stderr, "sporco_b200 autotune: column pass %dx%d M=%d:", g.H, g.W, g.M);
-      for (int i = 0; i < nc; ++i) fprintf(stderr, " G=%d %.3f ms", cand[i], best_ms[i]);
-      fprintf(stderr, " -> G=%d\n", cand[bi]);
+      for (int i = 0; i < nc; ++i)
+        fprintf(stderr, " r%d/G=%d %.3f ms", cand[i].rm, cand[i].G, cand[i].ms);
+      fprintf(stderr, " -> r%d/G=%d\n", cand[bi].rm, cand[bi].G);
     }
     int dev = 0;
     CU_TRY(cudaGetDevice(&dev));
@@ -794,7 +841,7 @@ struct Solve {
       bool known = false;
       for (const TunedG& e : g_tuned)
         known = known || (e.dev == dev && e.fn == fn && e.H == g.H && e.W == g.W && e.M == g.M);
-      if (!known) g_tuned.push_back({dev, fn, g.H, g.W, g.M, cand[bi]});
+      if (!known) g_tuned.push_back({dev, fn, g.H, g.W, g.M, cand[bi].G, cand[bi].rm});
     }
     return init_iterates();
   }
@@ -1127,8 +1174,14 @@ static int unrolled_plan(const sc_problem* p, const sc_options* o, int seg, Unro
 }
 
 // Cluster size of the unrolled forward and of its recomputation, which must
-// sum the maps in the same order (the occupancy model of the trace kernel).
+// sum the maps in the same order: the autotuned size of the production
+// convolution solve for this shape (the forward tunes it), else the
+// occupancy model of the trace kernel.
 static int unrolled_cluster(const Unrolled& u, int* G) {
+  const void* fc = u.conv_mode == COL_SOLVE_C8 ? (const void*)col_fn<COL_SOLVE_C8>(u.pl.g.H)
+                                               : (const void*)col_fn<COL_SOLVE_C16>(u.pl.g.H);
+  int rm = 0;
+  if (tuned_size(fc, u.pl.g, G, &rm) && rm == col_radix(u.pl.g.H)) return SC_OK;
   const void* fn = u.trace_mode == COL_SOLVE_C8T ? (const void*)col_fn<COL_SOLVE_C8T>(u.pl.g.H)
                                                  : (const void*)col_fn<COL_SOLVE_C16T>(u.pl.g.H);
   int st = prepare_fn(fn, true);
@@ -1172,6 +1225,9 @@ extern "C" int sc_unrolled_forward(const sc_problem* p, const sc_options* o, int
   // the transform solve
   if (u.conv) {
     sv.col_mode = u.conv_mode;
+    // the first solve of a shape tunes the cluster size of the production
+    // solve (the recomputation then uses the same size)
+    if (autotune_enabled() && (st = sv.tune_col())) return st;
     if ((st = unrolled_cluster(u, &sv.force_G))) return st;
   } else {
     sv.col_mode = COL_SOLVE;

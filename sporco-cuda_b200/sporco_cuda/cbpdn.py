@@ -40,7 +40,7 @@ from . import _lib
 F32 = np.float32
 
 __all__ = ["cbpdn", "cbpdnmsk", "cbpdngrd", "cbpdngrdmsk", "SolverError",
-           "solve_device", "resolve_options", "ConvBPDN", "cbpdn_batched"]
+           "solve_device", "resolve_options", "ConvBPDN", "cbpdn_batched", "cbpdn_multi"]
 
 SolverError = _lib.SolverError
 
@@ -585,6 +585,60 @@ class ConvBPDN:
     @property
     def rho(self):
         return self._ds.state()["rho"][0]
+
+
+# --------------------------------------------- multi-channel / multi-signal --
+
+def cbpdn_multi(D, S, lmbda, opt, W=None, mu=None, dev=0):
+    """Multi-channel and multi-signal CBPDN with a single-channel dictionary.
+
+    No counterpart in the reference, which solves one 2-D single-channel
+    signal per call (cbpdn.pyx:87); this is sporco's ConvBPDN layout for a
+    signal with C channels and K signals and a dictionary without a channel
+    axis: ``D`` (Kr, Kc, M), ``S`` (H, W, C) or (H, W, C, K); the result is
+    (H, W, C, K, M), every channel of every signal with its own coefficient
+    maps (the problem separates over channels and signals).  All C K images
+    are solved in one batched device solve (one rho, residual and stopping
+    state per image).  ``mu`` (not None) adds the gradient term of
+    ``cbpdngrd``; a mask ``W`` of shape (H, W), (H, W, C) or (H, W, C, K)
+    gives the AMS problem of ``cbpdnmsk`` / ``cbpdngrdmsk``.  numpy in,
+    numpy out; CUDA tensors in, tensors out."""
+    import torch
+    as_torch = _is_torch(D)
+    device = D.device if as_torch else torch.device("cuda", dev)
+    Dt = torch.as_tensor(D, device=device, dtype=torch.float32)
+    St = torch.as_tensor(S, device=device, dtype=torch.float32)
+    if Dt.ndim != 3:
+        raise ValueError("D must be (Kr, Kc, M): a single-channel dictionary")
+    if St.ndim == 3:
+        St = St[..., None]
+    if St.ndim != 4:
+        raise ValueError("S must be (H, W, C) or (H, W, C, K)")
+    H, Wd, C, K = St.shape
+    Sb = St.permute(2, 3, 0, 1).reshape(C * K, H, Wd).contiguous()
+    grd = mu is not None
+    ams = W is not None
+    l1 = _opt_get(opt, "L1Weight")
+    gw = _opt_get(opt, "GradWeight") if grd else 1.0
+    mask = None
+    if ams:
+        Wt = torch.as_tensor(W, device=device)
+        while Wt.ndim < 4:
+            Wt = Wt[..., None]
+        mask = Wt.expand(H, Wd, C, K).permute(2, 3, 0, 1).reshape(C * K, H, Wd).to(torch.int32)
+        d0 = torch.zeros((Dt.shape[0], Dt.shape[1], 1), device=device)
+        d0[0, 0] = 1.0
+        Dt = torch.cat((d0, Dt), dim=2)
+        l1, gw = _ams_weights(None, Dt.shape[2], {"L1Weight": _np(l1), "GradWeight": _np(gw)},
+                              grd)
+    if hasattr(l1, "ndim") and np.ndim(l1) == 3:
+        l1 = np.ascontiguousarray(np.rollaxis(_np(l1), 2, 0))
+    Y = solve_device(Dt.permute(2, 0, 1).contiguous(), Sb, lmbda, opt,
+                     mu=0.0 if mu is None else mu, grd=grd, l1=l1, gw=gw, mask=mask)
+    X = Y.reshape(C, K, Y.shape[1], H, Wd).permute(3, 4, 0, 1, 2)  # (H, W, C, K, M)
+    if ams:
+        X = X[..., 1:]
+    return X if as_torch else X.contiguous().cpu().numpy()
 
 
 # ------------------------------------------------------------- batched form --

@@ -872,6 +872,7 @@ def run_reference(args, cfg, rank, world):
                 gens.append(OT.iterate(prob, res, xi, record=False))
             done = 0
     value = sum(counts) / sum(times)
+    ref_gpu = reference_gpu_leg(args, cfg, D, S, mask)
     sample = ("%s: %d timed steps of one continuing FP64 solve (%d ADMM iterations of %s in "
               "all, set-up in the untimed warm-up; torch CPU, %d threads, maps in chunks of 16)"
               % (cfg["workload"], args.steps, sum(counts), " and ".join(cfg["variants"]),
@@ -887,7 +888,55 @@ def run_reference(args, cfg, rank, world):
                          "sample": sample},
         "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "reference_gpu": ref_gpu,
     }
+
+
+def reference_gpu_leg(args, cfg, D, S, mask):
+    """The reference's own CUDA implementation of the path (its sources,
+    unchanged, built for sm_100a into oracle/_ref by oracle/Makefile) on the
+    same workload, through its own C ABI with host buffers: every call plans
+    its FFTs, allocates, copies in, runs its host-driven iterations and
+    copies out, as a caller of the reference sees it.  Its default
+    HighMemSolve = 0 (its fastest mode; its solve coefficients then go
+    stale after a change of rho).  One untimed call per variant, then timed
+    calls for at most about 30 s."""
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no CUDA device"}
+        from oracle import ref_abi
+    except Exception as e:  # pragma: no cover
+        return {"unavailable": "reference build not importable: %s" % e}
+    if not ref_abi.available():
+        return {"unavailable": "oracle/_ref not built (make -C oracle ref REF=<reference tree>)"}
+    Dk = np.ascontiguousarray(np.moveaxis(D, 0, 2))
+
+    def call(v):
+        opt = dict(opt_for(cfg, v), AuxVarObj=False, HighMemSolve=False, NonNegCoef=False,
+                   NoBndryCross=False)
+        if v == "cbpdn":
+            ref_abi.cbpdn(Dk, S, cfg["lmbda"], opt)
+        elif v == "cbpdngrd":
+            ref_abi.cbpdngrd(Dk, S, cfg["lmbda"], cfg["mu"], opt)
+        else:
+            ref_abi.cbpdnmsk(Dk, S * mask, mask, cfg["lmbda"], opt)
+    for v in cfg["variants"]:
+        call(v)
+    n, t0 = 0, time.perf_counter()
+    while n < max(1, args.steps):
+        for v in cfg["variants"]:
+            call(v)
+        n += 1
+        if time.perf_counter() - t0 > 30.0:
+            break
+    dt = time.perf_counter() - t0
+    iters = n * cfg["iters"] * len(cfg["variants"])
+    return {"value": iters / dt, "unit": "iter/s", "calls": n * len(cfg["variants"]),
+            "ms_per_call": 1e3 * dt / (n * len(cfg["variants"])),
+            "kind": "the reference's CUDA sources built for sm_100a (oracle/_ref), its C ABI "
+                    "with host buffers (set-up, copies and %d iterations per call; "
+                    "HighMemSolve off)" % cfg["iters"]}
 
 
 def main():

@@ -22,11 +22,13 @@ typedef void (*ColFn)(ColParams);
   X(48) X(96) X(192) X(384) X(768) X(1536)
 
 // Row modes with compile-time FFT plans: the iteration, the rho fix-up, the
-// adjoint step and the 2-D FFT tools; the set-up modes (dictionary, warm
-// start) always use the runtime plan.
+// adjoint step, the 2-D FFT tools and the row spectra of Y - U from given
+// iterates (the adjoint's restart from a checkpoint must transform exactly
+// as the iteration does, so that its recomputation reproduces the forward
+// iterates bit for bit); the dictionary set-up uses the runtime plan.
 __host__ __device__ constexpr bool row_specialised(int mode) {
   return mode == ROW_ITER || mode == ROW_ITER_YU || mode == ROW_FIXUP || mode == ROW_FWD_REAL ||
-         mode == ROW_INV_REAL || mode == ROW_ADJ;
+         mode == ROW_INV_REAL || mode == ROW_ADJ || mode == ROW_FWD_YU;
 }
 
 // sc_inst_row_iter.cu: ROW_ITER, ROW_ITER_YU

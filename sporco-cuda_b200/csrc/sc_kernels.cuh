@@ -1131,8 +1131,9 @@ col_kernel(ColParams P) {
           float2* rp = red + (size_t)(it & 1) * (NT / 32) * KMAX * T;
 #pragma unroll
           for (int tp = 0; tp < KMAX; ++tp) {
+            if (tp >= Kr) break;  // uniform over the CTA
             float2 a = make_float2(0.f, 0.f);
-            if (tp < Kr) {
+            {
 #pragma unroll
               for (int i = 0; i < L; ++i) {
                 const float2 c = w[i + tp];                        // -cb'(s + t)

@@ -24,7 +24,8 @@ OPT = {"MaxMainIter": 25, "RelStopTol": 0.0, "AutoRho": {"Enabled": True}}
 def test_channels_and_signals_separate(variant):
     rng = np.random.default_rng(61)
     H, W, C, K, M = 48, 40, 3, 2, 5
-    D = rng.standard_normal((6, 6, M)).astype(np.float32)
+    D = rng.standard_normal((6, 6, M))
+    D = (D / np.sqrt(np.sum(D * D, axis=(0, 1), keepdims=True))).astype(np.float32)
     S = rng.standard_normal((H, W, C, K)).astype(np.float32)
     Wm = (rng.random((H, W, C)) < 0.7).astype(np.float32) if variant == "cbpdnmsk" else None
     mu = 0.2 if variant == "cbpdngrd" else None

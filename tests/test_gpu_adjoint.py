@@ -153,7 +153,11 @@ def test_unrolled_gradients_match_fp64_autograd_and_fd(shape, form, monkeypatch)
             g = g.double().cpu()
             assert float(torch.linalg.norm(g - r) / torch.linalg.norm(r)) < 1e-4
     # directional central differences of the FP64 loss along the GPU's
-    # pattern (smooth around the point), against the GPU gradient
+    # pattern, against the GPU gradient.  That loss is smooth in the solve,
+    # but its L1 term |Y_K| still has a kink wherever an active coefficient
+    # is within the step of zero; a central difference means something only
+    # where both one-sided differences agree, so a step that straddles a kink
+    # is shrunk until it does not.
     rng = np.random.default_rng(7)
     for g, base, which in ((Dg.grad, D, "D"), (Sg.grad, S, "S")):
         dd = torch.tensor(rng.standard_normal(base.shape))
@@ -163,7 +167,12 @@ def test_unrolled_gradients_match_fp64_autograd_and_fd(shape, form, monkeypatch)
             s = torch.tensor(S, dtype=torch.float64) if which == "D" else x
             return float(A.loss(d, s, Sc64, lam, rho, alpha, iters, BETA, masks=masks))
         x0 = torch.tensor(base, dtype=torch.float64)
-        eps = 1e-6
-        fd = (f(x0 + eps * dd) - f(x0 - eps * dd)) / (2 * eps)
+        f0 = f(x0)
+        for eps in (1e-6, 1e-7, 1e-8):
+            fp, fm = f(x0 + eps * dd), f(x0 - eps * dd)
+            fwd, bwd = (fp - f0) / eps, (f0 - fm) / eps
+            if abs(fwd - bwd) <= 1e-3 * max(1.0, abs(fwd)):
+                break
+        fd = (fp - fm) / (2 * eps)
         an = float(np.sum(g.double().cpu().numpy() * dd.numpy()))
-        assert abs(fd - an) <= 1e-4 * max(1.0, abs(fd)), (which, fd, an)
+        assert abs(fd - an) <= 1e-4 * max(1.0, abs(fd)), (which, eps, fd, an)

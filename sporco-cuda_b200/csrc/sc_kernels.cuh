@@ -1104,6 +1104,43 @@ col_kernel(ColParams P) {
           }
         }
         if constexpr (ADJ) {
+          // gE_m(t) partial sums over this thread's rows, taken before o is
+          // scaled to q_m = o / rho: rho sc'(s + t) conj(q_m(s)) =
+          // W4(s + t) conj(o(s)) with W4 = sc' (the SCtr tile); the window w
+          // is -cb', x the forward's row spectra of X at this step
+          const float2* xs = P.Xh + (size_t)b * M * plane + c0 + cc + (size_t)m * plane +
+                             (size_t)r0 * Wp;
+          float2 xv[L];
+#pragma unroll
+          for (int i = 0; i < L; ++i) xv[i] = colok ? xs[(size_t)i * Wp] : make_float2(0.f, 0.f);
+          const int lane = tid & 31, wid = tid >> 5;
+          float2* rp = red + (size_t)(it & 1) * (NT / 32) * KMAX * T;
+#pragma unroll
+          for (int tp = 0; tp < KMAX; ++tp) {
+            if (tp >= Kr) break;  // uniform over the CTA
+            float2 a = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int i = 0; i < L; ++i) {
+              const float2 c = w[i + tp];                    // -cb'(s + t)
+              const float2 sv = W4[rslot(i + tp) * T + cc];  // sc'(s + t)
+              // a += sv conj(o) + c conj(x)
+              a.x = fmaf(sv.x, o[i].x, a.x);
+              a.x = fmaf(sv.y, o[i].y, a.x);
+              a.y = fmaf(sv.y, o[i].x, a.y);
+              a.y = fmaf(-sv.x, o[i].y, a.y);
+              a.x = fmaf(c.x, xv[i].x, a.x);
+              a.x = fmaf(c.y, xv[i].y, a.x);
+              a.y = fmaf(c.y, xv[i].x, a.y);
+              a.y = fmaf(-c.x, xv[i].y, a.y);
+            }
+            // sum over the lanes of this column in the warp (same tid % T)
+#pragma unroll
+            for (int off = T; off < 32; off <<= 1) {
+              a.x += __shfl_xor_sync(0xffffffffu, a.x, off);
+              a.y += __shfl_xor_sync(0xffffffffu, a.y, off);
+            }
+            if (lane < T) rp[((size_t)wid * KMAX + tp) * T + lane] = a;
+          }
 #pragma unroll
           for (int i = 0; i < L; ++i) o[i] = make_float2(o[i].x * irho, o[i].y * irho);  // q_m
         }
@@ -1116,46 +1153,6 @@ col_kernel(ColParams P) {
                          (size_t)r0 * Wp;
 #pragma unroll
             for (int i = 0; i < L; ++i) xt[(size_t)i * Wp] = o[i];
-          }
-        }
-        if constexpr (ADJ) {
-          // gE_m(t) partial sums over this thread's rows: the window w is
-          // -cb', W4 the forward's sc / rho (times rho: sc'), x the forward's
-          // row spectra of X at this step
-          const float2* xs = P.Xh + (size_t)b * M * plane + c0 + cc + (size_t)m * plane +
-                             (size_t)r0 * Wp;
-          float2 xv[L];
-#pragma unroll
-          for (int i = 0; i < L; ++i) xv[i] = colok ? xs[(size_t)i * Wp] : make_float2(0.f, 0.f);
-          const int lane = tid & 31, wid = tid >> 5;
-          float2* rp = red + (size_t)(it & 1) * (NT / 32) * KMAX * T;
-#pragma unroll
-          for (int tp = 0; tp < KMAX; ++tp) {
-            if (tp >= Kr) break;  // uniform over the CTA
-            float2 a = make_float2(0.f, 0.f);
-            {
-#pragma unroll
-              for (int i = 0; i < L; ++i) {
-                const float2 c = w[i + tp];                        // -cb'(s + t)
-                const float2 sv = W4[rslot(i + tp) * T + cc];      // sc'(s + t) / rho
-                // a += rho sv conj(q) + c conj(x)
-                a.x = fmaf(rho * sv.x, o[i].x, a.x);
-                a.x = fmaf(rho * sv.y, o[i].y, a.x);
-                a.y = fmaf(rho * sv.y, o[i].x, a.y);
-                a.y = fmaf(-rho * sv.x, o[i].y, a.y);
-                a.x = fmaf(c.x, xv[i].x, a.x);
-                a.x = fmaf(c.y, xv[i].y, a.x);
-                a.y = fmaf(c.y, xv[i].x, a.y);
-                a.y = fmaf(-c.x, xv[i].y, a.y);
-              }
-            }
-            // sum over the lanes of this column in the warp (same tid % T)
-#pragma unroll
-            for (int off = T; off < 32; off <<= 1) {
-              a.x += __shfl_xor_sync(0xffffffffu, a.x, off);
-              a.y += __shfl_xor_sync(0xffffffffu, a.y, off);
-            }
-            if (lane < T) rp[((size_t)wid * KMAX + tp) * T + lane] = a;
           }
         }
         __syncthreads();  // before the buffer is refilled

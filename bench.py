@@ -147,15 +147,15 @@ def graded_kernel_bytes(H, W, M):
 # in proportion to the maps, with the capture each comes from (kernels as of
 # the commit named there).
 MEASURED_TRAFFIC_PER_MAP = {
-    (2048, 2048): {"row_kernel": ((807e6 + 744e6) / 24,
-                                  "ncu capture at 2048x2048, M=24, scaled by the maps "
-                                  "(captured at commit 2d8664f)"),
-                   "col_kernel": ((827.5e6 + 352.6e6) / 24,
-                                  "ncu capture at 2048x2048, M=24 (clusters of 2), "
-                                  "scaled by the maps (captured at commit 2d8664f)")},
+    (2048, 2048): {"row_kernel": ((807.1e6 + 745.2e6) / 24,
+                                  "ncu capture at 2048x2048, M=24 (kernels of commit a104647), "
+                                  "scaled by the maps"),
+                   "col_kernel": ((826.7e6 + 353.7e6) / 24,
+                                  "ncu capture at 2048x2048, M=24 (kernels of commit a104647), "
+                                  "scaled by the maps")},
     (512, 512): {"col_kernel": (((216.1e6 + 49.3e6) + (218.5e6 + 56.2e6)) / 2 / 100,
                                 "ncu captures at 512x512, M=100, mean of the gradient and "
-                                "masked column solves (captured at commit 2d8664f)")},
+                                "masked column solves (kernels of commit 2d8664f)")},
 }
 
 

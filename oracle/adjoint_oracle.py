@@ -65,9 +65,12 @@ def reconstruct(D, Y):
                             s=(H, W))
 
 
-def loss(D, S, Sc, lmbda, rho, alpha, K, beta, masks=None):
+def loss(D, S, Sc, lmbda, rho, alpha, K, beta, masks=None, l1sign=None):
     """||D * Y_K - S_clean||^2 + beta ||Y_K||_1 of the unrolled solve (masks:
-    see :func:`unrolled`)."""
+    see :func:`unrolled`).  l1sign: optional signs (B, M, H, W) of another
+    computation's Y_K; ||Y_K||_1 is then taken as sum(l1sign Y_K), its value
+    wherever the signs agree, without the kink of |y| at zero."""
     Y = unrolled(D, S, lmbda, rho, alpha, K, masks=masks)
     R = reconstruct(D, Y)
-    return torch.sum((R - Sc) ** 2) + beta * torch.sum(torch.abs(Y))
+    l1 = torch.sum(torch.abs(Y)) if l1sign is None else torch.sum(l1sign * Y)
+    return torch.sum((R - Sc) ** 2) + beta * l1

@@ -109,7 +109,10 @@ def test_unrolled_gradients_match_fp64_autograd_and_fd(shape, form, monkeypatch)
     forward's own shrinkage pattern (identical to the plain FP64 loss
     wherever the patterns agree, smooth in D and S around the point), and
     the plain FP64 gradient is compared as well whenever the FP64 forward
-    produces the same pattern.  "transform" forces the transform-solve
+    produces the same pattern (the L1 term likewise takes the GPU's signs of
+    Y_K, the value of |Y_K| wherever the signs agree, so that an active
+    coefficient next to zero puts no kink inside the difference step).
+    "transform" forces the transform-solve
     adjoint (SPORCO_B200_ADJOINT) where the convolution form would run."""
     import sporco_cuda.adjoint as adj
     B, H, W, M, K, iters = shape
@@ -128,12 +131,13 @@ def test_unrolled_gradients_match_fp64_autograd_and_fd(shape, form, monkeypatch)
     L.backward()
     masks = _gpu_masks(D, S, iters)
     Sc64 = torch.tensor(Sc, dtype=torch.float64)
+    sgn = torch.sign(X.detach()).permute(0, 3, 1, 2).double().cpu()  # the GPU's Y_K signs
 
     def ref_grads(use_masks):
         Dt = torch.tensor(D, dtype=torch.float64, requires_grad=True)
         St = torch.tensor(S, dtype=torch.float64, requires_grad=True)
         Lr = A.loss(Dt, St, Sc64, lam, rho, alpha, iters, BETA,
-                    masks=masks if use_masks else None)
+                    masks=masks if use_masks else None, l1sign=sgn if use_masks else None)
         Lr.backward()
         return float(Lr), Dt.grad, St.grad
 
@@ -153,11 +157,8 @@ def test_unrolled_gradients_match_fp64_autograd_and_fd(shape, form, monkeypatch)
             g = g.double().cpu()
             assert float(torch.linalg.norm(g - r) / torch.linalg.norm(r)) < 1e-4
     # directional central differences of the FP64 loss along the GPU's
-    # pattern, against the GPU gradient.  That loss is smooth in the solve,
-    # but its L1 term |Y_K| still has a kink wherever an active coefficient
-    # is within the step of zero; a central difference means something only
-    # where both one-sided differences agree, so a step that straddles a kink
-    # is shrunk until it does not.
+    # pattern (and the GPU's signs of Y_K in its L1 term: smooth around the
+    # point), against the GPU gradient
     rng = np.random.default_rng(7)
     for g, base, which in ((Dg.grad, D, "D"), (Sg.grad, S, "S")):
         dd = torch.tensor(rng.standard_normal(base.shape))
@@ -165,14 +166,11 @@ def test_unrolled_gradients_match_fp64_autograd_and_fd(shape, form, monkeypatch)
         def f(x):
             d = torch.tensor(D, dtype=torch.float64) if which == "S" else x
             s = torch.tensor(S, dtype=torch.float64) if which == "D" else x
-            return float(A.loss(d, s, Sc64, lam, rho, alpha, iters, BETA, masks=masks))
+            return float(A.loss(d, s, Sc64, lam, rho, alpha, iters, BETA, masks=masks,
+                                l1sign=sgn))
         x0 = torch.tensor(base, dtype=torch.float64)
-        f0 = f(x0)
-        for eps in (1e-6, 1e-7, 1e-8):
-            fp, fm = f(x0 + eps * dd), f(x0 - eps * dd)
-            fwd, bwd = (fp - f0) / eps, (f0 - fm) / eps
-            if abs(fwd - bwd) <= 1e-3 * max(1.0, abs(fwd)):
-                break
+        eps = 1e-6
+        fp, fm = f(x0 + eps * dd), f(x0 - eps * dd)
         fd = (fp - fm) / (2 * eps)
         an = float(np.sum(g.double().cpu().numpy() * dd.numpy()))
         assert abs(fd - an) <= 1e-4 * max(1.0, abs(fd)), (which, eps, fd, an)

@@ -361,16 +361,21 @@ static int resident_clusters(const void* fn, int NT, size_t smem, int G, int* ou
   return SC_OK;
 }
 
+// Cluster sizes the column pass is launched with (the model's and the
+// autotuner's candidates).  Clusters lie within a GPC; with one CTA per SM a
+// size that divides the GPCs' SM counts badly leaves SMs idle, which sizes
+// other than the powers of two can avoid.
+static const int kClusterSizes[] = {8, 6, 4, 3, 2};
+
 // CTAs per cluster of a clustered column launch over `units` column tiles
-// (tiles x images).  Candidates 8, 4, 2 (at most M); the estimated time is
-// (maps per CTA) x (rounds of resident clusters over the units), ties go to
-// the larger cluster.  A cluster of 8 CTAs that each fill an SM leaves the
-// SMs of a GPC beyond a multiple of 8 idle; smaller clusters pack the GPCs
-// more tightly at the price of more maps per CTA.
+// (tiles x images).  Candidates kClusterSizes (at most M); the estimated time
+// is (maps per CTA) x (rounds of resident clusters over the units), ties go
+// to the larger cluster.  Larger clusters split the maps more finely, smaller
+// ones pack the GPCs more tightly.
 static int cluster_size(const void* fn, int NT, size_t smem, int M, long units, int* G_out) {
   int best = std::min(8, M);
   long best_cost = -1;
-  for (int G = 8; G >= 2; G /= 2) {
+  for (int G : kClusterSizes) {
     if (G > M) continue;
     int nc = 0;
     int st = resident_clusters(fn, NT, smem, G, &nc);
@@ -777,7 +782,7 @@ struct Solve {
   // times the iteration's column pass for every column plan the length has
   // (the default radix, and radix 8 where the default is 16: twice the
   // threads per column, half the rows per thread) at every cluster size the
-  // device can hold with it (8, 4, 2 CTAs, at most M; two rounds, the faster
+  // device can hold with it (kClusterSizes, at most M; two rounds, the faster
   // time of each kept) on the freshly initialised state, keeps the fastest
   // (radix, cluster size) for later launches of that shape and initialises
   // the iterates again (the trials overwrite the spectra).  It waits for the
@@ -798,7 +803,7 @@ struct Solve {
       const ColShape sh = col_shape(g.H, rm);
       if ((st = prepare_fn(f, true))) return st;
       const size_t smem = col_smem_bytes(col_mode, sh.hlen);
-      for (int G = 8; G >= 2; G /= 2) {
+      for (int G : kClusterSizes) {
         int n = 0;
         if (G > g.M) continue;
         if ((st = resident_clusters(f, sh.NT, smem, G, &n))) return st;

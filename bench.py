@@ -690,14 +690,14 @@ def run_adjoint(args, cfg, rank, world, local_rank):
     opt = {"MaxMainIter": cfg["iters"], "RelStopTol": 0.0, "RelaxParam": 1.8, "rho": None,
            "AutoRho": {"Enabled": False}}
 
-    def fwd_bwd():
+    def fwd_bwd(checkpoints="sqrt"):
         Dg = Dk.clone().requires_grad_(True)
         Sg = S.clone().requires_grad_(True)
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         t2 = torch.cuda.Event(enable_timing=True)
         t0.record()
-        X = adj.cbpdn_unrolled(Dg, Sg, cfg["lmbda"], opt)
+        X = adj.cbpdn_unrolled(Dg, Sg, cfg["lmbda"], opt, checkpoints=checkpoints)
         R = adj.reconstruct(Dg, X)
         L = torch.sum((R - Sc) ** 2) + 0.01 * torch.sum(torch.abs(X))
         t1.record()
@@ -719,6 +719,17 @@ def run_adjoint(args, cfg, rank, world, local_rank):
     launches = _lib.sc_launch_count() - n0
     ms = f_ms + b_ms
     value = replicas.job_rate(B * cfg["iters"] * args.steps, ms)
+    # every step's trace kept in the forward pass (no recomputation; about
+    # K (R + C) bytes of workspace), for comparison
+    fwd_bwd("all")
+    torch.cuda.synchronize()
+    fa = ba = 0.0
+    for _ in range(args.steps):
+        f, b_ = fwd_bwd("all")
+        fa += f
+        ba += b_
+    fa = replicas.max_over_ranks(fa)
+    ba = replicas.max_over_ranks(ba)
     f_ms = replicas.max_over_ranks(f_ms)
     b_ms = replicas.max_over_ranks(b_ms)
     ms = f_ms + b_ms
@@ -757,6 +768,10 @@ def run_adjoint(args, cfg, rank, world, local_rank):
         "backward_over_forward": b_ms / f_ms,
         "fused_forward_solve_ms": fused_ms,
         "backward_over_fused_forward": (b_ms / args.steps) / fused_ms,
+        "all_traces": {"forward_ms": fa / args.steps, "backward_ms": ba / args.steps,
+                       "backward_over_forward": ba / fa,
+                       "backward_over_fused_forward": (ba / args.steps) / fused_ms,
+                       "checkpoints": "every step's trace kept in the forward pass"},
         "e2e": None, "roofline": roof, "rel_err": rel, "cpu_baseline": cpu,
         "gpu_launches": launches, "clocks": clk.summary(),
     }

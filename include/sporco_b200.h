@@ -247,7 +247,10 @@ unsigned long long sc_launch_count(void);
  * = NULL), and the reverse pass of those iterations.
  *   sc_unrolled_forward writes Y_K to p->Y and keeps (Y, U) every seg
  *     iterations in the workspace (seg: 1..K; ceil(sqrt(K)) balances memory
- *     against the one recomputation of each segment in the backward pass).
+ *     against the one recomputation of each segment in the backward pass;
+ *     seg = K with filters of at most 16 rows and compiled column lengths
+ *     below 512 keeps the trace of every step instead, so that the backward
+ *     recomputes nothing, in a workspace of about K (R + C) bytes).
  *   sc_unrolled_backward, after a forward call with the same problem,
  *     options, seg and workspace, takes gY = dLoss/dY_K (B, M, H, W) and
  *     writes dLoss/dD to gD (M, Kr, Kc) and dLoss/dS to gS (B, H, W).

@@ -1237,6 +1237,34 @@ extern "C" int sc_unrolled_forward(const sc_problem* p, const sc_options* o, int
   } else {
     sv.col_mode = COL_SOLVE;
   }
+  if (u.conv && u.seg == u.K) {
+    // One segment (seg = K): the forward keeps the trace of every step that
+    // the reverse pass needs (Y, the row spectra of X and sc / rho), so the
+    // backward recomputes nothing.  The trace-keeping kernels are the
+    // recomputation's.
+    float* ckY = (float*)(w + u.ckY);
+    float* Ytr = (float*)(w + u.Ytr);
+    float2* Xtr = (float2*)(w + u.Xtr);
+    float2* SCtr = (float2*)(w + u.SCtr);
+    const Geom& g = u.pl.g;
+    const size_t Cs = (size_t)g.B * g.H * g.Wp;
+    if ((st = sv.state_yu(ckY, (float*)(w + u.ckU)))) return st;  // zeros
+    auto Yat = [&](int i) { return i == 0 ? ckY : Ytr + u.R * (i - 1); };
+    for (int i = 0; i < u.K; ++i) {
+      ColParams cf = sv.cp;
+      cf.Xtr = Xtr + u.C * i;
+      cf.SCtr = SCtr + Cs * i;
+      st = u.trace_mode == COL_SOLVE_C8T ? launch_col<COL_SOLVE_C8T>(u.pl, cf, g.B, s, sv.force_G)
+                                         : launch_col<COL_SOLVE_C16T>(u.pl, cf, g.B, s, sv.force_G);
+      if (st) return st;
+      RowParams rr = sv.rp;
+      rr.Y = Yat(i);
+      rr.Yo = Yat(i + 1);
+      if ((st = launch_row<ROW_ITER_YU>(u.pl, rr, g.B, s))) return st;
+    }
+    CU_TRY(cudaMemcpyAsync(p->Y, Yat(u.K), sizeof(float) * u.R, cudaMemcpyDeviceToDevice, s));
+    return SC_OK;
+  }
   for (int j = 0; j < u.nseg; ++j) {
     // (Y, U) of the state at the segment's start
     if ((st = sv.state_yu((float*)(w + u.ckY + sizeof(float) * u.R * j),
@@ -1306,9 +1334,12 @@ extern "C" int sc_unrolled_backward(const sc_problem* p, const sc_options* o, in
   const size_t Cs = (size_t)B * g.H * g.Wp;  // complex entries of one SC trace
   int G = 0;
   if (u.conv && (st = unrolled_cluster(u, &G))) return st;
-  // set-up writes zeros to the problem's Y: give it a trace slot instead of
-  // the caller's result
-  u.p.Y = Ytr;
+  // one segment with the convolution form: the forward kept every step's
+  // trace, nothing is recomputed
+  const bool traced = u.conv && u.seg == u.K;
+  // set-up writes zeros to the problem's Y: give it a slot that holds zeros
+  // anyway (the traced forward's start) or is rewritten (a trace slot)
+  u.p.Y = traced ? ckY : Ytr;
   Solve sv;
   sv.tune = false;
   if ((st = sv.setup(&u.p, &u.o, ws, pl.total, s))) return st;
@@ -1328,13 +1359,15 @@ extern "C" int sc_unrolled_backward(const sc_problem* p, const sc_options* o, in
     // Y of step i of this segment: i = 0 is the checkpoint
     auto Yat = [&](int i) { return i == 0 ? ckY + u.R * j : Ytr + u.R * (i - 1); };
     // recompute the segment
+    if (!traced) {
     CU_TRY(cudaMemcpyAsync(sv.U, ckU + u.R * j, sizeof(float) * u.R, cudaMemcpyDeviceToDevice, s));
     {
       RowParams rf = sv.rp;
       rf.Y = Yat(0);
       if ((st = launch_row<ROW_FWD_YU>(pl, rf, B, s))) return st;
     }
-    for (int i = 0; i < n; ++i) {
+    }
+    for (int i = 0; i < n && !traced; ++i) {
       ColParams cf = sv.cp;
       cf.Xtr = Xtr + u.C * i;
       if (u.conv) {

@@ -6,13 +6,18 @@ rho: adaptive rho and early stopping are not differentiated) and returns the
 coefficient maps; its backward pass returns dLoss/dD and dLoss/dS through all
 iterations.  Both passes are single calls into the native library
 (``sc_unrolled_forward`` / ``sc_unrolled_backward``): the forward pass is the
-solver's own fused iteration, keeping (Y, U) every ceil(sqrt(K)) iterations;
-the backward pass recomputes each segment once from its checkpoint (keeping
-Y and the coefficient spectra of every step) and reverses it with fused
-kernels of the same shape as the forward ones: the shrinkage subgradient
-mask, the transposed Sherman-Morrison solve (the system is Hermitian, so it
-is the forward solve again) and the dictionary and signal gradients
-accumulated in the frequency domain.
+solver's own fused iteration, keeping (Y, U) every ceil(sqrt(K)) iterations
+(``checkpoints="sqrt"``, the default); the backward pass recomputes each
+segment once from its checkpoint (keeping Y, the row spectra of X and sc of
+every step) and reverses it with fused kernels of the same shape as the
+forward ones: the shrinkage subgradient mask, the transposed
+Sherman-Morrison solve (the system is Hermitian, so it is the forward solve
+again) and the dictionary and signal gradients (for filters of at most 16
+rows, in the convolution form: the dictionary gradient as correlations over
+the filter rows).  ``checkpoints="all"`` keeps every step's trace in the
+forward pass instead (memory about K times one iterate and one spectrum),
+and the backward pass recomputes nothing; an integer sets the segment
+length.
 
 Shapes: D (Kr, Kc, M), S (B, H, W) or (H, W) float32 CUDA tensors; the result
 is (B, H, W, M) (or (H, W, M)).
@@ -79,7 +84,7 @@ def _l1_weight(opt, M, H, W, device):
 
 class _Unrolled(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, D, S, lmbda, opt):
+    def forward(ctx, D, S, lmbda, opt, checkpoints="sqrt"):
         Dm = D.detach().permute(2, 0, 1).contiguous().float()
         Sb = S.detach().float().contiguous()
         B, H, W = Sb.shape
@@ -95,7 +100,12 @@ class _Unrolled(torch.autograd.Function):
         Y = torch.empty((B, M, H, W), device=S.device)
         ds = prepare_device(Dm, Sb, lmbda, fopt, l1=_l1_weight(opt, M, H, W, S.device), Y=Y,
                             check_every=0, workspace=False)
-        seg = max(1, int(math.ceil(math.sqrt(K))))
+        if checkpoints == "all":
+            seg = K
+        elif checkpoints == "sqrt":
+            seg = max(1, int(math.ceil(math.sqrt(K))))
+        else:
+            seg = int(checkpoints)
         nbytes = _lib.sc_unrolled_workspace_size(C.byref(ds.prob), C.byref(ds.opts), seg)
         if nbytes == 0:
             _lib.check_last()
@@ -117,14 +127,14 @@ class _Unrolled(torch.autograd.Function):
             C.byref(ds.prob), C.byref(ds.opts), ctx.seg, C.c_void_p(ctx.ws.data_ptr()),
             ctx.ws.numel(), C.c_void_p(gY.data_ptr()), C.c_void_p(gD.data_ptr()),
             C.c_void_p(gS.data_ptr()), _stream()))
-        return gD.permute(1, 2, 0).contiguous().reshape(ctx.dshape), gS, None, None
+        return gD.permute(1, 2, 0).contiguous().reshape(ctx.dshape), gS, None, None, None
 
 
-def cbpdn_unrolled(D, S, lmbda, opt):
+def cbpdn_unrolled(D, S, lmbda, opt, checkpoints="sqrt"):
     """Differentiable fixed-iteration cbpdn (see the module docstring)."""
     single = S.ndim == 2
     Sb = S[None] if single else S
-    X = _Unrolled.apply(D, Sb, lmbda, opt)
+    X = _Unrolled.apply(D, Sb, lmbda, opt, checkpoints)
     return X[0] if single else X
 
 

@@ -113,19 +113,22 @@ def test_unrolled_gradients_match_fp64_autograd_and_fd(shape, form, monkeypatch)
     Y_K, the value of |Y_K| wherever the signs agree, so that an active
     coefficient next to zero puts no kink inside the difference step).
     "transform" forces the transform-solve
-    adjoint (SPORCO_B200_ADJOINT) where the convolution form would run."""
+    adjoint (SPORCO_B200_ADJOINT) where the convolution form would run;
+    "traced" keeps every step's trace in the forward pass (one segment) so
+    that the backward pass recomputes nothing."""
     import sporco_cuda.adjoint as adj
     B, H, W, M, K, iters = shape
+    if shape[0:2] == (2, 24) and form != "default":
+        pytest.skip("the transform form is the only one here")
     if form == "transform":
-        if shape[0:2] == (2, 24):
-            pytest.skip("the transform form is the default here")
         monkeypatch.setenv("SPORCO_B200_ADJOINT", "transform")
+    ckpt = "all" if form == "traced" else "sqrt"
     D, S, Sc = _problem(B, H, W, M, K)
     lam, rho, alpha = _consts()
     opt = dict(_opt(), MaxMainIter=iters)
     Dg = torch.tensor(D, device="cuda", requires_grad=True)
     Sg = torch.tensor(S, device="cuda", requires_grad=True)
-    X = adj.cbpdn_unrolled(Dg, Sg, LAM, opt)
+    X = adj.cbpdn_unrolled(Dg, Sg, LAM, opt, checkpoints=ckpt)
     R = adj.reconstruct(Dg, X)
     L = torch.sum((R - torch.tensor(Sc, device="cuda")) ** 2) + BETA * torch.sum(torch.abs(X))
     L.backward()

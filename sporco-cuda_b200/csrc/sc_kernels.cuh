@@ -907,17 +907,19 @@ col_kernel(ColParams P) {
         issue_E(m0, Es);
       }
       cp_async_commit();
+      // One barrier per map: after it, map m's tiles are visible and every
+      // thread is done with map m - 1's buffers, which then take map m + 1.
       int it = 0;
       for (int m = m0; m < m1; ++m, ++it) {
         const float2* cur = (it & 1) ? Bt : A;
         const float2* ecur = Es + (it & 1) * KMAX * T;
+        cp_async_wait<0>();  // P(m), E(m): the only copies in flight
+        __syncthreads();
         if (m + 1 < m1) {
           issue_tile(Fi + (size_t)(m + 1) * plane, (it & 1) ? A : Bt);
           issue_E(m + 1, Es + ((it + 1) & 1) * KMAX * T);
         }
         cp_async_commit();
-        cp_async_wait<1>();  // P(m), E(m)
-        __syncthreads();
         // w[j] = P(r0 - (KMAX - 1) + j): the window of all L outputs
         float2 w[NW];
 #pragma unroll
@@ -939,7 +941,6 @@ col_kernel(ColParams P) {
             }
           }
         }
-        __syncthreads();  // before the buffer is refilled
       }
       cp_async_commit();
       cp_async_wait<0>();
@@ -1052,17 +1053,29 @@ col_kernel(ColParams P) {
       if constexpr (!GRD) load_window();
       // rho / d at this thread's rows (GRD)
       const float rho_c = rho;
+      // One barrier per map as in pass 1, except in the adjoint, whose
+      // per-warp partial sums need a barrier after the map as well.
       it = 0;
       for (int m = m0; m < m1; ++m, ++it) {
         float2* cur = (it & 1) ? Ct : Bt;
         const float2* ecur = Es + (it & 1) * KMAX * T;
-        if (m + 1 < m1) {
-          issue_tile(Fi + (size_t)(m + 1) * plane, (it & 1) ? Bt : Ct);
-          issue_E(m + 1, Es + ((it + 1) & 1) * KMAX * T);
+        if constexpr (ADJ) {
+          if (m + 1 < m1) {
+            issue_tile(Fi + (size_t)(m + 1) * plane, (it & 1) ? Bt : Ct);
+            issue_E(m + 1, Es + ((it + 1) & 1) * KMAX * T);
+          }
+          cp_async_commit();
+          cp_async_wait<1>();  // P(m), E(m)
+          __syncthreads();
+        } else {
+          cp_async_wait<0>();  // P(m), E(m): the only copies in flight
+          __syncthreads();
+          if (m + 1 < m1) {
+            issue_tile(Fi + (size_t)(m + 1) * plane, (it & 1) ? Bt : Ct);
+            issue_E(m + 1, Es + ((it + 1) & 1) * KMAX * T);
+          }
+          cp_async_commit();
         }
-        cp_async_commit();
-        cp_async_wait<1>();  // P(m), E(m)
-        __syncthreads();
         float2 o[L];
         if constexpr (GRD) {
           // IFFTcol(rho Z^_m / d) as conj(FFT(conj(rho FFT(P_m) / d)))
@@ -1155,8 +1168,8 @@ col_kernel(ColParams P) {
             for (int i = 0; i < L; ++i) xt[(size_t)i * Wp] = o[i];
           }
         }
-        __syncthreads();  // before the buffer is refilled
         if constexpr (ADJ) {
+          __syncthreads();  // the partial sums, and before the buffer is refilled
           // gE += the column sums, warps in a fixed order (one thread per
           // filter row and column)
           const float2* rp = red + (size_t)(it & 1) * (NT / 32) * KMAX * T;

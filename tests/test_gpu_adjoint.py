@@ -95,7 +95,7 @@ def _gpu_masks(D, S, iters):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("form", ["default", "transform"])
+@pytest.mark.parametrize("form", ["default", "transform", "traced"])
 @pytest.mark.parametrize("shape", SHAPES)
 def test_unrolled_gradients_match_fp64_autograd_and_fd(shape, form, monkeypatch):
     """The hand-written adjoint against torch FP64 autograd and FP64 central

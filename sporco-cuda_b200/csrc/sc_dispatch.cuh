@@ -50,6 +50,13 @@ ColFn sc_col_fn_aux(int mode, int n);
 // SOLVE_W).
 ColFn sc_col_fn_conv_r8(int mode, int n);
 ColFn sc_col_fn_solve_r8(int mode, int n);
+// Two-column tiles of the convolution solves (C8, C16, G16) at the compiled
+// lengths from 512, with the default radix (rm 16) or the radix-8 plan (rm 8,
+// lengths 512, 768, 1024): sc_inst_col_conv_t2.cu; nullptr elsewhere.
+ColFn sc_col_fn_conv_t2(int mode, int n, int rm);
+__host__ __device__ constexpr bool col_has_t2(int mode) {
+  return mode == COL_SOLVE_C8 || mode == COL_SOLVE_C16 || mode == COL_SOLVE_G16;
+}
 // The column-pass modes with a radix-8 alternative.
 __host__ __device__ constexpr bool col_has_r8(int mode) {
   return mode == COL_SOLVE_C8 || mode == COL_SOLVE_C16 || mode == COL_SOLVE_G16 ||
@@ -73,6 +80,10 @@ inline ColFn col_fn(int n) {
     return sc_col_fn_aux(MODE, n);
 }
 
+// MODE at length n with column radix rm and tiles of tw columns (nullptr
+// when that variant is not compiled).
+template <int MODE>
+inline ColFn col_fn_variant(int n, int rm, int tw);
 // The radix-8 alternative of MODE at length n (nullptr when there is none).
 template <int MODE>
 inline ColFn col_fn_r8(int n) {
@@ -82,4 +93,13 @@ inline ColFn col_fn_r8(int n) {
     return sc_col_fn_solve_r8(MODE, n);
   else
     return nullptr;
+}
+
+template <int MODE>
+inline ColFn col_fn_variant(int n, int rm, int tw) {
+  if (tw == SC_COL_TILE) return rm == col_radix(n) ? col_fn<MODE>(n) : col_fn_r8<MODE>(n);
+  if constexpr (col_has_t2(MODE)) {
+    if (tw == 2) return sc_col_fn_conv_t2(MODE, n, rm);
+  }
+  return nullptr;
 }

@@ -45,3 +45,20 @@ ColFn col_table_r8(int n) {
 #undef SC_COL_CASE
   return nullptr;
 }
+
+// Two-column tiles at the compiled lengths from 512 (rm 16: the default
+// plans; rm 8: the radix-8 plans at 512, 768, 1024).  nullptr otherwise.
+#define SC_SPEC_COL_T2(X) X(512) X(768) X(1024) X(1536) X(2048)
+template <int MODE>
+ColFn col_table_t2(int n, int rm) {
+  if (rm == 8) {
+#define SC_COL_CASE(k) case k: return col_kernel<MODE, k, 8, 2>;
+    switch (n) { SC_SPEC_COL_R8(SC_COL_CASE) default: break; }
+#undef SC_COL_CASE
+    return nullptr;
+  }
+#define SC_COL_CASE(k) case k: return col_kernel<MODE, k, 0, 2>;
+  switch (n) { SC_SPEC_COL_T2(SC_COL_CASE) default: break; }
+#undef SC_COL_CASE
+  return nullptr;
+}

@@ -736,13 +736,16 @@ row_kernel(RowParams P) {
 // [slot(kr) * T + c]; thread tid works on column c = tid % T and, in the
 // element loops, on rows kr = tid / T + i g.
 // RADIX: the radix of the column transform plan (0: col_radix(NH)); it sets
-// the threads per column (NH / RADIX) and the rows per thread.
-template <int MODE, int NH, int RADIX = 0>
+// the threads per column (NH / RADIX) and the rows per thread.  TW: columns
+// per tile (4, or 2 for the convolution solves: half the shared memory and
+// threads per CTA, twice the tiles).
+template <int MODE, int NH, int RADIX = 0, int TW = SC_COL_TILE>
 __global__ void __launch_bounds__(SC_COL_MAX_THREADS)
 col_kernel(ColParams P) {
   pdl_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  constexpr int T = SC_COL_TILE;
+  constexpr int T = TW;
+  static_assert(T == 2 || T == 4, "tiles of 2 or 4 columns");
   constexpr int RM = RADIX > 0 ? RADIX : col_radix(NH);
   // elements of the tile per thread (compile-time bound)
   constexpr int EPT = NH > 0 ? (NH + ct_threads(NH, RM) - 1) / ct_threads(NH, RM) : SC_MAXE;
@@ -854,15 +857,17 @@ col_kernel(ColParams P) {
       // ADJ: the forward's sc / rho tile, then per-warp correlation partials
       float2* W4 = Es + 2 * KMAX * T;
       float2* red = W4 + TL;      // [2][NT / 32][KMAX][T]
+      // 16-byte copies: T / 2 per tile row
+      constexpr int CPR = T / 2;
       auto issue_tile = [&](const float2* base, float2* dst) {
-        for (int q = tid; q < 2 * H; q += NT) {
-          const int kr = q >> 1, h = q & 1;
+        for (int q = tid; q < CPR * H; q += NT) {
+          const int kr = q / CPR, h = q % CPR;
           cp_async16(dst + slot(kr) * T + 2 * h, base + (size_t)kr * Wp + c0 + 2 * h);
         }
       };
       auto issue_E = [&](int m, float2* dst) {
-        for (int q = tid; q < 2 * Kr; q += NT) {
-          const int r = q >> 1, h = q & 1;
+        for (int q = tid; q < CPR * Kr; q += NT) {
+          const int r = q / CPR, h = q % CPR;
           cp_async16(dst + r * T + 2 * h, P.E + ((size_t)m * Kr + r) * Wp + c0 + 2 * h);
         }
       };

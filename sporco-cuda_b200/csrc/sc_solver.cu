@@ -401,6 +401,7 @@ struct TunedG {
   int H, W, M;
   int G;
   int rm;          // column-transform radix (8, or the default col_radix(H))
+  int tw;          // columns per tile (SC_COL_TILE, or 2)
 };
 static std::vector<TunedG> g_tuned;
 
@@ -425,7 +426,26 @@ static int forced_cluster(int M) {
   return G >= 1 && G <= 16 ? std::min(G, M) : 0;
 }
 
-static bool tuned_size(const void* fn, const Geom& g, int* G, int* rm = nullptr) {
+// SPORCO_B200_COL_TILE=2 or 4 fixes the tile width of the column pass where
+// that variant is compiled (elsewhere it is ignored); 0 or unset: the tuned
+// choice.
+static int forced_tile() {
+  const char* e = getenv("SPORCO_B200_COL_TILE");
+  if (!e || !*e) return 0;
+  const int tw = atoi(e);
+  return tw == 2 || tw == SC_COL_TILE ? tw : 0;
+}
+
+// SPORCO_B200_COL_RADIX=8 takes the radix-8 column plans where they are
+// compiled (lengths 512, 768, 1024; elsewhere it is ignored); 0 or unset:
+// the tuned choice.
+static int forced_radix() {
+  const char* e = getenv("SPORCO_B200_COL_RADIX");
+  return e && atoi(e) == 8 ? 8 : 0;
+}
+
+static bool tuned_size(const void* fn, const Geom& g, int* G, int* rm = nullptr,
+                       int* tw = nullptr) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return false;
   std::lock_guard<std::mutex> lock(g_cache_mu);
@@ -433,51 +453,65 @@ static bool tuned_size(const void* fn, const Geom& g, int* G, int* rm = nullptr)
     if (e.dev == dev && e.fn == fn && e.H == g.H && e.W == g.W && e.M == g.M) {
       *G = e.G;
       if (rm) *rm = e.rm;
+      if (tw) *tw = e.tw;
       return true;
     }
   return false;
 }
 
 // Threads per column, threads per CTA and shared-memory slots per column of
-// the compiled column transform of length H with radix rm.
+// the compiled column transform of length H with radix rm, tiles of tw
+// columns.
 struct ColShape {
   int g, NT, hlen;
 };
-static ColShape col_shape(int H, int rm) {
+static ColShape col_shape(int H, int rm, int tw = SC_COL_TILE) {
   const int g = ct_threads(H, rm);
-  return {g, SC_COL_TILE * g, ct_len(H, rm, SC_COL_TILE)};
+  return {g, tw * g, ct_len(H, rm, tw)};
 }
 
 // force_G > 0: launch with that cluster size, force_rm > 0 with that column
-// radix (the autotuner's trials); otherwise the tuned choice for the shape,
-// else the occupancy model's cluster size at the default radix.
+// radix, force_tw > 0 with tiles of that many columns (the autotuner's
+// trials); otherwise the tuned choice for the shape, else the occupancy
+// model's cluster size at the default radix and tile.
 template <int MODE>
 static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s, int force_G = 0,
-                      int force_rm = 0) {
+                      int force_rm = 0, int force_tw = 0) {
   cp.Hs = pl.Hs;
   if (col_clustered(MODE)) {
-    const ColFn fn0 = col_fn<MODE>(cp.g.H);  // default radix: the tuning key
+    const ColFn fn0 = col_fn<MODE>(cp.g.H);  // default radix and tile: the tuning key
     int G = force_G > 0 ? force_G : forced_cluster(cp.g.M);
-    int rm = force_rm;
+    int rm = force_rm, tw = force_tw;
     if (G <= 0) {
-      int tG = 0, trm = 0;
-      if (tuned_size((const void*)fn0, cp.g, &tG, &trm)) {
+      int tG = 0, trm = 0, ttw = 0;
+      if (tuned_size((const void*)fn0, cp.g, &tG, &trm, &ttw)) {
         G = tG;
         if (rm <= 0) rm = trm;
+        if (tw <= 0) tw = ttw;
       }
     }
+    if (force_rm <= 0 && forced_radix() > 0 && col_fn_variant<MODE>(cp.g.H, 8, SC_COL_TILE))
+      rm = 8;
     if (rm <= 0) rm = col_radix(cp.g.H);
+    if (force_tw <= 0) {
+      const int ftw = forced_tile();
+      if (ftw > 0 && col_fn_variant<MODE>(cp.g.H, rm, ftw)) tw = ftw;
+    }
+    if (tw <= 0) tw = SC_COL_TILE;
     ColFn fn = fn0;
     ColShape sh{pl.col_g, pl.col_NT, pl.col_hlen};
-    if (rm != col_radix(cp.g.H)) {
-      fn = col_fn_r8<MODE>(cp.g.H);
-      if (!fn) return set_status(SC_ERR_INVALID, "no radix-%d column plan at %d", rm, cp.g.H);
-      sh = col_shape(cp.g.H, rm);
+    if (rm != col_radix(cp.g.H) || tw != SC_COL_TILE) {
+      fn = col_fn_variant<MODE>(cp.g.H, rm, tw);
+      if (!fn)
+        return set_status(SC_ERR_INVALID, "no radix-%d column plan with %d-column tiles at %d",
+                          rm, tw, cp.g.H);
+      sh = col_shape(cp.g.H, rm, tw);
     }
     int st = prepare_fn((const void*)fn, true);
     if (st) return st;
-    const size_t smem = col_smem_bytes(MODE, sh.hlen);
-    const long units = (long)pl.col_ntiles * B;
+    const size_t smem = col_smem_bytes(MODE, sh.hlen, tw);
+    const int ntiles = (cp.g.Wf + tw - 1) / tw;
+    const long units = (long)ntiles * B;
     if (G > 0 && force_G <= 0) {
       int n = 0;  // an override or a tuned size only where such a cluster fits
       if ((st = resident_clusters((const void*)fn, sh.NT, smem, G, &n))) return st;
@@ -488,7 +522,7 @@ static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s, int f
     cp.gsz = sh.g;
     cp.G = G;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(G, pl.col_ntiles, B);
+    cfg.gridDim = dim3(G, ntiles, B);
     cfg.blockDim = dim3(sh.NT);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
@@ -750,64 +784,71 @@ struct Solve {
     return SC_OK;
   }
 
-  // The column pass of the iteration at cluster size G and column radix rm
-  // (0: the tuned choice, else the model at the default radix).
-  int launch_iter_col(int G, int rm = 0) {
+  // The column pass of the iteration at cluster size G, column radix rm and
+  // tiles of tw columns (0: the tuned choice, else the model at the default
+  // radix and tile).
+  int launch_iter_col(int G, int rm = 0, int tw = 0) {
     const int B = pl.g.B;
     if (G <= 0) G = force_G;
     switch (col_mode) {
-      case COL_SOLVE_W: return launch_col<COL_SOLVE_W>(pl, cp, B, s, G, rm);
-      case COL_SOLVE: return launch_col<COL_SOLVE>(pl, cp, B, s, G, rm);
-      case COL_SOLVE_C8: return launch_col<COL_SOLVE_C8>(pl, cp, B, s, G, rm);
-      case COL_SOLVE_C16: return launch_col<COL_SOLVE_C16>(pl, cp, B, s, G, rm);
-      case COL_SOLVE_G16: return launch_col<COL_SOLVE_G16>(pl, cp, B, s, G, rm);
-      default: return launch_col<COL_SOLVE_P>(pl, cp, B, s, G, rm);
+      case COL_SOLVE_W: return launch_col<COL_SOLVE_W>(pl, cp, B, s, G, rm, tw);
+      case COL_SOLVE: return launch_col<COL_SOLVE>(pl, cp, B, s, G, rm, tw);
+      case COL_SOLVE_C8: return launch_col<COL_SOLVE_C8>(pl, cp, B, s, G, rm, tw);
+      case COL_SOLVE_C16: return launch_col<COL_SOLVE_C16>(pl, cp, B, s, G, rm, tw);
+      case COL_SOLVE_G16: return launch_col<COL_SOLVE_G16>(pl, cp, B, s, G, rm, tw);
+      default: return launch_col<COL_SOLVE_P>(pl, cp, B, s, G, rm, tw);
     }
   }
-  // The iteration's column kernel at the default radix (r8: the radix-8
-  // alternative, nullptr when the length has none).
-  const void* iter_col_fn(bool r8 = false) const {
+  // The iteration's column kernel with radix rm and tiles of tw columns
+  // (nullptr when that variant is not compiled for the length).
+  const void* iter_col_fn(int rm, int tw) const {
     const int H = pl.g.H;
     switch (col_mode) {
-      case COL_SOLVE_W: return r8 ? (const void*)col_fn_r8<COL_SOLVE_W>(H) : (const void*)col_fn<COL_SOLVE_W>(H);
-      case COL_SOLVE: return r8 ? (const void*)col_fn_r8<COL_SOLVE>(H) : (const void*)col_fn<COL_SOLVE>(H);
-      case COL_SOLVE_C8: return r8 ? (const void*)col_fn_r8<COL_SOLVE_C8>(H) : (const void*)col_fn<COL_SOLVE_C8>(H);
-      case COL_SOLVE_C16: return r8 ? (const void*)col_fn_r8<COL_SOLVE_C16>(H) : (const void*)col_fn<COL_SOLVE_C16>(H);
-      case COL_SOLVE_G16: return r8 ? (const void*)col_fn_r8<COL_SOLVE_G16>(H) : (const void*)col_fn<COL_SOLVE_G16>(H);
-      default: return r8 ? (const void*)col_fn_r8<COL_SOLVE_P>(H) : (const void*)col_fn<COL_SOLVE_P>(H);
+      case COL_SOLVE_W: return (const void*)col_fn_variant<COL_SOLVE_W>(H, rm, tw);
+      case COL_SOLVE: return (const void*)col_fn_variant<COL_SOLVE>(H, rm, tw);
+      case COL_SOLVE_C8: return (const void*)col_fn_variant<COL_SOLVE_C8>(H, rm, tw);
+      case COL_SOLVE_C16: return (const void*)col_fn_variant<COL_SOLVE_C16>(H, rm, tw);
+      case COL_SOLVE_G16: return (const void*)col_fn_variant<COL_SOLVE_G16>(H, rm, tw);
+      default: return (const void*)col_fn_variant<COL_SOLVE_P>(H, rm, tw);
     }
   }
 
   // Autotuner of the column pass: the first solve of a shape in a process
-  // times the iteration's column pass for every column plan the length has
-  // (the default radix, and radix 8 where the default is 16: twice the
-  // threads per column, half the rows per thread) at every cluster size the
-  // device can hold with it (kClusterSizes, at most M; two rounds, the faster
-  // time of each kept) on the freshly initialised state, keeps the fastest
-  // (radix, cluster size) for later launches of that shape and initialises
-  // the iterates again (the trials overwrite the spectra).  It waits for the
-  // device once, at that first set-up.
+  // times the iteration's column pass for every variant the length has
+  // compiled: the column plan (the default radix, and radix 8 where the
+  // default is 16: twice the threads per column, half the rows per thread),
+  // the tile width (4 columns, or 2 for the convolution solves at lengths
+  // from 512: half the threads and shared memory per CTA, twice the tiles)
+  // and every cluster size the device can hold with it (kClusterSizes, at
+  // most M); two rounds, the faster time of each kept, on the freshly
+  // initialised state.  It keeps the fastest (radix, tile, cluster size) for
+  // later launches of that shape and initialises the iterates again (the
+  // trials overwrite the spectra).  It waits for the device once, at that
+  // first set-up.
   int tune_col() {
     const Geom& g = pl.g;
-    const void* fn = iter_col_fn();
+    const int rdef = col_radix(g.H);
+    const void* fn = iter_col_fn(rdef, SC_COL_TILE);
     int G0 = 0;
     if (forced_cluster(g.M) > 0 || tuned_size(fn, g, &G0)) return SC_OK;
     int st;
-    struct Cand { int rm, G; float ms; };
+    struct Cand { int rm, tw, G; float ms; };
     std::vector<Cand> cand;
-    const int rdef = col_radix(g.H);
-    for (int r8 = 0; r8 < 2; ++r8) {
-      const void* f = iter_col_fn(r8 != 0);
-      if (!f || (r8 && rdef == 8)) continue;
-      const int rm = r8 ? 8 : rdef;
-      const ColShape sh = col_shape(g.H, rm);
-      if ((st = prepare_fn(f, true))) return st;
-      const size_t smem = col_smem_bytes(col_mode, sh.hlen);
-      for (int G : kClusterSizes) {
-        int n = 0;
-        if (G > g.M) continue;
-        if ((st = resident_clusters(f, sh.NT, smem, G, &n))) return st;
-        if (n >= 1) cand.push_back({rm, G, 1e30f});
+    for (int k = 0; k < 2; ++k) {
+      const int rm = k ? 8 : rdef;
+      if (k && rdef == 8) continue;
+      for (int tw : {SC_COL_TILE, 2}) {
+        const void* f = iter_col_fn(rm, tw);
+        if (!f) continue;
+        const ColShape sh = col_shape(g.H, rm, tw);
+        if ((st = prepare_fn(f, true))) return st;
+        const size_t smem = col_smem_bytes(col_mode, sh.hlen, tw);
+        for (int G : kClusterSizes) {
+          int n = 0;
+          if (G > g.M) continue;
+          if ((st = resident_clusters(f, sh.NT, smem, G, &n))) return st;
+          if (n >= 1) cand.push_back({rm, tw, G, 1e30f});
+        }
       }
     }
     const int nc = (int)cand.size();
@@ -820,7 +861,7 @@ struct Solve {
       for (int i = 0; i < nc && !st; ++i) {
         float ms = 0.f;
         if (cudaEventRecord(e0, s) != cudaSuccess) { st = SC_ERR_CUDA; break; }
-        st = launch_iter_col(cand[i].G, cand[i].rm);
+        st = launch_iter_col(cand[i].G, cand[i].rm, cand[i].tw);
         if (!st && cudaEventRecord(e1, s) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
             cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
           cand[i].ms = std::min(cand[i].ms, ms);
@@ -835,8 +876,8 @@ struct Solve {
     if (autotune_verbose()) {
       fprintf(stderr, "sporco_b200 autotune: column pass %dx%d M=%d:", g.H, g.W, g.M);
       for (int i = 0; i < nc; ++i)
-        fprintf(stderr, " r%d/G=%d %.3f ms", cand[i].rm, cand[i].G, cand[i].ms);
-      fprintf(stderr, " -> r%d/G=%d\n", cand[bi].rm, cand[bi].G);
+        fprintf(stderr, " r%d/t%d/G=%d %.3f ms", cand[i].rm, cand[i].tw, cand[i].G, cand[i].ms);
+      fprintf(stderr, " -> r%d/t%d/G=%d\n", cand[bi].rm, cand[bi].tw, cand[bi].G);
     }
     int dev = 0;
     CU_TRY(cudaGetDevice(&dev));
@@ -846,7 +887,8 @@ struct Solve {
       bool known = false;
       for (const TunedG& e : g_tuned)
         known = known || (e.dev == dev && e.fn == fn && e.H == g.H && e.W == g.W && e.M == g.M);
-      if (!known) g_tuned.push_back({dev, fn, g.H, g.W, g.M, cand[bi].G, cand[bi].rm});
+      if (!known)
+        g_tuned.push_back({dev, fn, g.H, g.W, g.M, cand[bi].G, cand[bi].rm, cand[bi].tw});
     }
     return init_iterates();
   }
@@ -1185,8 +1227,9 @@ static int unrolled_plan(const sc_problem* p, const sc_options* o, int seg, Unro
 static int unrolled_cluster(const Unrolled& u, int* G) {
   const void* fc = u.conv_mode == COL_SOLVE_C8 ? (const void*)col_fn<COL_SOLVE_C8>(u.pl.g.H)
                                                : (const void*)col_fn<COL_SOLVE_C16>(u.pl.g.H);
-  int rm = 0;
-  if (tuned_size(fc, u.pl.g, G, &rm) && rm == col_radix(u.pl.g.H)) return SC_OK;
+  int rm = 0, tw = 0;
+  if (tuned_size(fc, u.pl.g, G, &rm, &tw) && rm == col_radix(u.pl.g.H) && tw == SC_COL_TILE)
+    return SC_OK;
   const void* fn = u.trace_mode == COL_SOLVE_C8T ? (const void*)col_fn<COL_SOLVE_C8T>(u.pl.g.H)
                                                  : (const void*)col_fn<COL_SOLVE_C16T>(u.pl.g.H);
   int st = prepare_fn(fn, true);

@@ -853,9 +853,9 @@ col_kernel(ColParams P) {
       float2* A = stg;            // cluster sum, its spectrum, then sc / rho
       float2* Bt = stg + TL;      // spectrum tiles (pass 1: with A; pass 2: with Ct)
       float2* Ct = stg + 2 * TL;  // partial sums of this CTA
-      float2* Es = stg + 3 * TL;  // [2][KMAX][T] filter rows
+      float2* Es = stg + 3 * TL;  // [3][KMAX][T] filter rows
       // ADJ: the forward's sc / rho tile, then per-warp correlation partials
-      float2* W4 = Es + 2 * KMAX * T;
+      float2* W4 = Es + 3 * KMAX * T;
       float2* red = W4 + TL;      // [2][NT / 32][KMAX][T]
       // 16-byte copies: T / 2 per tile row
       constexpr int CPR = T / 2;
@@ -904,25 +904,33 @@ col_kernel(ColParams P) {
       };
 
       // ------------------------------------------------------------ pass 1
+      // The three tile buffers rotate: map m's tiles are copied two maps
+      // ahead.  One barrier per map: after it, map m's tiles are visible and
+      // every thread is done with map m - 1's buffers, which then take map
+      // m + 2.
+      auto buf = [&](int i) -> float2* { return i == 0 ? A : i == 1 ? Bt : Ct; };
       float2 acc[L];
 #pragma unroll
       for (int i = 0; i < L; ++i) acc[i] = make_float2(0.f, 0.f);
-      if (m0 < m1) {
-        issue_tile(Fi + (size_t)m0 * plane, A);
-        issue_E(m0, Es);
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        if (m0 + q < m1) {
+          issue_tile(Fi + (size_t)(m0 + q) * plane, buf(q));
+          issue_E(m0 + q, Es + q * KMAX * T);
+        }
+        cp_async_commit();
       }
-      cp_async_commit();
-      // One barrier per map: after it, map m's tiles are visible and every
-      // thread is done with map m - 1's buffers, which then take map m + 1.
       int it = 0;
-      for (int m = m0; m < m1; ++m, ++it) {
-        const float2* cur = (it & 1) ? Bt : A;
-        const float2* ecur = Es + (it & 1) * KMAX * T;
-        cp_async_wait<0>();  // P(m), E(m): the only copies in flight
+      int bi = 0;  // it mod 3
+      for (int m = m0; m < m1; ++m, ++it, bi = bi == 2 ? 0 : bi + 1) {
+        const float2* cur = buf(bi);
+        const float2* ecur = Es + bi * KMAX * T;
+        cp_async_wait<1>();  // P(m), E(m) (those of m + 1 may still be in flight)
         __syncthreads();
-        if (m + 1 < m1) {
-          issue_tile(Fi + (size_t)(m + 1) * plane, (it & 1) ? A : Bt);
-          issue_E(m + 1, Es + ((it + 1) & 1) * KMAX * T);
+        if (m + 2 < m1) {
+          const int bn = bi == 0 ? 2 : bi - 1;  // (it + 2) mod 3
+          issue_tile(Fi + (size_t)(m + 2) * plane, buf(bn));
+          issue_E(m + 2, Es + bn * KMAX * T);
         }
         cp_async_commit();
         // w[j] = P(r0 - (KMAX - 1) + j): the window of all L outputs
@@ -980,6 +988,17 @@ col_kernel(ColParams P) {
 #pragma unroll
         for (int i = 0; i < L; ++i) A[rslot(i) * T + cc] = acc[i];
         __syncthreads();
+      }
+      // The plain solves (and their trace twins) copy pass 2's tiles two maps
+      // ahead as well, over the three tile buffers (A is free once the
+      // window is in registers): the second tile lands in Ct, free now.
+      constexpr bool PIPE3 = !GRD && !ADJ;
+      if constexpr (PIPE3) {
+        if (m0 + 1 < m1) {
+          issue_tile(Fi + (size_t)(m0 + 1) * plane, Ct);
+          issue_E(m0 + 1, Es + KMAX * T);
+        }
+        cp_async_commit();
       }
       // ------------ SC = S^ - cb, sc = IFFTcol(SC) / rho (GRD: IFFTcol(SC / d))
       // 1 / d at row kr of this thread's column (GRD)
@@ -1059,12 +1078,24 @@ col_kernel(ColParams P) {
       // rho / d at this thread's rows (GRD)
       const float rho_c = rho;
       // One barrier per map as in pass 1, except in the adjoint, whose
-      // per-warp partial sums need a barrier after the map as well.
+      // per-warp partial sums need a barrier after the map as well.  PIPE3:
+      // buffers Bt, Ct, A in rotation, copies two maps ahead; otherwise Bt
+      // and Ct alternate, copies one map ahead.
       it = 0;
-      for (int m = m0; m < m1; ++m, ++it) {
-        float2* cur = (it & 1) ? Ct : Bt;
-        const float2* ecur = Es + (it & 1) * KMAX * T;
-        if constexpr (ADJ) {
+      bi = 0;
+      for (int m = m0; m < m1; ++m, ++it, bi = bi == 2 ? 0 : bi + 1) {
+        float2* cur = PIPE3 ? (bi == 0 ? Bt : bi == 1 ? Ct : A) : (it & 1) ? Ct : Bt;
+        const float2* ecur = Es + (PIPE3 ? bi : (it & 1)) * KMAX * T;
+        if constexpr (PIPE3) {
+          cp_async_wait<1>();  // P(m), E(m) (those of m + 1 may still be in flight)
+          __syncthreads();
+          if (m + 2 < m1) {
+            const int bn = bi == 0 ? 2 : bi - 1;  // (it + 2) mod 3
+            issue_tile(Fi + (size_t)(m + 2) * plane, bn == 0 ? Bt : bn == 1 ? Ct : A);
+            issue_E(m + 2, Es + bn * KMAX * T);
+          }
+          cp_async_commit();
+        } else if constexpr (ADJ) {
           if (m + 1 < m1) {
             issue_tile(Fi + (size_t)(m + 1) * plane, (it & 1) ? Bt : Ct);
             issue_E(m + 1, Es + ((it + 1) & 1) * KMAX * T);

@@ -909,9 +909,6 @@ col_kernel(ColParams P) {
       // every thread is done with map m - 1's buffers, which then take map
       // m + 2.
       auto buf = [&](int i) -> float2* { return i == 0 ? A : i == 1 ? Bt : Ct; };
-      float2 acc[L];
-#pragma unroll
-      for (int i = 0; i < L; ++i) acc[i] = make_float2(0.f, 0.f);
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
         if (m0 + q < m1) {
@@ -920,40 +917,86 @@ col_kernel(ColParams P) {
         }
         cp_async_commit();
       }
-      int it = 0;
-      int bi = 0;  // it mod 3
-      for (int m = m0; m < m1; ++m, ++it, bi = bi == 2 ? 0 : bi + 1) {
-        const float2* cur = buf(bi);
-        const float2* ecur = Es + bi * KMAX * T;
-        cp_async_wait<1>();  // P(m), E(m) (those of m + 1 may still be in flight)
-        __syncthreads();
-        if (m + 2 < m1) {
-          const int bn = bi == 0 ? 2 : bi - 1;  // (it + 2) mod 3
-          issue_tile(Fi + (size_t)(m + 2) * plane, buf(bn));
-          issue_E(m + 2, Es + bn * KMAX * T);
+      // The map loop; body(cur, ecur) consumes map m's tile and filter rows.
+      auto pass1_maps = [&](auto&& body) {
+        int bi = 0;  // (m - m0) mod 3
+        for (int m = m0; m < m1; ++m, bi = bi == 2 ? 0 : bi + 1) {
+          cp_async_wait<1>();  // P(m), E(m) (those of m + 1 may still be in flight)
+          __syncthreads();
+          if (m + 2 < m1) {
+            const int bn = bi == 0 ? 2 : bi - 1;  // (m - m0 + 2) mod 3
+            issue_tile(Fi + (size_t)(m + 2) * plane, buf(bn));
+            issue_E(m + 2, Es + bn * KMAX * T);
+          }
+          cp_async_commit();
+          body(buf(bi), Es + bi * KMAX * T);
         }
-        cp_async_commit();
-        // w[j] = P(r0 - (KMAX - 1) + j): the window of all L outputs
-        float2 w[NW];
+      };
+      float2 acc[L];
+      if (Kr == KMAX) {
+        // All KMAX taps: three real multiply-adds per complex one (Gauss):
+        // with e = c + i d and P = a + i b,
+        //   Re(e P) = c (a + b) - b (c + d),  Im(e P) = c (a + b) + a (d - c),
+        // the sums of c (a + b), b (c + d) and a (d - c) kept apart over the
+        // maps and taps; c + d and d - c are formed once per map and tap,
+        // a + b once per map and window element.
+        float k1[L], k3[L], k2[L];
 #pragma unroll
-        for (int j = 0; j < NW; ++j)
-          w[j] = (j < KMAX - Kr) ? make_float2(0.f, 0.f) : cur[rslot(j - (KMAX - 1)) * T + cc];
-        // last tap first: it uses the window values that were loaded first
+        for (int i = 0; i < L; ++i) k1[i] = k2[i] = k3[i] = 0.f;
+        pass1_maps([&](const float2* cur, const float2* ecur) {
+          float ec[KMAX], ep[KMAX], em[KMAX];
 #pragma unroll
-        for (int tp = KMAX - 1; tp >= 0; --tp) {
-          if (tp < Kr) {
+          for (int tp = 0; tp < KMAX; ++tp) {
             const float2 e = ecur[tp * T + cc];
+            ec[tp] = e.x;
+            ep[tp] = e.x + e.y;
+            em[tp] = e.y - e.x;
+          }
+          // window element j = P(r0 - (KMAX - 1) + j) meets output i at tap
+          // KMAX - 1 + i - j (the last tap first, as in the general form)
+#pragma unroll
+          for (int j = 0; j < NW; ++j) {
+            const float2 v = cur[rslot(j - (KMAX - 1)) * T + cc];
+            const float sab = v.x + v.y;
 #pragma unroll
             for (int i = 0; i < L; ++i) {
-              const float2 v = w[i - tp + KMAX - 1];
-              // four fused multiply-adds per complex multiply-add
-              acc[i].x = fmaf(e.x, v.x, acc[i].x);
-              acc[i].x = fmaf(-e.y, v.y, acc[i].x);
-              acc[i].y = fmaf(e.x, v.y, acc[i].y);
-              acc[i].y = fmaf(e.y, v.x, acc[i].y);
+              const int tp = KMAX - 1 + i - j;
+              if (tp >= 0 && tp < KMAX) {
+                k1[i] = fmaf(ec[tp], sab, k1[i]);
+                k3[i] = fmaf(ep[tp], v.y, k3[i]);
+                k2[i] = fmaf(em[tp], v.x, k2[i]);
+              }
             }
           }
-        }
+        });
+#pragma unroll
+        for (int i = 0; i < L; ++i) acc[i] = make_float2(k1[i] - k3[i], k1[i] + k2[i]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < L; ++i) acc[i] = make_float2(0.f, 0.f);
+        pass1_maps([&](const float2* cur, const float2* ecur) {
+          // w[j] = P(r0 - (KMAX - 1) + j): the window of all L outputs
+          float2 w[NW];
+#pragma unroll
+          for (int j = 0; j < NW; ++j)
+            w[j] = (j < KMAX - Kr) ? make_float2(0.f, 0.f) : cur[rslot(j - (KMAX - 1)) * T + cc];
+          // last tap first: it uses the window values that were loaded first
+#pragma unroll
+          for (int tp = KMAX - 1; tp >= 0; --tp) {
+            if (tp < Kr) {
+              const float2 e = ecur[tp * T + cc];
+#pragma unroll
+              for (int i = 0; i < L; ++i) {
+                const float2 v = w[i - tp + KMAX - 1];
+                // four fused multiply-adds per complex multiply-add
+                acc[i].x = fmaf(e.x, v.x, acc[i].x);
+                acc[i].x = fmaf(-e.y, v.y, acc[i].x);
+                acc[i].y = fmaf(e.x, v.y, acc[i].y);
+                acc[i].y = fmaf(e.y, v.x, acc[i].y);
+              }
+            }
+          }
+        });
       }
       cp_async_commit();
       cp_async_wait<0>();
@@ -989,12 +1032,15 @@ col_kernel(ColParams P) {
         for (int i = 0; i < L; ++i) A[rslot(i) * T + cc] = acc[i];
         __syncthreads();
       }
-      // The plain solves (and their trace twins) copy pass 2's tiles two maps
-      // ahead as well, over the three tile buffers (A is free once the
-      // window is in registers): the second tile lands in Ct, free now.
+      // The plain solves (and their trace twins) with fewer than KMAX taps
+      // copy pass 2's tiles two maps ahead as well, over the three tile
+      // buffers (A is free once the window is in registers): the second tile
+      // lands in Ct, free now.  With all KMAX taps (GAUSS2) pass 2 streams
+      // the window from A and alternates Bt and Ct.
       constexpr bool PIPE3 = !GRD && !ADJ;
+      const bool GAUSS2 = PIPE3 && Kr == KMAX;
       if constexpr (PIPE3) {
-        if (m0 + 1 < m1) {
+        if (m0 + 1 < m1 && !GAUSS2) {
           issue_tile(Fi + (size_t)(m0 + 1) * plane, Ct);
           issue_E(m0 + 1, Es + KMAX * T);
         }
@@ -1063,6 +1109,76 @@ col_kernel(ColParams P) {
       const float hs = (float)H;
       float2* Fo = Fi + c0 + cc;
       __syncthreads();  // sc complete before the windows are read
+      auto store_out = [&](int m, const float2* o) {
+        if (colok) {
+          float2* dst = Fo + (size_t)m * plane + (size_t)r0 * Wp;
+#pragma unroll
+          for (int i = 0; i < L; ++i) dst[(size_t)i * Wp] = o[i];
+          if constexpr (TRACE) {
+            float2* xt = P.Xtr + (size_t)b * M * plane + c0 + cc + (size_t)m * plane +
+                         (size_t)r0 * Wp;
+#pragma unroll
+            for (int i = 0; i < L; ++i) xt[(size_t)i * Wp] = o[i];
+          }
+        }
+      };
+      if constexpr (PIPE3) {
+        if (GAUSS2) {
+          // Gauss's form as in pass 1, for conj(E_m(t)) = c + i d
+          // (c = Re E, d = -Im E) times the window sc(r + t) / rho = a + i b
+          // streamed from A; the sums start from H P_m.
+          int it = 0;
+          for (int m = m0; m < m1; ++m, ++it) {
+            const float2* cur = (it & 1) ? Ct : Bt;
+            const float2* ecur = Es + (it & 1) * KMAX * T;
+            cp_async_wait<0>();  // P(m), E(m): the only copies in flight
+            __syncthreads();
+            if (m + 1 < m1) {
+              issue_tile(Fi + (size_t)(m + 1) * plane, (it & 1) ? Bt : Ct);
+              issue_E(m + 1, Es + ((it + 1) & 1) * KMAX * T);
+            }
+            cp_async_commit();
+            float ec[KMAX], ep[KMAX], em[KMAX];
+#pragma unroll
+            for (int tp = 0; tp < KMAX; ++tp) {
+              const float2 e = ecur[tp * T + cc];
+              ec[tp] = e.x;
+              ep[tp] = e.x - e.y;
+              em[tp] = -e.y - e.x;
+            }
+            float k1[L], k3[L], k2[L];
+#pragma unroll
+            for (int i = 0; i < L; ++i) {
+              const float2 pv = cur[rslot(i) * T + cc];
+              k1[i] = 0.f;
+              k3[i] = -hs * pv.x;
+              k2[i] = hs * pv.y;
+            }
+            // window element j = sc(r0 + j) / rho meets output i at tap j - i
+#pragma unroll
+            for (int j = 0; j < NW; ++j) {
+              const float2 v = A[rslot(j) * T + cc];
+              const float sab = v.x + v.y;
+#pragma unroll
+              for (int i = 0; i < L; ++i) {
+                const int tp = j - i;
+                if (tp >= 0 && tp < KMAX) {
+                  k1[i] = fmaf(ec[tp], sab, k1[i]);
+                  k3[i] = fmaf(ep[tp], v.y, k3[i]);
+                  k2[i] = fmaf(em[tp], v.x, k2[i]);
+                }
+              }
+            }
+            float2 o[L];
+#pragma unroll
+            for (int i = 0; i < L; ++i) o[i] = make_float2(k1[i] - k3[i], k1[i] + k2[i]);
+            store_out(m, o);
+          }
+          cp_async_commit();
+          cp_async_wait<0>();
+          return;
+        }
+      }
       // w[j] = sc(r0 + j) / rho (GRD: sc'(r0 + j)): the window of all L
       // outputs, the same for every map (GRD: re-read per map, so that it is
       // not held across the transforms)
@@ -1081,8 +1197,8 @@ col_kernel(ColParams P) {
       // per-warp partial sums need a barrier after the map as well.  PIPE3:
       // buffers Bt, Ct, A in rotation, copies two maps ahead; otherwise Bt
       // and Ct alternate, copies one map ahead.
-      it = 0;
-      bi = 0;
+      int it = 0;
+      int bi = 0;
       for (int m = m0; m < m1; ++m, ++it, bi = bi == 2 ? 0 : bi + 1) {
         float2* cur = PIPE3 ? (bi == 0 ? Bt : bi == 1 ? Ct : A) : (it & 1) ? Ct : Bt;
         const float2* ecur = Es + (PIPE3 ? bi : (it & 1)) * KMAX * T;
@@ -1193,17 +1309,7 @@ col_kernel(ColParams P) {
 #pragma unroll
           for (int i = 0; i < L; ++i) o[i] = make_float2(o[i].x * irho, o[i].y * irho);  // q_m
         }
-        if (colok) {
-          float2* dst = Fo + (size_t)m * plane + (size_t)r0 * Wp;
-#pragma unroll
-          for (int i = 0; i < L; ++i) dst[(size_t)i * Wp] = o[i];
-          if constexpr (TRACE) {
-            float2* xt = P.Xtr + (size_t)b * M * plane + c0 + cc + (size_t)m * plane +
-                         (size_t)r0 * Wp;
-#pragma unroll
-            for (int i = 0; i < L; ++i) xt[(size_t)i * Wp] = o[i];
-          }
-        }
+        store_out(m, o);
         if constexpr (ADJ) {
           __syncthreads();  // the partial sums, and before the buffer is refilled
           // gE += the column sums, warps in a fixed order (one thread per

@@ -162,18 +162,22 @@ MEASURED_TRAFFIC_PER_MAP = {
 def design_bytes(H, W, M, variant="cbpdn", K=None):
     """Per-iteration HBM bytes this design moves for one image.  Row pass:
     reads and writes the spectra F (2C) and the state V = Y + U (2R).  Column pass, by
-    solve: the convolution solves (filters of at most 16 rows, compiled
-    column length; with the gradient term one GradWeight for every map)
-    read F twice and write it (3C); the transform solve also reads the
-    dictionary spectra twice (+2 C_D, C_D = C per image); with a
-    map-dependent gradient term it also writes and re-reads the column
-    spectra between its two passes (+2C)."""
+    solve: the plain convolution solves (filters of at most 16 rows,
+    compiled column length) read F once and write the correction to it
+    (2C; the row pass adds Y - U itself); the gradient convolution solve
+    (one GradWeight for every map) reads F twice and writes it (3C); the
+    transform solve also reads the dictionary spectra twice (+2 C_D,
+    C_D = C per image); with a map-dependent gradient term it also writes
+    and re-reads the column spectra between its two passes (+2C)."""
     R = 4.0 * M * H * W
     Cs = 8.0 * M * H * (W // 2 + 1)
     grd = variant in ("cbpdngrd", "cbpdngrdmsk")
     per_map = variant == "cbpdngrdmsk"
     conv = not per_map and K is not None and K <= 16 and H in SPEC_COL
-    col = 3 * Cs if conv else 3 * Cs + 2 * Cs + (2 * Cs if grd else 0)
+    if conv:
+        col = 3 * Cs if grd else 2 * Cs
+    else:
+        col = 3 * Cs + 2 * Cs + (2 * Cs if grd else 0)
     return 2 * R + 2 * Cs + col
 
 

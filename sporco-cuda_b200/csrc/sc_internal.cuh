@@ -83,6 +83,8 @@ struct RowParams {
                            // of every map are zero (H, W: none)
   float relax;
   float invN;              // 1 / (H W)
+  int delta;               // ROW_ITER*: F holds the column pass's correction only,
+                           // X = (Y - U) + IFFTrow(F) / (H W) (ColParams::delta)
   double* partials;        // (B, nblk, 5)
   ImgState* st;            // (B,)
   // setup / tool modes
@@ -108,6 +110,8 @@ struct ColParams {
   const float2* Dh;        // (M, H, Wp)
   const float2* Sh;        // (B, H, Wp)
   int grd;
+  int delta;               // the plain convolution solves (COL_SOLVE_C8 / C16) write
+                           // only sum_t conj(E_m(t)) sc(r + t) / rho, not H P_m plus it
   float mu;
   const float* wgrd;       // (M,)
   const float* Psum;       // (H, Wp) sum_m |Df_m|^2 (solve with one d for all maps)

@@ -161,6 +161,7 @@ struct IterC {
   float a, a1;   // RelaxParam, 1 - RelaxParam
   bool relax;    // RelaxParam != 1
   float uscale;  // the stored U is read scaled by this (1/rsf after a rho change)
+  bool delta;    // x is the column pass's correction to Y - U (RowParams::delta)
 };
 
 // One element of the iteration's element-wise step: over-relaxation,
@@ -168,7 +169,8 @@ struct IterC {
 // row pair).  VS: the stored state is V = Y + U of the previous iteration
 // (s0), whose Y is recomputed as its shrinkage at the previous threshold
 // tq; else s0, s1 are Y and U.  FAST: scalar thresholds tc, tq (weights
-// applied), no AMS row.  Writes V (VS) or Y and U; returns y - u.
+// applied), no AMS row.  x: X, or with c.delta the column pass's correction
+// to Y - U.  Writes V (VS) or Y and U; returns y - u.
 template <bool VS, bool FAST>
 __device__ __forceinline__ float iter_elem(float x, float s0, float s1, const RowW& r, int k,
                                            float tc, float tq, const IterC& c, float* f,
@@ -182,6 +184,8 @@ __device__ __forceinline__ float iter_elem(float x, float s0, float s1, const Ro
     yo = s0;
     uo = s1 * c.uscale;
   }
+  // X = IFFT2(Z^ + conj(Df) SC / rho) = (Y - U) + IFFT2(conj(Df) SC / rho)
+  if (c.delta) x += yo - uo;
   const float xr = c.relax ? c.a * x + c.a1 * yo : x;
   const float v = xr + uo;
   const float y = FAST ? soft_threshold(v, tc) : shrink_y(v, tc, r, k);
@@ -461,6 +465,7 @@ row_kernel(RowParams P) {
     ic.a1 = 1.f - P.relax;
     ic.relax = P.relax != 1.f;
     ic.uscale = uscale;
+    ic.delta = P.delta != 0;
     // State rows of the pair (V, or Y and U) are written here.
     auto out0 = [&](long r0) -> float* {
       return (VS ? P.U : P.Yo) + (size_t)b * img_real + (size_t)r0 * W;
@@ -729,6 +734,12 @@ row_kernel(RowParams P) {
   }
 }
 
+// A compile-time int passed to generic lambdas.
+template <int V>
+struct IntC {
+  static constexpr int value = V;
+};
+
 // =========================================================== column pass ==
 // Grid (G, ntiles, B).  For COL_SOLVE the G CTAs of one column tile form a
 // thread-block cluster; each handles a contiguous chunk of the maps.  Tiles
@@ -932,36 +943,59 @@ col_kernel(ColParams P) {
           body(buf(bi), Es + bi * KMAX * T);
         }
       };
+      // Filter-row counts with compile-time tap loops in Gauss's form below:
+      // KMAX, and 12 and 11 for the 16-tap modes (11 x 11 and 12 x 12
+      // filters) at up to 8 rows per thread (with 16, the extra variants
+      // cost the 16-tap one about 2 %).  f(IntC<KR>) runs for such a count;
+      // false otherwise.
+      auto with_taps = [&](auto&& f) -> bool {
+        if (Kr == KMAX) {
+          f(IntC<KMAX>{});
+          return true;
+        }
+        if constexpr (KMAX == 16 && L <= 8) {
+          if (Kr == 12) {
+            f(IntC<12>{});
+            return true;
+          }
+          if (Kr == 11) {
+            f(IntC<11>{});
+            return true;
+          }
+        }
+        return false;
+      };
       float2 acc[L];
-      if (Kr == KMAX) {
-        // All KMAX taps: three real multiply-adds per complex one (Gauss):
-        // with e = c + i d and P = a + i b,
+      const bool gauss1 = with_taps([&](auto kc) {
+        // Three real multiply-adds per complex one (Gauss): with e = c + i d
+        // and P = a + i b,
         //   Re(e P) = c (a + b) - b (c + d),  Im(e P) = c (a + b) + a (d - c),
         // the sums of c (a + b), b (c + d) and a (d - c) kept apart over the
         // maps and taps; c + d and d - c are formed once per map and tap,
         // a + b once per map and window element.
+        constexpr int KR = decltype(kc)::value;
         float k1[L], k3[L], k2[L];
 #pragma unroll
         for (int i = 0; i < L; ++i) k1[i] = k2[i] = k3[i] = 0.f;
         pass1_maps([&](const float2* cur, const float2* ecur) {
-          float ec[KMAX], ep[KMAX], em[KMAX];
+          float ec[KR], ep[KR], em[KR];
 #pragma unroll
-          for (int tp = 0; tp < KMAX; ++tp) {
+          for (int tp = 0; tp < KR; ++tp) {
             const float2 e = ecur[tp * T + cc];
             ec[tp] = e.x;
             ep[tp] = e.x + e.y;
             em[tp] = e.y - e.x;
           }
-          // window element j = P(r0 - (KMAX - 1) + j) meets output i at tap
-          // KMAX - 1 + i - j (the last tap first, as in the general form)
+          // window element j = P(r0 - (KR - 1) + j) meets output i at tap
+          // KR - 1 + i - j (the last tap first, as in the general form)
 #pragma unroll
-          for (int j = 0; j < NW; ++j) {
-            const float2 v = cur[rslot(j - (KMAX - 1)) * T + cc];
+          for (int j = 0; j < L + KR - 1; ++j) {
+            const float2 v = cur[rslot(j - (KR - 1)) * T + cc];
             const float sab = v.x + v.y;
 #pragma unroll
             for (int i = 0; i < L; ++i) {
-              const int tp = KMAX - 1 + i - j;
-              if (tp >= 0 && tp < KMAX) {
+              const int tp = KR - 1 + i - j;
+              if (tp >= 0 && tp < KR) {
                 k1[i] = fmaf(ec[tp], sab, k1[i]);
                 k3[i] = fmaf(ep[tp], v.y, k3[i]);
                 k2[i] = fmaf(em[tp], v.x, k2[i]);
@@ -971,7 +1005,8 @@ col_kernel(ColParams P) {
         });
 #pragma unroll
         for (int i = 0; i < L; ++i) acc[i] = make_float2(k1[i] - k3[i], k1[i] + k2[i]);
-      } else {
+      });
+      if (!gauss1) {
 #pragma unroll
         for (int i = 0; i < L; ++i) acc[i] = make_float2(0.f, 0.f);
         pass1_maps([&](const float2* cur, const float2* ecur) {
@@ -1001,9 +1036,13 @@ col_kernel(ColParams P) {
       cp_async_commit();
       cp_async_wait<0>();
       __syncthreads();
+      // DL: the plain solves with ColParams::delta write only the
+      // correction sum_t conj(E_m(t)) sc(r + t) / rho (the row pass adds
+      // Y - U, whose row spectra P_m are), so pass 2 reads no P tiles
+      const bool DL = !GRD && !ADJ && !TRACE && P.delta;
       // pass 2's first tile lands during the reduction and the transforms
       if (m0 < m1) {
-        issue_tile(Fi + (size_t)m0 * plane, Bt);
+        if (!DL) issue_tile(Fi + (size_t)m0 * plane, Bt);
         issue_E(m0, Es);
         if constexpr (ADJ) issue_tile(P.SCtr + (size_t)b * plane, W4);
       }
@@ -1032,16 +1071,17 @@ col_kernel(ColParams P) {
         for (int i = 0; i < L; ++i) A[rslot(i) * T + cc] = acc[i];
         __syncthreads();
       }
-      // The plain solves (and their trace twins) with fewer than KMAX taps
-      // copy pass 2's tiles two maps ahead as well, over the three tile
-      // buffers (A is free once the window is in registers): the second tile
-      // lands in Ct, free now.  With all KMAX taps (GAUSS2) pass 2 streams
-      // the window from A and alternates Bt and Ct.
+      // The plain solves (and their trace twins) copy pass 2's tiles two
+      // maps ahead as well, over the three tile buffers (A is free once the
+      // window is in registers): the second tile lands in Ct, free now.  With
+      // a tap count in Gauss's form (GAUSS2) pass 2 streams the window from A
+      // instead and alternates Bt and Ct.
       constexpr bool PIPE3 = !GRD && !ADJ;
-      const bool GAUSS2 = PIPE3 && Kr == KMAX;
+      const bool GAUSS2 =
+          PIPE3 && (Kr == KMAX || (KMAX == 16 && L <= 8 && (Kr == 12 || Kr == 11)));
       if constexpr (PIPE3) {
         if (m0 + 1 < m1 && !GAUSS2) {
-          issue_tile(Fi + (size_t)(m0 + 1) * plane, Ct);
+          if (!DL) issue_tile(Fi + (size_t)(m0 + 1) * plane, Ct);
           issue_E(m0 + 1, Es + KMAX * T);
         }
         cp_async_commit();
@@ -1122,11 +1162,46 @@ col_kernel(ColParams P) {
           }
         }
       };
+      // o[i] += sum_t conj(E_m(t)) w(r0 + i + t) over KR taps in Gauss's form
+      // (as in pass 1, for conj(E) = c + i d, c = Re E, d = -Im E), the
+      // window w = sc / rho (GRD: sc') streamed from A.
+      auto conv2 = [&](auto kc, const float2* ecur, float2* o) {
+        constexpr int KR = decltype(kc)::value;
+        float ec[KR], ep[KR], em[KR];
+#pragma unroll
+        for (int tp = 0; tp < KR; ++tp) {
+          const float2 e = ecur[tp * T + cc];
+          ec[tp] = e.x;
+          ep[tp] = e.x - e.y;
+          em[tp] = -e.y - e.x;
+        }
+        float k1[L], k3[L], k2[L];
+#pragma unroll
+        for (int i = 0; i < L; ++i) {
+          k1[i] = 0.f;
+          k3[i] = -o[i].x;
+          k2[i] = o[i].y;
+        }
+        // window element j meets output i at tap j - i
+#pragma unroll
+        for (int j = 0; j < L + KR - 1; ++j) {
+          const float2 v = A[rslot(j) * T + cc];
+          const float sab = v.x + v.y;
+#pragma unroll
+          for (int i = 0; i < L; ++i) {
+            const int tp = j - i;
+            if (tp >= 0 && tp < KR) {
+              k1[i] = fmaf(ec[tp], sab, k1[i]);
+              k3[i] = fmaf(ep[tp], v.y, k3[i]);
+              k2[i] = fmaf(em[tp], v.x, k2[i]);
+            }
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < L; ++i) o[i] = make_float2(k1[i] - k3[i], k1[i] + k2[i]);
+      };
       if constexpr (PIPE3) {
         if (GAUSS2) {
-          // Gauss's form as in pass 1, for conj(E_m(t)) = c + i d
-          // (c = Re E, d = -Im E) times the window sc(r + t) / rho = a + i b
-          // streamed from A; the sums start from H P_m.
           int it = 0;
           for (int m = m0; m < m1; ++m, ++it) {
             const float2* cur = (it & 1) ? Ct : Bt;
@@ -1134,44 +1209,17 @@ col_kernel(ColParams P) {
             cp_async_wait<0>();  // P(m), E(m): the only copies in flight
             __syncthreads();
             if (m + 1 < m1) {
-              issue_tile(Fi + (size_t)(m + 1) * plane, (it & 1) ? Bt : Ct);
+              if (!DL) issue_tile(Fi + (size_t)(m + 1) * plane, (it & 1) ? Bt : Ct);
               issue_E(m + 1, Es + ((it + 1) & 1) * KMAX * T);
             }
             cp_async_commit();
-            float ec[KMAX], ep[KMAX], em[KMAX];
-#pragma unroll
-            for (int tp = 0; tp < KMAX; ++tp) {
-              const float2 e = ecur[tp * T + cc];
-              ec[tp] = e.x;
-              ep[tp] = e.x - e.y;
-              em[tp] = -e.y - e.x;
-            }
-            float k1[L], k3[L], k2[L];
-#pragma unroll
-            for (int i = 0; i < L; ++i) {
-              const float2 pv = cur[rslot(i) * T + cc];
-              k1[i] = 0.f;
-              k3[i] = -hs * pv.x;
-              k2[i] = hs * pv.y;
-            }
-            // window element j = sc(r0 + j) / rho meets output i at tap j - i
-#pragma unroll
-            for (int j = 0; j < NW; ++j) {
-              const float2 v = A[rslot(j) * T + cc];
-              const float sab = v.x + v.y;
-#pragma unroll
-              for (int i = 0; i < L; ++i) {
-                const int tp = j - i;
-                if (tp >= 0 && tp < KMAX) {
-                  k1[i] = fmaf(ec[tp], sab, k1[i]);
-                  k3[i] = fmaf(ep[tp], v.y, k3[i]);
-                  k2[i] = fmaf(em[tp], v.x, k2[i]);
-                }
-              }
-            }
             float2 o[L];
 #pragma unroll
-            for (int i = 0; i < L; ++i) o[i] = make_float2(k1[i] - k3[i], k1[i] + k2[i]);
+            for (int i = 0; i < L; ++i) {
+              const float2 pv = DL ? make_float2(0.f, 0.f) : cur[rslot(i) * T + cc];
+              o[i] = make_float2(hs * pv.x, hs * pv.y);
+            }
+            with_taps([&](auto kc) { conv2(kc, ecur, o); });
             store_out(m, o);
           }
           cp_async_commit();
@@ -1207,7 +1255,7 @@ col_kernel(ColParams P) {
           __syncthreads();
           if (m + 2 < m1) {
             const int bn = bi == 0 ? 2 : bi - 1;  // (it + 2) mod 3
-            issue_tile(Fi + (size_t)(m + 2) * plane, bn == 0 ? Bt : bn == 1 ? Ct : A);
+            if (!DL) issue_tile(Fi + (size_t)(m + 2) * plane, bn == 0 ? Bt : bn == 1 ? Ct : A);
             issue_E(m + 2, Es + bn * KMAX * T);
           }
           cp_async_commit();
@@ -1229,6 +1277,7 @@ col_kernel(ColParams P) {
           cp_async_commit();
         }
         float2 o[L];
+        bool convd = false;  // the convolution term is added (GRD, Gauss's form)
         if constexpr (GRD) {
           // IFFTcol(rho Z^_m / d) as conj(FFT(conj(rho FFT(P_m) / d)))
           fft_any<NH, T, RM>(cur + cc, P.ph, P.twH, t, g);
@@ -1246,17 +1295,20 @@ col_kernel(ColParams P) {
             const float2 v = cur[rslot(i) * T + cc];
             o[i] = make_float2(v.x, -v.y);
           }
-          load_window();
+          // (Gauss's form only at up to 8 rows per thread: with 16, its
+          // registers next to the transforms' would spill)
+          if constexpr (L <= 8) convd = with_taps([&](auto kc) { conv2(kc, ecur, o); });
+          if (!convd) load_window();
         } else {
 #pragma unroll
           for (int i = 0; i < L; ++i) {
-            const float2 pv = cur[rslot(i) * T + cc];
+            const float2 pv = DL ? make_float2(0.f, 0.f) : cur[rslot(i) * T + cc];
             o[i] = make_float2(hs * pv.x, hs * pv.y);
           }
         }
 #pragma unroll
         for (int tp = 0; tp < KMAX; ++tp) {
-          if (tp < Kr) {
+          if (tp < Kr && !convd) {
             const float2 e = ecur[tp * T + cc];
 #pragma unroll
             for (int i = 0; i < L; ++i) {

@@ -156,6 +156,12 @@ __device__ __forceinline__ float shrink_y(float v, float th, const RowW& r, int 
   return k >= r.kcut ? 0.f : y;
 }
 
+// A compile-time int passed to generic lambdas.
+template <int V>
+struct IntC {
+  static constexpr int value = V;
+};
+
 // Per-launch constants of the iteration's element-wise step.
 struct IterC {
   float a, a1;   // RelaxParam, 1 - RelaxParam
@@ -169,9 +175,10 @@ struct IterC {
 // row pair).  VS: the stored state is V = Y + U of the previous iteration
 // (s0), whose Y is recomputed as its shrinkage at the previous threshold
 // tq; else s0, s1 are Y and U.  FAST: scalar thresholds tc, tq (weights
-// applied), no AMS row.  x: X, or with c.delta the column pass's correction
-// to Y - U.  Writes V (VS) or Y and U; returns y - u.
-template <bool VS, bool FAST>
+// applied), no AMS row.  x: X, or with c.delta (DL = 1; DL < 0: as c.delta
+// says) the column pass's correction to Y - U.  Writes V (VS) or Y and U;
+// returns y - u.
+template <bool VS, bool FAST, int DL = -1>
 __device__ __forceinline__ float iter_elem(float x, float s0, float s1, const RowW& r, int k,
                                            float tc, float tq, const IterC& c, float* f,
                                            float* o0, float* o1) {
@@ -185,7 +192,7 @@ __device__ __forceinline__ float iter_elem(float x, float s0, float s1, const Ro
     uo = s1 * c.uscale;
   }
   // X = IFFT2(Z^ + conj(Df) SC / rho) = (Y - U) + IFFT2(conj(Df) SC / rho)
-  if (c.delta) x += yo - uo;
+  if (DL == 1 || (DL < 0 && c.delta)) x += yo - uo;
   const float xr = c.relax ? c.a * x + c.a1 * yo : x;
   const float v = xr + uo;
   const float y = FAST ? soft_threshold(v, tc) : shrink_y(v, tc, r, k);
@@ -475,13 +482,16 @@ row_kernel(RowParams P) {
     // rows): x from the inverse transform zz; returns the packed y - u.
     // fast: both rows present, scalar thresholds, no AMS row.
     // fast: both rows present, scalar thresholds (tc*, tq*), no AMS row
-    auto elem_fast = [&](float tc0, float tc1, float tq0, float tq1, int k, float2 zz,
+    // (dl: IntC<1> when F holds the column pass's correction, else IntC<0>)
+    auto elem_fast = [&](auto dl, float tc0, float tc1, float tq0, float tq1, int k, float2 zz,
                          float* O0, float* Q0, float* f) -> float2 {
+      constexpr int DL = decltype(dl)::value;
       const RowW w{};
-      const float yu0 = iter_elem<VS, true>(zz.x * P.invN, ysm[k], TWO ? usm[k] : 0.f, w, k,
-                                            tc0, tq0, ic, f, O0 + k, Q0 + k);
-      const float yu1 = iter_elem<VS, true>(-zz.y * P.invN, ysm[W + k], TWO ? usm[W + k] : 0.f,
-                                            w, k, tc1, tq1, ic, f, O0 + W + k, Q0 + W + k);
+      const float yu0 = iter_elem<VS, true, DL>(zz.x * P.invN, ysm[k], TWO ? usm[k] : 0.f, w,
+                                                k, tc0, tq0, ic, f, O0 + k, Q0 + k);
+      const float yu1 = iter_elem<VS, true, DL>(-zz.y * P.invN, ysm[W + k],
+                                                TWO ? usm[W + k] : 0.f, w, k, tc1, tq1, ic, f,
+                                                O0 + W + k, Q0 + W + k);
       return make_float2(yu0, yu1);
     };
     auto elem_gen = [&](const RowW& w0, const RowW& w1, bool has1, int k, float2 zz, float* O0,
@@ -556,10 +566,14 @@ row_kernel(RowParams P) {
           float* O0 = out0(r0);
           float* Q0 = outu(r0);
           float f[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-          if (fast) {
+          if (fast && ic.delta) {
 #pragma unroll
             for (int m = 0; m < EM; ++m)
-              v[m] = elem_fast(tc0, tc1, tq0, tq1, t + g * m, v[m], O0, Q0, f);
+              v[m] = elem_fast(IntC<1>{}, tc0, tc1, tq0, tq1, t + g * m, v[m], O0, Q0, f);
+          } else if (fast) {
+#pragma unroll
+            for (int m = 0; m < EM; ++m)
+              v[m] = elem_fast(IntC<0>{}, tc0, tc1, tq0, tq1, t + g * m, v[m], O0, Q0, f);
           } else {
 #pragma unroll
             for (int m = 0; m < EM; ++m) v[m] = elem_gen(w0, w1, has1, t + g * m, v[m], O0, Q0, f);
@@ -635,9 +649,12 @@ row_kernel(RowParams P) {
           float* O0 = out0(r0);
           float* Q0 = outu(r0);
           float f[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-          if (fast) {
+          if (fast && ic.delta) {
             for (int k = t; k < W; k += g)
-              z[zs(k)] = elem_fast(tc0, tc1, tq0, tq1, k, z[zs(k)], O0, Q0, f);
+              z[zs(k)] = elem_fast(IntC<1>{}, tc0, tc1, tq0, tq1, k, z[zs(k)], O0, Q0, f);
+          } else if (fast) {
+            for (int k = t; k < W; k += g)
+              z[zs(k)] = elem_fast(IntC<0>{}, tc0, tc1, tq0, tq1, k, z[zs(k)], O0, Q0, f);
           } else {
             for (int k = t; k < W; k += g) z[zs(k)] = elem_gen(w0, w1, has1, k, z[zs(k)], O0, Q0, f);
           }
@@ -733,12 +750,6 @@ row_kernel(RowParams P) {
     }
   }
 }
-
-// A compile-time int passed to generic lambdas.
-template <int V>
-struct IntC {
-  static constexpr int value = V;
-};
 
 // =========================================================== column pass ==
 // Grid (G, ntiles, B).  For COL_SOLVE the G CTAs of one column tile form a

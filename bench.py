@@ -147,11 +147,11 @@ def graded_kernel_bytes(H, W, M):
 # in proportion to the maps, with the capture each comes from (kernels as of
 # the commit named there).
 MEASURED_TRAFFIC_PER_MAP = {
-    (2048, 2048): {"row_kernel": ((807.1e6 + 745.2e6) / 24,
-                                  "ncu capture at 2048x2048, M=24 (kernels of commit a104647), "
+    (2048, 2048): {"row_kernel": ((807.2e6 + 744.6e6) / 24,
+                                  "ncu capture at 2048x2048, M=24 (kernels of commit 193bd5b), "
                                   "scaled by the maps"),
-                   "col_kernel": ((826.7e6 + 353.7e6) / 24,
-                                  "ncu capture at 2048x2048, M=24 (kernels of commit a104647), "
+                   "col_kernel": ((454.6e6 + 357.5e6) / 24,
+                                  "ncu capture at 2048x2048, M=24 (kernels of commit 193bd5b), "
                                   "scaled by the maps")},
     (512, 512): {"col_kernel": (((216.1e6 + 49.3e6) + (218.5e6 + 56.2e6)) / 2 / 100,
                                 "ncu captures at 512x512, M=100, mean of the gradient and "
@@ -164,7 +164,8 @@ def design_bytes(H, W, M, variant="cbpdn", K=None):
     reads and writes the spectra F (2C) and the state V = Y + U (2R).  Column pass, by
     solve: the plain convolution solves (filters of at most 16 rows,
     compiled column length) read F once and write the correction to it
-    (2C; the row pass adds Y - U itself); the gradient convolution solve
+    (2C; the row pass adds Y - U itself; masked problems read F twice and
+    write it whole, 3C); the gradient convolution solve
     (one GradWeight for every map) reads F twice and writes it (3C); the
     transform solve also reads the dictionary spectra twice (+2 C_D,
     C_D = C per image); with a map-dependent gradient term it also writes
@@ -174,8 +175,9 @@ def design_bytes(H, W, M, variant="cbpdn", K=None):
     grd = variant in ("cbpdngrd", "cbpdngrdmsk")
     per_map = variant == "cbpdngrdmsk"
     conv = not per_map and K is not None and K <= 16 and H in SPEC_COL
+    masked = variant in ("cbpdnmsk", "cbpdngrdmsk")
     if conv:
-        col = 3 * Cs if grd else 2 * Cs
+        col = 3 * Cs if grd or masked else 2 * Cs
     else:
         col = 3 * Cs + 2 * Cs + (2 * Cs if grd else 0)
     return 2 * R + 2 * Cs + col

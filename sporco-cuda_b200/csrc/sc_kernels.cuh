@@ -1250,6 +1250,13 @@ col_kernel(ColParams P) {
         }
       };
       if constexpr (!GRD) load_window();
+      if constexpr (ADJ) {
+        // A is free once every window is loaded: it takes the tile of the
+        // forward's row spectra of X of each map in turn
+        __syncthreads();
+        if (m0 < m1) issue_tile(P.Xh + ((size_t)b * M + m0) * plane, A);
+        cp_async_commit();
+      }
       // rho / d at this thread's rows (GRD)
       const float rho_c = rho;
       // One barrier per map as in pass 1, except in the adjoint, whose
@@ -1335,16 +1342,78 @@ col_kernel(ColParams P) {
           // gE_m(t) partial sums over this thread's rows, taken before o is
           // scaled to q_m = o / rho: rho sc'(s + t) conj(q_m(s)) =
           // W4(s + t) conj(o(s)) with W4 = sc' (the SCtr tile); the window w
-          // is -cb', x the forward's row spectra of X at this step
-          const float2* xs = P.Xh + (size_t)b * M * plane + c0 + cc + (size_t)m * plane +
-                             (size_t)r0 * Wp;
+          // is -cb', xv the forward's row spectra of X at this step (its tile
+          // staged in A)
           float2 xv[L];
 #pragma unroll
-          for (int i = 0; i < L; ++i) xv[i] = colok ? xs[(size_t)i * Wp] : make_float2(0.f, 0.f);
+          for (int i = 0; i < L; ++i) xv[i] = A[rslot(i) * T + cc];
           const int lane = tid & 31, wid = tid >> 5;
           float2* rp = red + (size_t)(it & 1) * (NT / 32) * KMAX * T;
+          // With a compile-time tap count (12 and 11 in the 16-tap modes, 8
+          // in the 8-tap ones; 16 accumulators would spill registers):
+          // window element j = s + t outer, one accumulator per tap
+          // (independent chains; every tap still sums over the rows in
+          // ascending order), each sc' value read once
+          auto with_taps_adj = [&](auto&& f) -> bool {
+            if constexpr (KMAX == 16 && L <= 8) {
+              if (Kr == 12) {
+                f(IntC<12>{});
+                return true;
+              }
+              if (Kr == 11) {
+                f(IntC<11>{});
+                return true;
+              }
+            } else if constexpr (KMAX == 8) {
+              if (Kr == 8) {
+                f(IntC<8>{});
+                return true;
+              }
+            }
+            return false;
+          };
+          const bool corr = with_taps_adj([&](auto kc) {
+            constexpr int KR = decltype(kc)::value;
+            float2 a[KR];
+#pragma unroll
+            for (int tp = 0; tp < KR; ++tp) a[tp] = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int j = 0; j < L + KR - 1; ++j) {
+              const float2 sv = W4[rslot(j) * T + cc];  // sc'(s + t)
+              const float2 c = w[j];                    // -cb'(s + t)
+#pragma unroll
+              for (int i = 0; i < L; ++i) {
+                const int tp = j - i;
+                if (tp >= 0 && tp < KR) {
+                  // a += sv conj(o) + c conj(x)
+                  a[tp].x = fmaf(sv.x, o[i].x, a[tp].x);
+                  a[tp].x = fmaf(sv.y, o[i].y, a[tp].x);
+                  a[tp].y = fmaf(sv.y, o[i].x, a[tp].y);
+                  a[tp].y = fmaf(-sv.x, o[i].y, a[tp].y);
+                  a[tp].x = fmaf(c.x, xv[i].x, a[tp].x);
+                  a[tp].x = fmaf(c.y, xv[i].y, a[tp].x);
+                  a[tp].y = fmaf(c.y, xv[i].x, a[tp].y);
+                  a[tp].y = fmaf(-c.x, xv[i].y, a[tp].y);
+                }
+              }
+            }
+            // sum over the lanes of this column in the warp (same tid % T)
+#pragma unroll
+            for (int off = T; off < 32; off <<= 1) {
+#pragma unroll
+              for (int tp = 0; tp < KR; ++tp) {
+                a[tp].x += __shfl_xor_sync(0xffffffffu, a[tp].x, off);
+                a[tp].y += __shfl_xor_sync(0xffffffffu, a[tp].y, off);
+              }
+            }
+            if (lane < T) {
+#pragma unroll
+              for (int tp = 0; tp < KR; ++tp) rp[((size_t)wid * KMAX + tp) * T + lane] = a[tp];
+            }
+          });
 #pragma unroll
           for (int tp = 0; tp < KMAX; ++tp) {
+            if (corr) break;
             if (tp >= Kr) break;  // uniform over the CTA
             float2 a = make_float2(0.f, 0.f);
 #pragma unroll
@@ -1374,7 +1443,9 @@ col_kernel(ColParams P) {
         }
         store_out(m, o);
         if constexpr (ADJ) {
-          __syncthreads();  // the partial sums, and before the buffer is refilled
+          __syncthreads();  // the partial sums, and before the buffers are refilled
+          if (m + 1 < m1) issue_tile(P.Xh + ((size_t)b * M + m + 1) * plane, A);
+          cp_async_commit();
           // gE += the column sums, warps in a fixed order (one thread per
           // filter row and column)
           const float2* rp = red + (size_t)(it & 1) * (NT / 32) * KMAX * T;

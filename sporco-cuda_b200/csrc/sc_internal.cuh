@@ -199,13 +199,13 @@ __host__ __device__ inline size_t row_slot_bytes(int mode, int zlen, int W, int 
 // SC_COL_TILE) interleaved columns.  The solve double-buffers the spectrum
 // tile and stages the dictionary tile: [F0][F1][D]; the cluster reduction
 // reuses [F1][D].  The convolution solves use three tiles and three staged
-// filter-row tiles.
-__host__ __device__ inline size_t col_smem_bytes(int mode, int hlen, int tw = SC_COL_TILE) {
+// filter-row tiles; the convolution adjoint two more tiles (the forward's
+// SC trace and row spectra of X) and per-warp partial sums of the
+// dictionary gradient for its nt threads (two maps).
+__host__ __device__ inline size_t col_smem_bytes(int mode, int hlen, int tw = SC_COL_TILE,
+                                                 int nt = SC_COL_MAX_THREADS) {
   const size_t tile = (size_t)tw * hlen * 8;
-  // the convolution adjoint stages one more tile (the forward's SC trace)
-  // and keeps per-warp partial sums of the dictionary gradient (two maps)
-  return (col_clustered(mode) ? (col_adj_conv(mode) ? 4 : 3) * tile : tile) +
+  return (col_clustered(mode) ? (col_adj_conv(mode) ? 5 : 3) * tile : tile) +
          (size_t)3 * col_taps(mode) * tw * 8 +
-         (col_adj_conv(mode) ? (size_t)2 * (SC_COL_MAX_THREADS / 32) * col_taps(mode) * tw * 8
-                             : 0);
+         (col_adj_conv(mode) ? (size_t)2 * (nt / 32) * col_taps(mode) * tw * 8 : 0);
 }

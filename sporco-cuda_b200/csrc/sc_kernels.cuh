@@ -878,7 +878,8 @@ col_kernel(ColParams P) {
       float2* Es = stg + 3 * TL;  // [3][KMAX][T] filter rows
       // ADJ: the forward's sc / rho tile, then per-warp correlation partials
       float2* W4 = Es + 3 * KMAX * T;
-      float2* red = W4 + TL;      // [2][NT / 32][KMAX][T]
+      float2* X5 = W4 + TL;       // ADJ: the forward's row spectra of X of the map
+      float2* red = X5 + TL;      // [2][NT / 32][KMAX][T]
       // 16-byte copies: T / 2 per tile row
       constexpr int CPR = T / 2;
       auto issue_tile = [&](const float2* base, float2* dst) {
@@ -1055,7 +1056,10 @@ col_kernel(ColParams P) {
       if (m0 < m1) {
         if (!DL) issue_tile(Fi + (size_t)m0 * plane, Bt);
         issue_E(m0, Es);
-        if constexpr (ADJ) issue_tile(P.SCtr + (size_t)b * plane, W4);
+        if constexpr (ADJ) {
+          issue_tile(P.SCtr + (size_t)b * plane, W4);
+          issue_tile(P.Xh + ((size_t)b * M + m0) * plane, X5);
+        }
       }
       cp_async_commit();
 
@@ -1175,16 +1179,23 @@ col_kernel(ColParams P) {
       };
       // o[i] += sum_t conj(E_m(t)) w(r0 + i + t) over KR taps in Gauss's form
       // (as in pass 1, for conj(E) = c + i d, c = Re E, d = -Im E), the
-      // window w = sc / rho (GRD: sc') streamed from A.
+      // window w = sc / rho (GRD: sc'; ADJ: -cb', from cb' in A) streamed
+      // from A.
       auto conv2 = [&](auto kc, const float2* ecur, float2* o) {
         constexpr int KR = decltype(kc)::value;
         float ec[KR], ep[KR], em[KR];
 #pragma unroll
         for (int tp = 0; tp < KR; ++tp) {
           const float2 e = ecur[tp * T + cc];
-          ec[tp] = e.x;
-          ep[tp] = e.x - e.y;
-          em[tp] = -e.y - e.x;
+          if constexpr (ADJ) {  // -conj(E)
+            ec[tp] = -e.x;
+            ep[tp] = e.y - e.x;
+            em[tp] = e.y + e.x;
+          } else {
+            ec[tp] = e.x;
+            ep[tp] = e.x - e.y;
+            em[tp] = -e.y - e.x;
+          }
         }
         float k1[L], k3[L], k2[L];
 #pragma unroll
@@ -1211,6 +1222,31 @@ col_kernel(ColParams P) {
 #pragma unroll
         for (int i = 0; i < L; ++i) o[i] = make_float2(k1[i] - k3[i], k1[i] + k2[i]);
       };
+      // Tap counts with compile-time loops in the adjoint (12 and 11 in the
+      // 16-tap modes, 8 in the 8-tap ones; with 16 the correlation's
+      // accumulators would spill registers): f(IntC<KR>) runs for such a
+      // count; false otherwise.
+      auto with_taps_adj = [&](auto&& f) -> bool {
+        if constexpr (KMAX == 16 && L <= 8) {
+          if (Kr == 12) {
+            f(IntC<12>{});
+            return true;
+          }
+          if (Kr == 11) {
+            f(IntC<11>{});
+            return true;
+          }
+        } else if constexpr (KMAX == 8) {
+          if (Kr == 8) {
+            f(IntC<8>{});
+            return true;
+          }
+        }
+        return false;
+      };
+      // ADJ with such a tap count: the convolution in Gauss's form and the
+      // correlation read cb' from A (no window in registers)
+      const bool ADJG = ADJ && (KMAX == 16 ? (L <= 8 && (Kr == 12 || Kr == 11)) : Kr == 8);
       if constexpr (PIPE3) {
         if (GAUSS2) {
           int it = 0;
@@ -1249,13 +1285,8 @@ col_kernel(ColParams P) {
           if constexpr (ADJ) w[j] = make_float2(-w[j].x, -w[j].y);  // -cb'
         }
       };
-      if constexpr (!GRD) load_window();
-      if constexpr (ADJ) {
-        // A is free once every window is loaded: it takes the tile of the
-        // forward's row spectra of X of each map in turn
-        __syncthreads();
-        if (m0 < m1) issue_tile(P.Xh + ((size_t)b * M + m0) * plane, A);
-        cp_async_commit();
+      if constexpr (!GRD) {
+        if (!ADJG) load_window();
       }
       // rho / d at this thread's rows (GRD)
       const float rho_c = rho;
@@ -1323,6 +1354,9 @@ col_kernel(ColParams P) {
             const float2 pv = DL ? make_float2(0.f, 0.f) : cur[rslot(i) * T + cc];
             o[i] = make_float2(hs * pv.x, hs * pv.y);
           }
+          if constexpr (ADJ) {
+            if (ADJG) convd = with_taps_adj([&](auto kc) { conv2(kc, ecur, o); });
+          }
         }
 #pragma unroll
         for (int tp = 0; tp < KMAX; ++tp) {
@@ -1342,36 +1376,17 @@ col_kernel(ColParams P) {
           // gE_m(t) partial sums over this thread's rows, taken before o is
           // scaled to q_m = o / rho: rho sc'(s + t) conj(q_m(s)) =
           // W4(s + t) conj(o(s)) with W4 = sc' (the SCtr tile); the window w
-          // is -cb', xv the forward's row spectra of X at this step (its tile
-          // staged in A)
+          // is -cb' (-A), xv the forward's row spectra of X at this step (its
+          // tile staged in X5)
           float2 xv[L];
 #pragma unroll
-          for (int i = 0; i < L; ++i) xv[i] = A[rslot(i) * T + cc];
+          for (int i = 0; i < L; ++i) xv[i] = X5[rslot(i) * T + cc];
           const int lane = tid & 31, wid = tid >> 5;
           float2* rp = red + (size_t)(it & 1) * (NT / 32) * KMAX * T;
-          // With a compile-time tap count (12 and 11 in the 16-tap modes, 8
-          // in the 8-tap ones; 16 accumulators would spill registers):
-          // window element j = s + t outer, one accumulator per tap
-          // (independent chains; every tap still sums over the rows in
-          // ascending order), each sc' value read once
-          auto with_taps_adj = [&](auto&& f) -> bool {
-            if constexpr (KMAX == 16 && L <= 8) {
-              if (Kr == 12) {
-                f(IntC<12>{});
-                return true;
-              }
-              if (Kr == 11) {
-                f(IntC<11>{});
-                return true;
-              }
-            } else if constexpr (KMAX == 8) {
-              if (Kr == 8) {
-                f(IntC<8>{});
-                return true;
-              }
-            }
-            return false;
-          };
+          // With a compile-time tap count: window element j = s + t outer,
+          // one accumulator per tap (independent chains; every tap still sums
+          // over the rows in ascending order), each sc' and cb' value read
+          // once
           const bool corr = with_taps_adj([&](auto kc) {
             constexpr int KR = decltype(kc)::value;
             float2 a[KR];
@@ -1380,7 +1395,8 @@ col_kernel(ColParams P) {
 #pragma unroll
             for (int j = 0; j < L + KR - 1; ++j) {
               const float2 sv = W4[rslot(j) * T + cc];  // sc'(s + t)
-              const float2 c = w[j];                    // -cb'(s + t)
+              const float2 cbv = A[rslot(j) * T + cc];
+              const float2 c = make_float2(-cbv.x, -cbv.y);  // -cb'(s + t)
 #pragma unroll
               for (int i = 0; i < L; ++i) {
                 const int tp = j - i;
@@ -1444,7 +1460,7 @@ col_kernel(ColParams P) {
         store_out(m, o);
         if constexpr (ADJ) {
           __syncthreads();  // the partial sums, and before the buffers are refilled
-          if (m + 1 < m1) issue_tile(P.Xh + ((size_t)b * M + m + 1) * plane, A);
+          if (m + 1 < m1) issue_tile(P.Xh + ((size_t)b * M + m + 1) * plane, X5);
           cp_async_commit();
           // gE += the column sums, warps in a fixed order (one thread per
           // filter row and column)

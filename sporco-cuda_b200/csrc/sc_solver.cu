@@ -509,7 +509,7 @@ static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s, int f
     }
     int st = prepare_fn((const void*)fn, true);
     if (st) return st;
-    const size_t smem = col_smem_bytes(MODE, sh.hlen, tw);
+    const size_t smem = col_smem_bytes(MODE, sh.hlen, tw, sh.NT);
     const int ntiles = (cp.g.Wf + tw - 1) / tw;
     const long units = (long)ntiles * B;
     if (G > 0 && force_G <= 0) {

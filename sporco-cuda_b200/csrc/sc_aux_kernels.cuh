@@ -125,6 +125,16 @@ __global__ void warm_state_kernel(ImgState* st, int B, int* ndone) {
   st[b].status = 0;
 }
 
+// The unrolled solve's trace steps run the iteration's row pass from a
+// given V without the finalize step: count the state as past its first
+// iteration, so that the row pass recomputes Y from V at lambda / rho (at
+// V = 0 that is 0, as before the first iteration).
+__global__ void trace_state_kernel(ImgState* st, int B) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  if (st[b].k == 0) st[b].k = 1;
+}
+
 // tw[j] = exp(-2 pi i j / n), evaluated in double precision.
 __global__ void twiddle_kernel(float2* tw, int n) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;

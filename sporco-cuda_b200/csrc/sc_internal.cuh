@@ -94,7 +94,10 @@ struct RowParams {
   float* dst;              // real rows out for ROW_INV_REAL
   // adjoint (ROW_ADJ)
   float* gV;               // (B, M, H, W) gradient w.r.t. V of the step, in place
-  const float* Ymask;      // (B, M, H, W) Y the step produced (nonzero: shrinkage active)
+  const float* Ymask;      // (B, M, H, W) Y the step produced (nonzero: shrinkage active),
+                           // or with vmask its V (active: the shrinkage of V is nonzero)
+  int vmask;
+  float* Vo;               // ROW_ITER: V written here (NULL: in place, into U)
   int first;               // 1: gV holds dLoss/dY of the last iterate, no Q yet
 };
 

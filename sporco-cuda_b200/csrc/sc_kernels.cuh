@@ -249,6 +249,7 @@ row_kernel(RowParams P) {
       uscale = (float)st.uscale;
     } else if constexpr (MODE == ROW_ADJ) {
       rho = (float)st.rho;
+      thr = (float)((double)P.lam[b] / st.rho);  // as the step's ROW_ITER had it
     } else {
       if (st.rsf == 1.0) return;
       rsf_c = (float)(1.0 - 1.0 / st.rsf);
@@ -475,7 +476,12 @@ row_kernel(RowParams P) {
     ic.delta = P.delta != 0;
     // State rows of the pair (V, or Y and U) are written here.
     auto out0 = [&](long r0) -> float* {
-      return (VS ? P.U : P.Yo) + (size_t)b * img_real + (size_t)r0 * W;
+      return (VS ? (P.Vo ? P.Vo : P.U) : P.Yo) + (size_t)b * img_real + (size_t)r0 * W;
+    };
+    // ROW_ADJ: the shrinkage of the step was active at element k of a row
+    // (Y != 0; from V with vmask, as the step computed Y)
+    auto active = [&](float src, const RowW& w, int k) -> bool {
+      return P.vmask ? shrink_y(src, thr, w, k) != 0.f : src != 0.f;
     };
     auto outu = [&](long r0) -> float* { return P.U + (size_t)b * img_real + (size_t)r0 * W; };
     // The element-wise step of the iteration on the pair element k (both
@@ -538,6 +544,7 @@ row_kernel(RowParams P) {
         if (ADJ && valid) {
           float* gv = P.gV + (size_t)b * img_real + (size_t)r0 * W;
           const bool firstq = P.first != 0;
+          const RowW aw0 = roww(r0, true), aw1 = roww(r1, has1);
 #pragma unroll
           for (int m = 0; m < EM; ++m) {
             const int k = t + g * m;
@@ -546,14 +553,14 @@ row_kernel(RowParams P) {
             const float v0 = ysm[k];
             const float gy0 = firstq ? v0 : ic.a1 * v0 + rho * q0;
             const float gu0 = firstq ? 0.f : v0 - rho * q0;
-            const float n0 = usm[k] != 0.f ? gy0 : gu0;
+            const float n0 = active(usm[k], aw0, k) ? gy0 : gu0;
             gv[k] = n0;
             float n1 = 0.f;
             if (has1) {
               const float v1 = ysm[W + k];
               const float gy1 = firstq ? v1 : ic.a1 * v1 + rho * q1;
               const float gu1 = firstq ? 0.f : v1 - rho * q1;
-              n1 = usm[W + k] != 0.f ? gy1 : gu1;
+              n1 = active(usm[W + k], aw1, k) ? gy1 : gu1;
               gv[W + k] = n1;
             }
             v[m] = make_float2(ic.a * n0, ic.a * n1);
@@ -622,6 +629,7 @@ row_kernel(RowParams P) {
           // step before: gY where its shrinkage was active (Y != 0), else gU.
           float* gv = P.gV + (size_t)b * img_real + (size_t)r0 * W;
           const bool firstq = P.first != 0;
+          const RowW aw0 = roww(r0, true), aw1 = roww(r1, has1);
           for (int k = t; k < W; k += g) {
             const float2 zz = z[zs(k)];
             const float q0 = firstq ? 0.f : zz.x * P.invN;
@@ -629,14 +637,14 @@ row_kernel(RowParams P) {
             const float v0 = ysm[k];
             const float gy0 = firstq ? v0 : ic.a1 * v0 + rho * q0;
             const float gu0 = firstq ? 0.f : v0 - rho * q0;
-            const float n0 = usm[k] != 0.f ? gy0 : gu0;
+            const float n0 = active(usm[k], aw0, k) ? gy0 : gu0;
             gv[k] = n0;
             float n1 = 0.f;
             if (has1) {
               const float v1 = ysm[W + k];
               const float gy1 = firstq ? v1 : ic.a1 * v1 + rho * q1;
               const float gu1 = firstq ? 0.f : v1 - rho * q1;
-              n1 = usm[W + k] != 0.f ? gy1 : gu1;
+              n1 = active(usm[W + k], aw1, k) ? gy1 : gu1;
               gv[W + k] = n1;
             }
             z[zs(k)] = make_float2(ic.a * n0, ic.a * n1);

@@ -1012,13 +1012,23 @@ struct Solve {
   }
 
   // Y and U from the state V into y and u (u may be NULL).
-  int state_yu(float* y, float* u) {
+  // Y and U from the state V (the solver's own, or v)
+  int state_yu(float* y, float* u, const float* v = nullptr) {
     const Geom& g = pl.g;
     const size_t n = (size_t)g.M * g.H * g.W;
     dim3 grid((unsigned)std::min<size_t>((n + 255) / 256, 1024), g.B);
-    state_yu_kernel<<<grid, 256, 0, s>>>(U, y, u, sts, p->lmbda, g.M, g.H, g.W, p->l1_kind,
+    state_yu_kernel<<<grid, 256, 0, s>>>(v ? v : U, y, u, sts, p->lmbda, g.M, g.H, g.W,
+                                         p->l1_kind,
                                          p->l1_scalar, p->l1w, p->mask, rp.nonneg, rp.bnd_r,
                                          rp.bnd_c);
+    CU_TRY(cudaGetLastError());
+    ++g_launches;
+    return SC_OK;
+  }
+
+  // trace steps without finalize (trace_state_kernel)
+  int trace_state() {
+    trace_state_kernel<<<(pl.g.B + 127) / 128, 128, 0, s>>>(sts, pl.g.B);
     CU_TRY(cudaGetLastError());
     ++g_launches;
     return SC_OK;
@@ -1151,8 +1161,10 @@ extern "C" int sc_cbpdn_solve_batch(const sc_problem* probs, int nprob, const sc
 
 // ------------------------------------------------ unrolled solve + adjoint --
 // Workspace of the unrolled solve: the solver's own workspace first, then
-//   ckY, ckU (nseg, B, M, H, W)  Y and U at the start of every segment
-//   Ytr      (seg, B, M, H, W)   Y after each step of the segment being reversed
+//   ckV      (nseg, B, M, H, W)  the state V = Y + U at the start of every segment
+//   Yt, Ut   (B, M, H, W)        Y and U of a segment's start (its restart)
+//   Vtr      (seg, B, M, H, W)   V after each step of the segment being reversed
+//                                (Y of the step = its shrinkage)
 //   Xtr      (seg, B, M, H, Wp)  x^ of each of those steps
 //   gV       (B, M, H, W)        gradient w.r.t. V of the step being reversed
 //   Fb       (B, M, H, Wp)       spectra of the reverse steps
@@ -1164,7 +1176,7 @@ struct Unrolled {
   Plan pl;
   int K = 0, seg = 0, nseg = 0;
   size_t R = 0, C = 0;  // floats of a real array, complex entries of a spectrum array
-  size_t ckY = 0, ckU = 0, Ytr = 0, Xtr = 0, gV = 0, Fb = 0, gDh = 0, gSh = 0, gDr = 0;
+  size_t ckV = 0, Yt = 0, Ut = 0, Vtr = 0, Xtr = 0, gV = 0, Fb = 0, gDh = 0, gSh = 0, gDr = 0;
   // convolution form (filters of at most 16 rows, compiled column lengths
   // below 512): the forward and the recomputation use the production
   // convolution solve, the reverse pass its convolution-form adjoint
@@ -1207,9 +1219,10 @@ static int unrolled_plan(const sc_problem* p, const sc_options* o, int seg, Unro
   u->C = (size_t)g.B * g.M * g.H * g.Wp;
   size_t off = u->pl.total;
   auto take = [&](size_t bytes) { size_t r = off; off = align256(off + bytes); return r; };
-  u->ckY = take(sizeof(float) * u->R * u->nseg);
-  u->ckU = take(sizeof(float) * u->R * u->nseg);
-  u->Ytr = take(sizeof(float) * u->R * seg);
+  u->ckV = take(sizeof(float) * u->R * u->nseg);
+  u->Yt = take(sizeof(float) * u->R);
+  u->Ut = take(sizeof(float) * u->R);
+  u->Vtr = take(sizeof(float) * u->R * seg);
   u->Xtr = take(sizeof(float2) * u->C * seg);
   u->gV = take(sizeof(float) * u->R);
   u->Fb = take(sizeof(float2) * u->C);
@@ -1295,17 +1308,17 @@ extern "C" int sc_unrolled_forward(const sc_problem* p, const sc_options* o, int
   }
   if (u.conv && u.seg == u.K) {
     // One segment (seg = K): the forward keeps the trace of every step that
-    // the reverse pass needs (Y, the row spectra of X and sc / rho), so the
+    // the reverse pass needs (V, the row spectra of X and sc / rho), so the
     // backward recomputes nothing.  The trace-keeping kernels are the
-    // recomputation's.
-    float* ckY = (float*)(w + u.ckY);
-    float* Ytr = (float*)(w + u.Ytr);
+    // recomputation's: the column pass's twin and the iteration's row pass
+    // writing each step's V to a trace slot.
+    float* Vtr = (float*)(w + u.Vtr);
     float2* Xtr = (float2*)(w + u.Xtr);
     float2* SCtr = (float2*)(w + u.SCtr);
     const Geom& g = u.pl.g;
     const size_t Cs = (size_t)g.B * g.H * g.Wp;
-    if ((st = sv.state_yu(ckY, (float*)(w + u.ckU)))) return st;  // zeros
-    auto Yat = [&](int i) { return i == 0 ? ckY : Ytr + u.R * (i - 1); };
+    if ((st = sv.trace_state())) return st;
+    auto Vat = [&](int i) { return i == 0 ? sv.U : Vtr + u.R * (i - 1); };  // V_0 = 0
     for (int i = 0; i < u.K; ++i) {
       ColParams cf = sv.cp;
       cf.Xtr = Xtr + u.C * i;
@@ -1314,18 +1327,16 @@ extern "C" int sc_unrolled_forward(const sc_problem* p, const sc_options* o, int
                                          : launch_col<COL_SOLVE_C16T>(u.pl, cf, g.B, s, sv.force_G);
       if (st) return st;
       RowParams rr = sv.rp;
-      rr.Y = Yat(i);
-      rr.Yo = Yat(i + 1);
-      if ((st = launch_row<ROW_ITER_YU>(u.pl, rr, g.B, s))) return st;
+      rr.U = Vat(i);
+      rr.Vo = Vat(i + 1);
+      if ((st = launch_row<ROW_ITER>(u.pl, rr, g.B, s))) return st;
     }
-    CU_TRY(cudaMemcpyAsync(p->Y, Yat(u.K), sizeof(float) * u.R, cudaMemcpyDeviceToDevice, s));
-    return SC_OK;
+    return sv.state_yu(p->Y, (float*)(w + u.Ut), Vat(u.K));
   }
   for (int j = 0; j < u.nseg; ++j) {
-    // (Y, U) of the state at the segment's start
-    if ((st = sv.state_yu((float*)(w + u.ckY + sizeof(float) * u.R * j),
-                          (float*)(w + u.ckU + sizeof(float) * u.R * j))))
-      return st;
+    // the state V at the segment's start
+    CU_TRY(cudaMemcpyAsync(w + u.ckV + sizeof(float) * u.R * j, sv.U, sizeof(float) * u.R,
+                           cudaMemcpyDeviceToDevice, s));
     if ((st = sv.launch(std::min(u.seg, u.K - j * u.seg), untimed))) return st;
   }
   sc_result res;
@@ -1372,9 +1383,10 @@ extern "C" int sc_unrolled_backward(const sc_problem* p, const sc_options* o, in
   if (!gY || !gD || !gS) return set_status(SC_ERR_INVALID, "null gradient pointer");
   cudaStream_t s = (cudaStream_t)stream;
   unsigned char* w = (unsigned char*)ws;
-  float* ckY = (float*)(w + u.ckY);
-  float* ckU = (float*)(w + u.ckU);
-  float* Ytr = (float*)(w + u.Ytr);
+  float* ckV = (float*)(w + u.ckV);
+  float* Yt = (float*)(w + u.Yt);
+  float* Ut = (float*)(w + u.Ut);
+  float* Vtr = (float*)(w + u.Vtr);
   float2* Xtr = (float2*)(w + u.Xtr);
   float* gV = (float*)(w + u.gV);
   float2* Fb = (float2*)(w + u.Fb);
@@ -1393,13 +1405,13 @@ extern "C" int sc_unrolled_backward(const sc_problem* p, const sc_options* o, in
   // one segment with the convolution form: the forward kept every step's
   // trace, nothing is recomputed
   const bool traced = u.conv && u.seg == u.K;
-  // set-up writes zeros to the problem's Y: give it a slot that holds zeros
-  // anyway (the traced forward's start) or is rewritten (a trace slot)
-  u.p.Y = traced ? ckY : Ytr;
+  // set-up writes zeros to the problem's Y: give it the restart's scratch
+  u.p.Y = Yt;
   Solve sv;
   sv.tune = false;
   if ((st = sv.setup(&u.p, &u.o, ws, pl.total, s))) return st;
   sv.cp.delta = sv.rp.delta = 0;  // as in the forward
+  if ((st = sv.trace_state())) return st;
   if (u.conv)
     CU_TRY(cudaMemsetAsync(gE, 0, sizeof(float2) * (size_t)B * g.M * Kr * g.Wp, s));
   else
@@ -1408,21 +1420,21 @@ extern "C" int sc_unrolled_backward(const sc_problem* p, const sc_options* o, in
   CU_TRY(cudaMemcpyAsync(gV, gY, sizeof(float) * u.R, cudaMemcpyDeviceToDevice, s));
 
   RowParams ra = sv.rp;
-  ra.F = Fb; ra.gV = gV; ra.first = 1;
+  ra.F = Fb; ra.gV = gV; ra.first = 1; ra.vmask = 1;
   ColParams ca = sv.cp;
   ca.F = Fb; ca.gDh = gDh; ca.gSh = gSh; ca.Xtr = nullptr; ca.gE = gE;
   for (int j = u.nseg - 1; j >= 0; --j) {
     const int n = std::min(u.seg, u.K - j * u.seg);
-    // Y of step i of this segment: i = 0 is the checkpoint
-    auto Yat = [&](int i) { return i == 0 ? ckY + u.R * j : Ytr + u.R * (i - 1); };
-    // recompute the segment
+    // V of step i of this segment: i = 0 is the checkpoint
+    auto Vat = [&](int i) { return i == 0 ? ckV + u.R * j : Vtr + u.R * (i - 1); };
+    // recompute the segment: the row spectra of Y - U at its start (from
+    // the Y and U of the checkpoint's V, transformed as the iteration does)
     if (!traced) {
-    CU_TRY(cudaMemcpyAsync(sv.U, ckU + u.R * j, sizeof(float) * u.R, cudaMemcpyDeviceToDevice, s));
-    {
+      if ((st = sv.state_yu(Yt, Ut, Vat(0)))) return st;
       RowParams rf = sv.rp;
-      rf.Y = Yat(0);
+      rf.Y = Yt;
+      rf.U = Ut;
       if ((st = launch_row<ROW_FWD_YU>(pl, rf, B, s))) return st;
-    }
     }
     for (int i = 0; i < n && !traced; ++i) {
       ColParams cf = sv.cp;
@@ -1436,12 +1448,12 @@ extern "C" int sc_unrolled_backward(const sc_problem* p, const sc_options* o, in
       }
       if (st) return st;
       RowParams rr = sv.rp;
-      rr.Y = Yat(i);
-      rr.Yo = Yat(i + 1);
-      if ((st = launch_row<ROW_ITER_YU>(pl, rr, B, s))) return st;
+      rr.U = Vat(i);
+      rr.Vo = Vat(i + 1);
+      if ((st = launch_row<ROW_ITER>(pl, rr, B, s))) return st;
     }
     // reverse it
-    ra.Ymask = Yat(n);
+    ra.Ymask = Vat(n);
     if ((st = launch_row<ROW_ADJ>(pl, ra, B, s))) return st;
     ra.first = 0;
     for (int i = n - 1; i >= 0; --i) {
@@ -1455,7 +1467,7 @@ extern "C" int sc_unrolled_backward(const sc_problem* p, const sc_options* o, in
       }
       if (st) return st;
       if (i > 0) {
-        ra.Ymask = Yat(i);
+        ra.Ymask = Vat(i);
         if ((st = launch_row<ROW_ADJ>(pl, ra, B, s))) return st;
       }
     }

@@ -183,3 +183,31 @@ def test_unrolled_gradients_match_fp64_autograd_and_fd(shape, form, monkeypatch)
         scale = max(abs(fd), np.linalg.norm(gn) * float(torch.linalg.norm(dd)) /
                     np.sqrt(gn.size))
         assert abs(fd - an) <= 1e-4 * scale, (which, fd, an, scale)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(1, 64, 64, 8, 7, 9), (2, 128, 128, 8, 11, 24)])
+def test_checkpoint_spacings_give_identical_results(shape):
+    """The backward pass recomputes each segment from its checkpoint (the
+    state V) with the trace-keeping twins of the forward's kernels, or,
+    with one segment, reads the traces the forward kept: every spacing must
+    reproduce the forward's iterates bit for bit, so the output and both
+    gradients are identical for every spacing."""
+    import sporco_cuda.adjoint as adj
+    B, H, W, M, K, iters = shape
+    D, S, Sc = _problem(B, H, W, M, K)
+    opt = dict(_opt(), MaxMainIter=iters)
+    out = {}
+    for ckpt in ("sqrt", "all", 2, iters - 1):
+        Dg = torch.tensor(D, device="cuda", requires_grad=True)
+        Sg = torch.tensor(S, device="cuda", requires_grad=True)
+        X = adj.cbpdn_unrolled(Dg, Sg, LAM, opt, checkpoints=ckpt)
+        R = adj.reconstruct(Dg, X)
+        L = torch.sum((R - torch.tensor(Sc, device="cuda")) ** 2) + BETA * torch.sum(torch.abs(X))
+        L.backward()
+        out[ckpt] = (X.detach().cpu(), Dg.grad.cpu(), Sg.grad.cpu())
+    X0, gD0, gS0 = out["sqrt"]
+    for ckpt, (X, gD, gS) in out.items():
+        assert torch.equal(X, X0), ckpt
+        assert torch.equal(gD, gD0), ckpt
+        assert torch.equal(gS, gS0), ckpt

@@ -109,6 +109,7 @@ struct ColParams {
   int gsz;                 // threads per transform (column)
   int G;                   // CTAs (cluster ranks) sharing one column tile
   int Hs;                  // shared-memory column stride (elements)
+  int tile0;               // column tile of blockIdx.y = 0 (a launch over part of the tiles)
   float2* F;               // (B, M, H, Wp)
   const float2* Dh;        // (M, H, Wp)
   const float2* Sh;        // (B, H, Wp)

@@ -786,7 +786,7 @@ col_kernel(ColParams P) {
   float2* stg = reinterpret_cast<float2*>(smem_raw);  // [F0][F1][D]
 
   const int b = blockIdx.z;
-  const int tile = blockIdx.y;
+  const int tile = P.tile0 + blockIdx.y;
   const int rank = blockIdx.x;
   const int c0 = tile * T;
   const int g = NH > 0 ? ct_threads(NH, RM) : P.gsz;

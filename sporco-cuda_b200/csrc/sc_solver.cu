@@ -402,6 +402,8 @@ struct TunedG {
   int G;
   int rm;          // column-transform radix (8, or the default col_radix(H))
   int tw;          // columns per tile (SC_COL_TILE, or 2)
+  int G2;          // > 0: the tiles of the last, partly filled round of
+                   // clusters of G run as a second launch with clusters of G2
 };
 static std::vector<TunedG> g_tuned;
 
@@ -444,8 +446,18 @@ static int forced_radix() {
   return e && atoi(e) == 8 ? 8 : 0;
 }
 
+// SPORCO_B200_COL_SPLIT=G2 splits the column pass's partly filled last
+// round of clusters off into a launch with clusters of G2 (where it applies;
+// 0 or unset: the tuned choice).
+static int forced_split() {
+  const char* e = getenv("SPORCO_B200_COL_SPLIT");
+  if (!e || !*e) return -1;
+  const int G2 = atoi(e);
+  return G2 >= 1 && G2 <= 16 ? G2 : -1;
+}
+
 static bool tuned_size(const void* fn, const Geom& g, int* G, int* rm = nullptr,
-                       int* tw = nullptr) {
+                       int* tw = nullptr, int* G2 = nullptr) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return false;
   std::lock_guard<std::mutex> lock(g_cache_mu);
@@ -454,6 +466,7 @@ static bool tuned_size(const void* fn, const Geom& g, int* G, int* rm = nullptr,
       *G = e.G;
       if (rm) *rm = e.rm;
       if (tw) *tw = e.tw;
+      if (G2) *G2 = e.G2;
       return true;
     }
   return false;
@@ -471,23 +484,27 @@ static ColShape col_shape(int H, int rm, int tw = SC_COL_TILE) {
 }
 
 // force_G > 0: launch with that cluster size, force_rm > 0 with that column
-// radix, force_tw > 0 with tiles of that many columns (the autotuner's
-// trials); otherwise the tuned choice for the shape, else the occupancy
-// model's cluster size at the default radix and tile.
+// radix, force_tw > 0 with tiles of that many columns, force_G2 >= 0 with
+// that tail split (0: none; see TunedG) (the autotuner's trials); otherwise
+// the tuned choice for the shape, else the occupancy model's cluster size at
+// the default radix and tile.
 template <int MODE>
 static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s, int force_G = 0,
-                      int force_rm = 0, int force_tw = 0) {
+                      int force_rm = 0, int force_tw = 0, int force_G2 = -1) {
   cp.Hs = pl.Hs;
+  cp.tile0 = 0;
   if (col_clustered(MODE)) {
     const ColFn fn0 = col_fn<MODE>(cp.g.H);  // default radix and tile: the tuning key
     int G = force_G > 0 ? force_G : forced_cluster(cp.g.M);
-    int rm = force_rm, tw = force_tw;
+    if (force_G2 < 0) force_G2 = forced_split();
+    int rm = force_rm, tw = force_tw, G2 = force_G2 > 0 ? force_G2 : 0;
     if (G <= 0) {
-      int tG = 0, trm = 0, ttw = 0;
-      if (tuned_size((const void*)fn0, cp.g, &tG, &trm, &ttw)) {
+      int tG = 0, trm = 0, ttw = 0, tG2 = 0;
+      if (tuned_size((const void*)fn0, cp.g, &tG, &trm, &ttw, &tG2)) {
         G = tG;
         if (rm <= 0) rm = trm;
         if (tw <= 0) tw = ttw;
+        if (force_G2 < 0) G2 = tG2;
       }
     }
     if (force_rm <= 0 && forced_radix() > 0 && col_fn_variant<MODE>(cp.g.H, 8, SC_COL_TILE))
@@ -520,22 +537,41 @@ static int launch_col(const Plan& pl, ColParams cp, int B, cudaStream_t s, int f
     if (G <= 0 && (st = cluster_size((const void*)fn, sh.NT, smem, cp.g.M, units, &G)))
       return st;
     cp.gsz = sh.g;
-    cp.G = G;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(G, ntiles, B);
-    cfg.blockDim = dim3(sh.NT);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[2];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = G;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    set_pdl(&attr[1]);
-    cfg.attrs = attr;
-    cfg.numAttrs = pdl_enabled() ? 2 : 1;
-    CU_TRY(cudaLaunchKernelEx(&cfg, fn, cp));
-    ++g_launches;
+    // Tail split: the tiles past the last full round of one image's
+    // resident clusters of G run as a second launch with clusters of G2
+    // (fewer maps per CTA), where all of them are resident at once.  Every
+    // image of a batch is split at the same tile, so that a batch sums the
+    // maps of every tile in the same order as a single solve.
+    int t1 = ntiles;
+    if (G2 > G) {
+      int n1 = 0, n2 = 0;
+      if ((st = resident_clusters((const void*)fn, sh.NT, smem, G, &n1))) return st;
+      if ((st = resident_clusters((const void*)fn, sh.NT, smem, G2, &n2))) return st;
+      const int t = n1 > 0 ? ntiles / n1 * n1 : ntiles;
+      if (n1 > 0 && t > 0 && t < ntiles && ntiles - t <= n2) t1 = t;
+    }
+    for (int part = 0; part < 2; ++part) {
+      const int Gp = part ? G2 : G;
+      const int ntl = part ? ntiles - t1 : t1;
+      if (ntl <= 0) continue;
+      cp.G = Gp;
+      cp.tile0 = part ? t1 : 0;
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(Gp, ntl, B);
+      cfg.blockDim = dim3(sh.NT);
+      cfg.dynamicSmemBytes = smem;
+      cfg.stream = s;
+      cudaLaunchAttribute attr[2];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = Gp;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      set_pdl(&attr[1]);
+      cfg.attrs = attr;
+      cfg.numAttrs = pdl_enabled() ? 2 : 1;
+      CU_TRY(cudaLaunchKernelEx(&cfg, fn, cp));
+      ++g_launches;
+    }
   } else {
     // forward / inverse only: maps split 8 ways, no cluster
     ColFn fn = col_fn<MODE>(cp.g.H);
@@ -794,19 +830,19 @@ struct Solve {
     return SC_OK;
   }
 
-  // The column pass of the iteration at cluster size G, column radix rm and
-  // tiles of tw columns (0: the tuned choice, else the model at the default
-  // radix and tile).
-  int launch_iter_col(int G, int rm = 0, int tw = 0) {
+  // The column pass of the iteration at cluster size G, column radix rm,
+  // tiles of tw columns and tail split G2 (0: the tuned choice, else the
+  // model at the default radix and tile; G2 < 0: the tuned split).
+  int launch_iter_col(int G, int rm = 0, int tw = 0, int G2 = -1) {
     const int B = pl.g.B;
     if (G <= 0) G = force_G;
     switch (col_mode) {
-      case COL_SOLVE_W: return launch_col<COL_SOLVE_W>(pl, cp, B, s, G, rm, tw);
-      case COL_SOLVE: return launch_col<COL_SOLVE>(pl, cp, B, s, G, rm, tw);
-      case COL_SOLVE_C8: return launch_col<COL_SOLVE_C8>(pl, cp, B, s, G, rm, tw);
-      case COL_SOLVE_C16: return launch_col<COL_SOLVE_C16>(pl, cp, B, s, G, rm, tw);
-      case COL_SOLVE_G16: return launch_col<COL_SOLVE_G16>(pl, cp, B, s, G, rm, tw);
-      default: return launch_col<COL_SOLVE_P>(pl, cp, B, s, G, rm, tw);
+      case COL_SOLVE_W: return launch_col<COL_SOLVE_W>(pl, cp, B, s, G, rm, tw, G2);
+      case COL_SOLVE: return launch_col<COL_SOLVE>(pl, cp, B, s, G, rm, tw, G2);
+      case COL_SOLVE_C8: return launch_col<COL_SOLVE_C8>(pl, cp, B, s, G, rm, tw, G2);
+      case COL_SOLVE_C16: return launch_col<COL_SOLVE_C16>(pl, cp, B, s, G, rm, tw, G2);
+      case COL_SOLVE_G16: return launch_col<COL_SOLVE_G16>(pl, cp, B, s, G, rm, tw, G2);
+      default: return launch_col<COL_SOLVE_P>(pl, cp, B, s, G, rm, tw, G2);
     }
   }
   // The iteration's column kernel with radix rm and tiles of tw columns
@@ -831,10 +867,13 @@ struct Solve {
   // from 512: half the threads and shared memory per CTA, twice the tiles)
   // and every cluster size the device can hold with it (kClusterSizes, at
   // most M); two rounds, the faster time of each kept, on the freshly
-  // initialised state.  It keeps the fastest (radix, tile, cluster size) for
-  // later launches of that shape and initialises the iterates again (the
-  // trials overwrite the spectra).  It waits for the device once, at that
-  // first set-up.
+  // initialised state.  For one image it then times the fastest with the
+  // tiles of a partly filled last round of clusters split off into a second
+  // launch with larger clusters (TunedG::G2), and keeps the split where it
+  // is faster by more than 1 %.  It keeps the fastest (radix, tile, cluster
+  // size, split) for later launches of that shape and initialises the
+  // iterates again (the trials overwrite the spectra).  It waits for the
+  // device once, at that first set-up.
   int tune_col() {
     const Geom& g = pl.g;
     const int rdef = col_radix(g.H);
@@ -871,23 +910,47 @@ struct Solve {
       for (int i = 0; i < nc && !st; ++i) {
         float ms = 0.f;
         if (cudaEventRecord(e0, s) != cudaSuccess) { st = SC_ERR_CUDA; break; }
-        st = launch_iter_col(cand[i].G, cand[i].rm, cand[i].tw);
+        st = launch_iter_col(cand[i].G, cand[i].rm, cand[i].tw, 0);
         if (!st && cudaEventRecord(e1, s) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
             cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
           cand[i].ms = std::min(cand[i].ms, ms);
       }
     }
+    int bi = 0;
+    for (int i = 1; i < nc && !st; ++i)
+      if (cand[i].ms < cand[bi].ms) bi = i;
+    // the tail split of the fastest
+    int best_G2 = 0;
+    float best_ms = cand[bi].ms;
+    std::vector<std::pair<int, float>> splits;
+    for (int G2 : kClusterSizes) {
+      if (st || g.B != 1 || G2 <= cand[bi].G || G2 > g.M) continue;
+      float t2 = 1e30f;
+      for (int round = 0; round < 2 && !st; ++round) {
+        float ms = 0.f;
+        if (cudaEventRecord(e0, s) != cudaSuccess) { st = SC_ERR_CUDA; break; }
+        st = launch_iter_col(cand[bi].G, cand[bi].rm, cand[bi].tw, G2);
+        if (!st && cudaEventRecord(e1, s) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
+            cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+          t2 = std::min(t2, ms);
+      }
+      splits.push_back({G2, t2});
+      if (t2 < 0.99f * best_ms) {
+        best_ms = t2;
+        best_G2 = G2;
+      }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (st) return st;
-    int bi = 0;
-    for (int i = 1; i < nc; ++i)
-      if (cand[i].ms < cand[bi].ms) bi = i;
     if (autotune_verbose()) {
       fprintf(stderr, "sporco_b200 autotune: column pass %dx%d M=%d:", g.H, g.W, g.M);
       for (int i = 0; i < nc; ++i)
         fprintf(stderr, " r%d/t%d/G=%d %.3f ms", cand[i].rm, cand[i].tw, cand[i].G, cand[i].ms);
-      fprintf(stderr, " -> r%d/t%d/G=%d\n", cand[bi].rm, cand[bi].tw, cand[bi].G);
+      for (const auto& sp : splits) fprintf(stderr, " split G2=%d %.3f ms", sp.first, sp.second);
+      fprintf(stderr, " -> r%d/t%d/G=%d", cand[bi].rm, cand[bi].tw, cand[bi].G);
+      if (best_G2 > 0) fprintf(stderr, " split G2=%d", best_G2);
+      fprintf(stderr, "\n");
     }
     int dev = 0;
     CU_TRY(cudaGetDevice(&dev));
@@ -898,7 +961,8 @@ struct Solve {
       for (const TunedG& e : g_tuned)
         known = known || (e.dev == dev && e.fn == fn && e.H == g.H && e.W == g.W && e.M == g.M);
       if (!known)
-        g_tuned.push_back({dev, fn, g.H, g.W, g.M, cand[bi].G, cand[bi].rm, cand[bi].tw});
+        g_tuned.push_back(
+            {dev, fn, g.H, g.W, g.M, cand[bi].G, cand[bi].rm, cand[bi].tw, best_G2});
     }
     return init_iterates();
   }

@@ -102,3 +102,44 @@ def test_tile_widths_agree_bitwise_and_with_oracle(tmp_path, size, M, K, variant
     Xo = _oracle(D, S, W, variant, iters)
     rel = np.linalg.norm(X2.astype(np.float64) - Xo) / np.linalg.norm(Xo)
     assert rel < REL_TOL, rel
+
+
+SPLIT_CHILD = r"""
+import sys
+import numpy as np
+sys.path[:0] = [{root!r}, {pkg!r}]
+import sporco_cuda.cbpdn as cb
+d = np.load({inp!r})
+opt = {{"MaxMainIter": int(d["iters"]), "RelStopTol": 0.0, "RelaxParam": 1.8, "rho": None,
+        "AutoRho": {{"Enabled": True, "Period": 1, "Scaling": 1000.0, "RsdlRatio": 1.2,
+                     "AutoScaling": True}}}}
+singles = [cb.cbpdn(d["D"], s, 0.05, opt) for s in (d["S0"], d["S1"])]
+batch = cb.cbpdn_batched(d["D"], [d["S0"], d["S1"]], 0.05, opt)
+np.savez({out!r}, X0=singles[0], X1=singles[1], B0=batch[0], B1=batch[1])
+"""
+
+
+@pytest.mark.gpu
+def test_tail_split_batch_equals_single_and_oracle(tmp_path):
+    """2048 x 2048 with clusters of 2: 257 column tiles fill three rounds of
+    the 74 resident clusters and part of a fourth, whose 35 tiles the split
+    runs as a second launch with clusters of 3.  A batch of two images is
+    split at the same tile, so it equals the two single solves bit for bit;
+    both agree with the FP64 oracle."""
+    D, S0 = _synth(2048, 2048, 8, 16, 301)
+    _, S1 = _synth(2048, 2048, 8, 16, 302)
+    iters = 6
+    inp = str(tmp_path / "in.npz")
+    out = str(tmp_path / "out.npz")
+    np.savez(inp, D=D, S0=S0, S1=S1, iters=iters)
+    code = SPLIT_CHILD.format(root=ROOT, pkg=os.path.join(ROOT, "sporco-cuda_b200"), inp=inp,
+                              out=out)
+    env = dict(os.environ, SPORCO_B200_COL_CLUSTER="2", SPORCO_B200_COL_SPLIT="3")
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    o = np.load(out)
+    assert np.array_equal(o["X0"], o["B0"]) and np.array_equal(o["X1"], o["B1"])
+    Xo = _oracle(D, S0, None, "cbpdn", iters)
+    rel = np.linalg.norm(o["X0"].astype(np.float64) - Xo) / np.linalg.norm(Xo)
+    assert rel < REL_TOL, rel

@@ -125,6 +125,22 @@ __global__ void warm_state_kernel(ImgState* st, int B, int* ndone) {
   st[b].status = 0;
 }
 
+// The convolution column solves' filter-row entries: for the row spectra e
+// of the first Kr rows of every filter (Dh, before the column transform),
+// (Re e, Im e, Re e + Im e, Im e - Re e), the sums the solves' three-multiply
+// complex products take.
+__global__ void filter_rows_kernel(const float2* __restrict__ Dh, float4* __restrict__ E, int M,
+                                   int Kr, int H, int Wp) {
+  const size_t n = (size_t)M * Kr * Wp;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t c = i % Wp, mr = i / Wp;
+    const size_t m = mr / Kr, r = mr - m * Kr;
+    const float2 e = Dh[(m * H + r) * Wp + c];
+    E[i] = make_float4(e.x, e.y, e.x + e.y, e.y - e.x);
+  }
+}
+
 // The unrolled solve's trace steps run the iteration's row pass from a
 // given V without the finalize step: count the state as past its first
 // iteration, so that the row pass recomputes Y from V at lambda / rho (at

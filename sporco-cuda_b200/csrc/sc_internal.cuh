@@ -119,7 +119,8 @@ struct ColParams {
   float mu;
   const float* wgrd;       // (M,)
   const float* Psum;       // (H, Wp) sum_m |Df_m|^2 (solve with one d for all maps)
-  const float2* E;         // (M, Kr, Wp) row spectra of the filter rows (COL_SOLVE_C*)
+  const float4* E;         // (M, Kr, Wp) row spectra e of the filter rows (COL_SOLVE_C*),
+                           // as (Re e, Im e, Re e + Im e, Im e - Re e)
   int Kr;                  // filter rows
   ImgState* st;
   float2* Xtr;             // COL_SOLVE_X: x^ also written here (B, M, H, Wp)
@@ -203,13 +204,13 @@ __host__ __device__ inline size_t row_slot_bytes(int mode, int zlen, int W, int 
 // SC_COL_TILE) interleaved columns.  The solve double-buffers the spectrum
 // tile and stages the dictionary tile: [F0][F1][D]; the cluster reduction
 // reuses [F1][D].  The convolution solves use three tiles and three staged
-// filter-row tiles; the convolution adjoint two more tiles (the forward's
+// filter-row tiles (16 bytes an entry); the convolution adjoint two more tiles (the forward's
 // SC trace and row spectra of X) and per-warp partial sums of the
 // dictionary gradient for its nt threads (two maps).
 __host__ __device__ inline size_t col_smem_bytes(int mode, int hlen, int tw = SC_COL_TILE,
                                                  int nt = SC_COL_MAX_THREADS) {
   const size_t tile = (size_t)tw * hlen * 8;
   return (col_clustered(mode) ? (col_adj_conv(mode) ? 5 : 3) * tile : tile) +
-         (size_t)3 * col_taps(mode) * tw * 8 +
+         (size_t)3 * col_taps(mode) * tw * 16 +
          (col_adj_conv(mode) ? (size_t)2 * (nt / 32) * col_taps(mode) * tw * 8 : 0);
 }

@@ -493,9 +493,12 @@ row_kernel(RowParams P) {
                          float* O0, float* Q0, float* f) -> float2 {
       constexpr int DL = decltype(dl)::value;
       const RowW w{};
-      const float yu0 = iter_elem<VS, true, DL>(zz.x * P.invN, ysm[k], TWO ? usm[k] : 0.f, w,
+      // (DL: the column pass has applied 1 / (H W) already)
+      const float x0 = DL == 1 ? zz.x : zz.x * P.invN;
+      const float x1 = DL == 1 ? -zz.y : -zz.y * P.invN;
+      const float yu0 = iter_elem<VS, true, DL>(x0, ysm[k], TWO ? usm[k] : 0.f, w,
                                                 k, tc0, tq0, ic, f, O0 + k, Q0 + k);
-      const float yu1 = iter_elem<VS, true, DL>(-zz.y * P.invN, ysm[W + k],
+      const float yu1 = iter_elem<VS, true, DL>(x1, ysm[W + k],
                                                 TWO ? usm[W + k] : 0.f, w, k, tc1, tq1, ic, f,
                                                 O0 + W + k, Q0 + W + k);
       return make_float2(yu0, yu1);
@@ -503,10 +506,11 @@ row_kernel(RowParams P) {
     auto elem_gen = [&](const RowW& w0, const RowW& w1, bool has1, int k, float2 zz, float* O0,
                         float* Q0, float* f) -> float2 {
       float yu1 = 0.f;
-      const float yu0 = iter_elem<VS, false>(zz.x * P.invN, ysm[k], TWO ? usm[k] : 0.f, w0, k,
+      const float xn = P.delta ? 1.f : P.invN;  // see elem_fast
+      const float yu0 = iter_elem<VS, false>(zz.x * xn, ysm[k], TWO ? usm[k] : 0.f, w0, k,
                                              thr, thr_prev, ic, f, O0 + k, Q0 + k);
       if (has1)
-        yu1 = iter_elem<VS, false>(-zz.y * P.invN, ysm[W + k], TWO ? usm[W + k] : 0.f, w1, k,
+        yu1 = iter_elem<VS, false>(-zz.y * xn, ysm[W + k], TWO ? usm[W + k] : 0.f, w1, k,
                                    thr, thr_prev, ic, f, O0 + W + k, Q0 + W + k);
       return make_float2(yu0, yu1);
     };
@@ -883,9 +887,11 @@ col_kernel(ColParams P) {
       float2* A = stg;            // cluster sum, its spectrum, then sc / rho
       float2* Bt = stg + TL;      // spectrum tiles (pass 1: with A; pass 2: with Ct)
       float2* Ct = stg + 2 * TL;  // partial sums of this CTA
-      float2* Es = stg + 3 * TL;  // [3][KMAX][T] filter rows
+      // [3][KMAX][T] filter rows, one float4 (two float2 slots) an entry
+      constexpr int ES = 2 * KMAX * T;  // float2 slots of one staged filter tile
+      float2* Es = stg + 3 * TL;
       // ADJ: the forward's sc / rho tile, then per-warp correlation partials
-      float2* W4 = Es + 3 * KMAX * T;
+      float2* W4 = Es + 3 * ES;
       float2* X5 = W4 + TL;       // ADJ: the forward's row spectra of X of the map
       float2* red = X5 + TL;      // [2][NT / 32][KMAX][T]
       // 16-byte copies: T / 2 per tile row
@@ -897,10 +903,16 @@ col_kernel(ColParams P) {
         }
       };
       auto issue_E = [&](int m, float2* dst) {
-        for (int q = tid; q < CPR * Kr; q += NT) {
-          const int r = q / CPR, h = q % CPR;
-          cp_async16(dst + r * T + 2 * h, P.E + ((size_t)m * Kr + r) * Wp + c0 + 2 * h);
+        float4* d4 = reinterpret_cast<float4*>(dst);
+        for (int q = tid; q < T * Kr; q += NT) {
+          const int r = q / T, h = q - r * T;
+          cp_async16(d4 + r * T + h, P.E + ((size_t)m * Kr + r) * Wp + c0 + h);
         }
+      };
+      // filter-row entry of tap tp of this thread's column: (Re e, Im e,
+      // Re e + Im e, Im e - Re e)
+      auto ent = [&](const float2* ecur, int tp) -> float4 {
+        return reinterpret_cast<const float4*>(ecur)[tp * T + cc];
       };
       const size_t plane = (size_t)H * Wp;
       const float2* Sh = P.Sh + (size_t)b * plane + c0;
@@ -944,7 +956,7 @@ col_kernel(ColParams P) {
       for (int q = 0; q < 2; ++q) {
         if (m0 + q < m1) {
           issue_tile(Fi + (size_t)(m0 + q) * plane, buf(q));
-          issue_E(m0 + q, Es + q * KMAX * T);
+          issue_E(m0 + q, Es + q * ES);
         }
         cp_async_commit();
       }
@@ -957,10 +969,10 @@ col_kernel(ColParams P) {
           if (m + 2 < m1) {
             const int bn = bi == 0 ? 2 : bi - 1;  // (m - m0 + 2) mod 3
             issue_tile(Fi + (size_t)(m + 2) * plane, buf(bn));
-            issue_E(m + 2, Es + bn * KMAX * T);
+            issue_E(m + 2, Es + bn * ES);
           }
           cp_async_commit();
-          body(buf(bi), Es + bi * KMAX * T);
+          body(buf(bi), Es + bi * ES);
         }
       };
       // Filter-row counts with compile-time tap loops in Gauss's form below:
@@ -1001,10 +1013,10 @@ col_kernel(ColParams P) {
           float ec[KR], ep[KR], em[KR];
 #pragma unroll
           for (int tp = 0; tp < KR; ++tp) {
-            const float2 e = ecur[tp * T + cc];
+            const float4 e = ent(ecur, tp);
             ec[tp] = e.x;
-            ep[tp] = e.x + e.y;
-            em[tp] = e.y - e.x;
+            ep[tp] = e.z;  // c + d
+            em[tp] = e.w;  // d - c
           }
           // window element j = P(r0 - (KR - 1) + j) meets output i at tap
           // KR - 1 + i - j (the last tap first, as in the general form)
@@ -1039,7 +1051,7 @@ col_kernel(ColParams P) {
 #pragma unroll
           for (int tp = KMAX - 1; tp >= 0; --tp) {
             if (tp < Kr) {
-              const float2 e = ecur[tp * T + cc];
+              const float4 e = ent(ecur, tp);
 #pragma unroll
               for (int i = 0; i < L; ++i) {
                 const float2 v = w[i - tp + KMAX - 1];
@@ -1060,6 +1072,7 @@ col_kernel(ColParams P) {
       // correction sum_t conj(E_m(t)) sc(r + t) / rho (the row pass adds
       // Y - U, whose row spectra P_m are), so pass 2 reads no P tiles
       const bool DL = !GRD && !ADJ && !TRACE && P.delta;
+      const float irho_s = DL ? (float)(1.0 / ((double)rho * H * G.W)) : irho;
       // pass 2's first tile lands during the reduction and the transforms
       if (m0 < m1) {
         if (!DL) issue_tile(Fi + (size_t)m0 * plane, Bt);
@@ -1105,7 +1118,7 @@ col_kernel(ColParams P) {
       if constexpr (PIPE3) {
         if (m0 + 1 < m1 && !GAUSS2) {
           if (!DL) issue_tile(Fi + (size_t)(m0 + 1) * plane, Ct);
-          issue_E(m0 + 1, Es + KMAX * T);
+          issue_E(m0 + 1, Es + ES);
         }
         cp_async_commit();
       }
@@ -1148,7 +1161,9 @@ col_kernel(ColParams P) {
               const float sd = __ldg(&P.Psum[(size_t)kr * Wp + c0 + cc]) * irho;
               const float qd = 1.f / (1.f + sd);
               const float2 cb = make_float2((Sv.x * sd + q.x) * qd, (Sv.y * sd + q.y) * qd);
-              v = make_float2((Sv.x - cb.x) * irho, -(Sv.y - cb.y) * irho);  // conj(SC) / rho
+              // conj(SC) / rho (DL: also times 1 / (H W), the row pass's
+              // normalisation of its inverse transform, which then skips it)
+              v = make_float2((Sv.x - cb.x) * irho_s, -(Sv.y - cb.y) * irho_s);
             }
             }
           }
@@ -1194,15 +1209,15 @@ col_kernel(ColParams P) {
         float ec[KR], ep[KR], em[KR];
 #pragma unroll
         for (int tp = 0; tp < KR; ++tp) {
-          const float2 e = ecur[tp * T + cc];
+          const float4 e = ent(ecur, tp);
           if constexpr (ADJ) {  // -conj(E)
             ec[tp] = -e.x;
-            ep[tp] = e.y - e.x;
-            em[tp] = e.y + e.x;
+            ep[tp] = e.w;   // d - c
+            em[tp] = e.z;   // c + d
           } else {
             ec[tp] = e.x;
-            ep[tp] = e.x - e.y;
-            em[tp] = -e.y - e.x;
+            ep[tp] = -e.w;  // c - d
+            em[tp] = -e.z;  // -(c + d)
           }
         }
         float k1[L], k3[L], k2[L];
@@ -1260,12 +1275,12 @@ col_kernel(ColParams P) {
           int it = 0;
           for (int m = m0; m < m1; ++m, ++it) {
             const float2* cur = (it & 1) ? Ct : Bt;
-            const float2* ecur = Es + (it & 1) * KMAX * T;
+            const float2* ecur = Es + (it & 1) * ES;
             cp_async_wait<0>();  // P(m), E(m): the only copies in flight
             __syncthreads();
             if (m + 1 < m1) {
               if (!DL) issue_tile(Fi + (size_t)(m + 1) * plane, (it & 1) ? Bt : Ct);
-              issue_E(m + 1, Es + ((it + 1) & 1) * KMAX * T);
+              issue_E(m + 1, Es + ((it + 1) & 1) * ES);
             }
             cp_async_commit();
             float2 o[L];
@@ -1306,20 +1321,20 @@ col_kernel(ColParams P) {
       int bi = 0;
       for (int m = m0; m < m1; ++m, ++it, bi = bi == 2 ? 0 : bi + 1) {
         float2* cur = PIPE3 ? (bi == 0 ? Bt : bi == 1 ? Ct : A) : (it & 1) ? Ct : Bt;
-        const float2* ecur = Es + (PIPE3 ? bi : (it & 1)) * KMAX * T;
+        const float2* ecur = Es + (PIPE3 ? bi : (it & 1)) * ES;
         if constexpr (PIPE3) {
           cp_async_wait<1>();  // P(m), E(m) (those of m + 1 may still be in flight)
           __syncthreads();
           if (m + 2 < m1) {
             const int bn = bi == 0 ? 2 : bi - 1;  // (it + 2) mod 3
             if (!DL) issue_tile(Fi + (size_t)(m + 2) * plane, bn == 0 ? Bt : bn == 1 ? Ct : A);
-            issue_E(m + 2, Es + bn * KMAX * T);
+            issue_E(m + 2, Es + bn * ES);
           }
           cp_async_commit();
         } else if constexpr (ADJ) {
           if (m + 1 < m1) {
             issue_tile(Fi + (size_t)(m + 1) * plane, (it & 1) ? Bt : Ct);
-            issue_E(m + 1, Es + ((it + 1) & 1) * KMAX * T);
+            issue_E(m + 1, Es + ((it + 1) & 1) * ES);
           }
           cp_async_commit();
           cp_async_wait<1>();  // P(m), E(m)
@@ -1329,7 +1344,7 @@ col_kernel(ColParams P) {
           __syncthreads();
           if (m + 1 < m1) {
             issue_tile(Fi + (size_t)(m + 1) * plane, (it & 1) ? Bt : Ct);
-            issue_E(m + 1, Es + ((it + 1) & 1) * KMAX * T);
+            issue_E(m + 1, Es + ((it + 1) & 1) * ES);
           }
           cp_async_commit();
         }
@@ -1369,7 +1384,7 @@ col_kernel(ColParams P) {
 #pragma unroll
         for (int tp = 0; tp < KMAX; ++tp) {
           if (tp < Kr && !convd) {
-            const float2 e = ecur[tp * T + cc];
+            const float4 e = ent(ecur, tp);
 #pragma unroll
             for (int i = 0; i < L; ++i) {
               const float2 v = w[i + tp];

@@ -232,7 +232,7 @@ static int plan_problem(const sc_problem* p, const sc_options* o, Plan* pl) {
   pl->off_Dh = take(sizeof(float2) * spec_img);
   pl->off_Sh = take(sizeof(float2) * (size_t)g.H * g.Wp * g.B);
   pl->off_Ps = take(sizeof(float) * (size_t)g.H * g.Wp);
-  pl->off_E = take(sizeof(float2) * (size_t)g.M * p->Kr * g.Wp);
+  pl->off_E = take(sizeof(float4) * (size_t)g.M * p->Kr * g.Wp);
   pl->off_twW = take(sizeof(float2) * g.W);
   pl->off_twH = take(sizeof(float2) * g.H);
   pl->off_part = take(sizeof(double) * 5 * (size_t)pl->row_nblk * g.B);
@@ -711,7 +711,7 @@ struct Solve {
                : (spec_col(pl.g.H) && p->Kr <= 8)  ? COL_SOLVE_C8
                : (spec_col(pl.g.H) && p->Kr <= 16) ? COL_SOLVE_C16
                                                    : COL_SOLVE_P;
-    float2* Erows = (float2*)((unsigned char*)workspace + pl.off_E);
+    float4* Erows = (float4*)((unsigned char*)workspace + pl.off_E);
 
     // warm_start 2: the spectra of D and S in the workspace are still valid
     const bool spectra = o->warm_start != 2;
@@ -730,9 +730,13 @@ struct Solve {
       r.pw = pl.pw; r.twW = twW; r.F = Dh; r.D = p->D; r.Kr = p->Kr; r.Kc = p->Kc;
       if ((st = launch_row<ROW_FWD_DICT>(pl, r, 1, s))) return st;
       // the row spectra of the filter rows, before the column transform
-      CU_TRY(cudaMemcpy2DAsync(Erows, sizeof(float2) * p->Kr * g.Wp, Dh,
-                               sizeof(float2) * g.H * g.Wp, sizeof(float2) * p->Kr * g.Wp, g.M,
-                               cudaMemcpyDeviceToDevice, s));
+      {
+        const size_t ne = (size_t)g.M * p->Kr * g.Wp;
+        filter_rows_kernel<<<(unsigned)std::min<size_t>((ne + 255) / 256, 4096), 256, 0, s>>>(
+            Dh, Erows, g.M, p->Kr, g.H, g.Wp);
+        CU_TRY(cudaGetLastError());
+        ++g_launches;
+      }
       ColParams c = {};
       c.g = g; c.g.B = 1; c.ph = pl.ph; c.twH = twH; c.twW = twW; c.F = Dh;
       if ((st = launch_col<COL_FWD>(pl, c, 1, s))) return st;

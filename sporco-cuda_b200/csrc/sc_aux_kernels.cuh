@@ -12,12 +12,14 @@ __global__ void psum_kernel(const float2* __restrict__ Dh, float* __restrict__ P
                             size_t plane) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= plane) return;
-  float s = 0.f;
+  // summed in double precision: the solves' 1 / (rho + Psum) passes Psum's
+  // relative error on to X almost undiminished (Psum >> rho for many maps)
+  double s = 0.0;
   for (int m = 0; m < M; ++m) {
     const float2 d = __ldg(&Dh[(size_t)m * plane + i]);
-    s += d.x * d.x + d.y * d.y;
+    s += (double)d.x * d.x + (double)d.y * d.y;
   }
-  Psum[i] = s;
+  Psum[i] = (float)s;
 }
 
 // ============================================================== finalize ==

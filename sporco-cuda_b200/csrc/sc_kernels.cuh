@@ -1149,21 +1149,23 @@ col_kernel(ColParams P) {
               v = make_float2(cb.x, -cb.y);  // conj(cb)
             } else {
             const float2 Sv = __ldg(&Sh[(size_t)kr * Wp + cc]);
+            // SC = S^ - cb with cb = (S^ Psum / d + rho q / d) / (1 + Psum / d),
+            // computed as SC = (S^ - rho q / d) / (1 + Psum / d): the same
+            // value without subtracting cb, which is close to S^ when
+            // Psum >> d (many maps), from S^ (that cancellation multiplied
+            // the rounding error of SC by about 1 + Psum / d)
             if constexpr (GRD) {
-              // cb = (S^ Psum / d + rho q / d) / (1 + Psum / d)
               const float id = inv_d(kr);
               const float sd = __ldg(&P.Psum[(size_t)kr * Wp + c0 + cc]) * id;
-              const float qd = 1.f / (1.f + sd);
-              const float2 cb = make_float2((Sv.x * sd + rho * q.x * id) * qd,
-                                            (Sv.y * sd + rho * q.y * id) * qd);
-              v = make_float2((Sv.x - cb.x) * id, -(Sv.y - cb.y) * id);  // conj(SC) / d
+              const float f = id / (1.f + sd);
+              const float rid = rho * id;
+              v = make_float2((Sv.x - rid * q.x) * f, -(Sv.y - rid * q.y) * f);  // conj(SC) / d
             } else {
               const float sd = __ldg(&P.Psum[(size_t)kr * Wp + c0 + cc]) * irho;
-              const float qd = 1.f / (1.f + sd);
-              const float2 cb = make_float2((Sv.x * sd + q.x) * qd, (Sv.y * sd + q.y) * qd);
               // conj(SC) / rho (DL: also times 1 / (H W), the row pass's
               // normalisation of its inverse transform, which then skips it)
-              v = make_float2((Sv.x - cb.x) * irho_s, -(Sv.y - cb.y) * irho_s);
+              const float f = irho_s / (1.f + sd);
+              v = make_float2((Sv.x - q.x) * f, -(Sv.y - q.y) * f);
             }
             }
           }
@@ -1572,9 +1574,9 @@ col_kernel(ColParams P) {
       if (k >= Wf) return make_float2(0.f, 0.f);
       const float2 Sv = __ldg(&Sh[(size_t)kr * Wp + c]);
       const float sd = __ldg(&P.Psum[(size_t)kr * Wp + k]) * irho;
+      // (S^ - acc) / (1 + Psum / rho): S^ - cb without the cancellation
       const float q = 1.f / (1.f + sd);
-      const float2 cb = make_float2((Sv.x * sd + acc.x) * q, (Sv.y * sd + acc.y) * q);
-      return make_float2(Sv.x - cb.x, Sv.y - cb.y);
+      return make_float2((Sv.x - acc.x) * q, (Sv.y - acc.y) * q);
     };
 #pragma unroll
     for (int i = 0; i < EPT; ++i) {
@@ -1956,9 +1958,9 @@ col_kernel(ColParams P) {
       if (k >= Wf) return make_float2(0.f, 0.f);
       const float2 Sv = __ldg(&Sh[(size_t)kr * Wp + c]);
       const float sd = denom(kr, c, ds);
+      // (S^ - rho acc) / (1 + sd): S^ - cb without the cancellation
       const float q = 1.f / (1.f + sd);
-      const float2 cb = make_float2((Sv.x * sd + rho * acc.x) * q, (Sv.y * sd + rho * acc.y) * q);
-      return make_float2(Sv.x - cb.x, Sv.y - cb.y);
+      return make_float2((Sv.x - rho * acc.x) * q, (Sv.y - rho * acc.y) * q);
     };
 #pragma unroll
     for (int i = 0; i < EPT; ++i) {

@@ -77,9 +77,13 @@ def _check(D, S, X, Xo, rho, info, lam, mu=0.0, grd=False, mask=None):
     rho_o = np.asarray(info["hist"]["rho"])
     assert len(rho) == len(rho_o)
     assert np.unique(rho_o).size > 1, "rho never changed: the fix-up did not run"
-    # continuous AutoScaling factors from float32 residual sums: 1e-4 (a
-    # flipped decision would differ by a factor of about 1.2 or more)
-    np.testing.assert_allclose(rho, rho_o, rtol=1e-4)
+    # rho is a product of continuous AutoScaling factors sqrt(r / (s xi)),
+    # and the dual residual s is the norm of the change of Y between two
+    # iterations: late in a solve it is small and carries the float32 error
+    # of both iterates, which grows along the trajectory (up to 1.4e-4 here
+    # at 25 iterations); 5e-4 still separates that from a flipped decision,
+    # which differs by a factor of about 1.2 or more
+    np.testing.assert_allclose(rho, rho_o, rtol=5e-4)
     assert _rel(X, Xo) < REL_TOL
     Dm = np.moveaxis(D, 2, 0).astype(np.float64)
     Sd = S.astype(np.float64) * (mask if mask is not None else 1.0)

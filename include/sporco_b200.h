@@ -245,8 +245,8 @@ unsigned long long sc_launch_count(void);
  * o->max_iter = K plain-cbpdn ADMM iterations at the fixed rho p->rho0 (no
  * stopping test, no adaptive rho; p->grd = 0, p->mask = NULL, p->U0 = p->U_out
  * = NULL), and the reverse pass of those iterations.
- *   sc_unrolled_forward writes Y_K to p->Y and keeps (Y, U) every seg
- *     iterations in the workspace (seg: 1..K; ceil(sqrt(K)) balances memory
+ *   sc_unrolled_forward writes Y_K to p->Y and keeps the state V = Y + U
+ *     every seg iterations in the workspace (seg: 1..K; ceil(sqrt(K)) balances memory
  *     against the one recomputation of each segment in the backward pass;
  *     seg = K with filters of at most 16 rows and compiled column lengths
  *     below 512 keeps the trace of every step instead, so that the backward
@@ -255,7 +255,7 @@ unsigned long long sc_launch_count(void);
  *     options, seg and workspace, takes gY = dLoss/dY_K (B, M, H, W) and
  *     writes dLoss/dD to gD (M, Kr, Kc) and dLoss/dS to gS (B, H, W).
  * The workspace (sc_unrolled_workspace_size bytes, 256-byte aligned) holds
- * the solver's own workspace, the checkpoints, one segment's Y and x^ of
+ * the solver's own workspace, the checkpoints, one segment's V and x^ of
  * every step, and the gradient spectra.  Returns 0 when the problem is not
  * a plain fixed-rho cbpdn problem or seg is out of range. */
 size_t sc_unrolled_workspace_size(const sc_problem *p, const sc_options *o, int seg);

@@ -6,10 +6,12 @@ rho: adaptive rho and early stopping are not differentiated) and returns the
 coefficient maps; its backward pass returns dLoss/dD and dLoss/dS through all
 iterations.  Both passes are single calls into the native library
 (``sc_unrolled_forward`` / ``sc_unrolled_backward``): the forward pass is the
-solver's own fused iteration, keeping (Y, U) every ceil(sqrt(K)) iterations
-(``checkpoints="sqrt"``, the default); the backward pass recomputes each
-segment once from its checkpoint (keeping Y, the row spectra of X and sc of
-every step) and reverses it with fused kernels of the same shape as the
+solver's own fused iteration, keeping the state V = Y + U every
+ceil(sqrt(K)) iterations (``checkpoints="sqrt"``, the default); the backward
+pass recomputes each segment once from its checkpoint with the same row pass
+(keeping V, the row spectra of X and sc of every step, so that the
+recomputed iterates equal the forward's bit for bit) and reverses it with
+fused kernels of the same shape as the
 forward ones: the shrinkage subgradient mask, the transposed
 Sherman-Morrison solve (the system is Hermitian, so it is the forward solve
 again) and the dictionary and signal gradients (for filters of at most 16
